@@ -1,0 +1,83 @@
+// fdtd_internal.h -- shared host/device definitions of the B200 FDTD library.
+//
+// Device data layout (HBM):
+//   fields      six float arrays E/H x,y,z in the reference order (i slowest,
+//               k fastest), ping-pong pairs: every step reads one set and
+//               writes the other, so that CTAs may recompute a neighbour's H
+//               row without racing with its owner;
+//   class map   one byte per cell: index of a coefficient class (DevClass)
+//               derived on the host from the material table, the interface
+//               map, the dispersive-neighbour rule and the PEC rule;
+//   CPML        psi slabs per face in the reference layout (boundary.c:102-280),
+//               psi_H ping-pong like the fields, psi_E in place;
+//   ADE state   E^{n-1}, P_D^n, P_D^{n-1} (+ 2 CP poles) per component, full
+//               grid arrays touched only by dispersive cells.
+#pragma once
+#include <stdint.h>
+
+#define FDTD_MAX_CLASSES 256
+#define FDTD_MAX_ADE 8
+
+// class flag bits
+#define CF_ADE_X      0x001u   // Ex taken by the ADE branch (tbc == 0)
+#define CF_ADE_Y      0x002u
+#define CF_ADE_Z      0x004u
+#define CF_ADE_BRANCH 0x008u   // the cell enters the dispersive branch
+#define CF_PEC_X      0x010u   // PEC rule zeroes Ex (yee.c:1138-1237)
+#define CF_PEC_Y      0x020u
+#define CF_PEC_Z      0x040u
+
+struct DevClass {
+    float ca[3];    // ordinary update E = ca*E + cb*curl (get_cabs, yee.c:1397-1493)
+    float cb[3];    // same cb, also used by the boundary_estep CPML corrections
+    float cba[3];   // CPML cb inside the ADE branch (yee.c:950-1057), from the ADE material
+    float da, db;   // H update (yee.c:219-243) and CPML-H db (get_db, yee.c:1620-1647)
+    float tsfe;     // (dt/dx)/epsilon(cell) of the TSF-E correction (source.c:548,566)
+    uint32_t flags;
+    int32_t ade;    // ADE coefficient set
+    float pad[2];
+};
+
+struct DevAde {      // calculate_ade_a/bp/c (plan.c:2737-2763), rounded to float
+    float c0dx;      // ade_c0 / dx
+    float c1, c2, c3;
+    float a0, a1, a2, one_m_a1;
+    float bp0[2], bp1[2], bp2[2], bp3[2], bp4[2];
+    float one_m_bp1[2];
+};
+
+struct DevPlan {
+    int xr, yr, zr;
+    int64_t si, sj;                 // strides of i and j (k stride is 1)
+    float dx;                       // cell size (cubic cells)
+    // fields: [0..2] = E x,y,z, [3..5] = H x,y,z
+    const float *fin[6];
+    float *fout[6];
+    const uint8_t *cls;
+    const DevClass *classes;
+    int nclasses;
+    // ADE
+    int nade;
+    const DevAde *ade;
+    float *ep[3], *dp[3], *dpp[3];
+    float *pp_[3][2], *p_[3][2];
+    // CPML: face order x0 xn y0 yn z0 zn
+    int cp_on[6], cp_d[6];
+    const float *be[6], *ce[6], *bh[6], *ch[6];
+    const float *ike[3], *ikh[3];   // 1/kappa per axis (E and H), length xr / yr / zr
+    float *psie[6][2];              // x: {peyx, pezx} y: {pexy, pezy} z: {pexz, peyz}
+    const float *psih_in[6][2];     // x: {phyx, phzx} y: {phxy, phzy} z: {phxz, phyz}
+    float *psih_out[6][2];
+    // TSF
+    int tsf_on;
+    int t0[3], t1[3];               // box corners i0 j0 k0 / in jn kn
+    int tskip[6];
+    const uint8_t *tmap[6];         // per face cell: bit0 apply (mat_too_close_check), bit1 PEC at the face cell
+    double corr, hcor;
+    double tax, tay, taz;           // propagation direction sin(t)cos(p), sin(t)sin(p), cos(t)
+    int trx_origin, try_origin, trz_origin;  // dcomp corner (source.c:54-107), or flags for the rx=0 quirk
+    int trx_zero;                   // dcomp leaves rx = 0 (theta > pi/2, phi in (pi/2, pi])
+    double gex, gey, gez, ghx, ghy, ghz;     // projections gex..ghz of a unit field (source.c:131-165)
+    const double *aux_e, *aux_h;
+    int jres;
+};

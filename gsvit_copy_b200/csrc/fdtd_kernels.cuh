@@ -1,0 +1,57 @@
+// fdtd_kernels.cuh -- launch interface of the device kernels (fdtd_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fdtd_internal.h"
+
+// fused tile: TK cells along k (contiguous, one warp per j row), TJ rows along j
+#define FDTD_TK 32
+#define FDTD_TJ 16
+
+struct DevAux {                 // 1D auxiliary grid of the TSF source (1dpool.c)
+    double *e, *h;              // res values each
+    double *bnd;                // 8 saved boundary values (Sv1DPool fbnx*)
+    const double *wave;
+    int nwave;
+    int res;
+    double ce, chh;             // (1/eps)*dt/(EPS0*dx1) and (1/mu)*dt/(MU0*dx1)
+    double lc;                  // Liao factor (dt*c - dx1)/(dt*c + dx1)
+    int *step;                  // device step counter
+    // probes of the previous step
+    int nprobes;
+    const int64_t *probe_cells;
+    const float *const *fields; // 6 pointers to the field set that holds the previous step
+    double *probe_out;          // [p][nsteps][6]
+    int nsteps_planned;
+};
+
+struct DevNfff {
+    int ns;                     // surface cells
+    int nfreq;
+    const int32_t *cell;        // linear index of the surface cell
+    const int32_t *nstride;     // +/- stride along the face normal
+    const float *const *e;      // 3 E field pointers (the set written by this step)
+    double2 *acc;               // [(f*6 + q)*ns + s], q = Ex,Ey,Ez, dEx,dEy,dEz
+    const double *omega_dt;     // nfreq
+    const int *step;            // device step counter (already advanced)
+    double inv2dx;
+};
+
+void launch_aux_step(const DevAux &a, cudaStream_t st);
+void launch_probe_capture(const DevAux &a, cudaStream_t st);
+cudaError_t launch_fused_step(const DevPlan &p, int ichunk, bool ade, int npoles, cudaStream_t st);
+void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st);
+
+struct DevFarfield {
+    int npoints, nfreq, ns;
+    const int32_t *points;      // 3*npoints
+    const int32_t *istart;
+    const int32_t *cell_ijk;    // 3*ns  (i,j,k of each surface cell)
+    const int8_t *face;         // ns, 0..5 = x0 xn y0 yn z0 zn
+    const double2 *acc;
+    const double *omega;        // nfreq
+    double dt, dx;
+    double2 *out;               // [(p*nfreq + f)*3 + c]
+};
+void launch_farfield_finalize(const DevFarfield &f, cudaStream_t st);

@@ -421,8 +421,8 @@ def rough_surface_scene(res: int = 512, zres: Optional[int] = None, dx: float = 
 
 def selftest_scene(code: str, res: int, nsteps: int) -> Scene:
     """GSvit self-test geometry of make_test (tests.c:93-268) for the TSF +
-    CPML + NFFF ids ('xx031111' electric voxel box with MATMODE_CHECK 1,
-    'xx035011' PEC box): res^3 cells of 1 um, CPML `10 3 -1 0.03 4`, TSF box
+    CPML + NFFF ids ("31111" electric voxel box with MATMODE_CHECK 1,
+    "35011" PEC box): res^3 cells of 1 um, CPML `10 3 -1 0.03 4`, TSF box
     [20, res-20] with theta = phi = pi/2, psi = 0 and the generated pulse
     `2 20e-6 10 5`, NFFF box [16, res-16] and one Ramahi point at res-12."""
     dx = 1e-6
@@ -430,13 +430,13 @@ def selftest_scene(code: str, res: int, nsteps: int) -> Scene:
     s = Scene(name=f"selftest_{res}{code}", xres=res, yres=res, zres=res, dx=dx, dt=dt, nsteps=nsteps)
     p0 = (res // 2 + 10, 30, 30)
     p1 = (res - 30, res - 30, res - 30)
-    if code == "031111":       # TEST_MATERIAL_ELECTRIC, matcheck -> ELECTRIC voxel data
+    if code == "31111":       # TEST_MATERIAL_ELECTRIC, matcheck -> ELECTRIC voxel data
         s.matmode = abi.MATMODE_ELECTRIC
         s.epsilon = np.full((res, res, res), np.float32(EPS0), dtype=np.float32)
         s.sigma = np.zeros((res, res, res), dtype=np.float32)
         voxel_box(s.epsilon, p0, p1, np.float32(f32(2.0) * EPS0))
         s.mats = []
-    elif code == "035011":     # TEST_MATERIAL_LINTAB_PEC, no matcheck -> FULL
+    elif code == "35011":     # TEST_MATERIAL_LINTAB_PEC, no matcheck -> FULL
         s.matmode = abi.MATMODE_FULL
         s.mats = [vacuum_material(), pec_material()]
         s.mat = np.zeros((res, res, res), dtype=np.int32)

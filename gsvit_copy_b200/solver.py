@@ -1,0 +1,131 @@
+"""Python host mirror of the C ABI: one `Solver` per plan.
+
+The method names follow the stages of GSvit's GPU driver they replace
+(sv_pool_gpu_copyto / copyfrom / ystep_* / getpoints / apply_farfield,
+pool.h:98-128); the work itself runs in libgsvit_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import abi
+
+
+class Solver:
+    def __init__(self, scene, device: int = 0):
+        self.lib = abi.load_library()
+        self.scene = scene
+        self._desc, self._keep = scene.desc()
+        h = C.c_void_p()
+        abi.check(self.lib.fdtd_plan_create(C.byref(self._desc), device, C.byref(h)), "fdtd_plan_create")
+        self.h = h
+        self.shape = (scene.xres, scene.yres, scene.zres)
+        self.n = scene.ncells
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fdtd_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle: Optional[int]):
+        abi.check(self.lib.fdtd_set_stream(self.h, C.c_void_p(stream_handle or 0)), "fdtd_set_stream")
+
+    def sync(self):
+        abi.check(self.lib.fdtd_sync(self.h), "fdtd_sync")
+
+    # -- fields (sv_pool_gpu_copyto / copyfrom)
+    def set_fields(self, comps: Sequence[Optional[np.ndarray]], mask: int = abi.EH):
+        arrs = [None if c is None else np.ascontiguousarray(c, dtype=np.float64).reshape(-1) for c in comps]
+        abi.check(self.lib.fdtd_set_fields(self.h, mask, abi.field_ptrs(arrs)), "fdtd_set_fields")
+
+    def fields(self, mask: int = abi.EH, dtype=np.float64):
+        if dtype == np.float32:
+            out = [np.empty(self.shape, dtype=np.float32) if mask & (1 << c) else None for c in range(6)]
+            abi.check(self.lib.fdtd_get_fields_f32(self.h, mask, abi.field_ptrs(out, C.c_float)), "fdtd_get_fields_f32")
+        else:
+            out = [np.empty(self.shape) if mask & (1 << c) else None for c in range(6)]
+            abi.check(self.lib.fdtd_get_fields(self.h, mask, abi.field_ptrs(out)), "fdtd_get_fields")
+        return out
+
+    # -- stepping
+    def step(self, n: int = 1):
+        abi.check(self.lib.fdtd_step(self.h, n), "fdtd_step")
+
+    def step_graph(self, n: int, chunk: int = 32):
+        abi.check(self.lib.fdtd_step_graph(self.h, n, chunk), "fdtd_step_graph")
+
+    def step_timed(self, n: int):
+        ms = C.c_double()
+        cnt = C.c_int()
+        abi.check(self.lib.fdtd_step_timed(self.h, n, C.byref(ms), C.byref(cnt)), "fdtd_step_timed")
+        return ms.value, cnt.value
+
+    @property
+    def step_count(self) -> int:
+        s = C.c_int()
+        abi.check(self.lib.fdtd_get_step(self.h, C.byref(s)), "fdtd_get_step")
+        return s.value
+
+    # -- outputs
+    def probes(self) -> np.ndarray:
+        p = 0 if self.scene.probes is None else len(self.scene.probes)
+        out = np.zeros((p, max(self.scene.nsteps, 1), 6))
+        if p:
+            abi.check(self.lib.fdtd_get_probes(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), out.size),
+                      "fdtd_get_probes")
+        return out
+
+    def nfff_spectrum(self) -> np.ndarray:
+        """Complex far-field DFT, shape (npoints, nfreq, 3)."""
+        f = self.scene.nfff
+        npt, nf = len(f["points"]), len(f["omega"])
+        out = np.zeros((npt, nf, 3, 2))
+        abi.check(self.lib.fdtd_nfff_spectrum(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), out.size),
+                  "fdtd_nfff_spectrum")
+        return out[..., 0] + 1j * out[..., 1]
+
+    def map(self, which: int) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.int32)
+        abi.check(self.lib.fdtd_get_map(self.h, which, out.ctypes.data_as(C.POINTER(C.c_int32)), out.size),
+                  "fdtd_get_map")
+        return out
+
+    @property
+    def nclasses(self) -> int:
+        v = C.c_int()
+        abi.check(self.lib.fdtd_get_nclasses(self.h, C.byref(v)), "fdtd_get_nclasses")
+        return v.value
+
+    def step_bytes(self) -> float:
+        v = C.c_double()
+        abi.check(self.lib.fdtd_step_bytes(self.h, C.byref(v)), "fdtd_step_bytes")
+        return v.value
+
+    # -- checkpoints
+    def snapshot(self) -> bytearray:
+        sz = C.c_size_t()
+        abi.check(self.lib.fdtd_snapshot_size(self.h, C.byref(sz)), "fdtd_snapshot_size")
+        buf = bytearray(sz.value)
+        cbuf = (C.c_char * sz.value).from_buffer(buf)
+        abi.check(self.lib.fdtd_snapshot_save(self.h, C.cast(cbuf, C.c_void_p), sz.value), "fdtd_snapshot_save")
+        return buf
+
+    def restore(self, buf: bytearray):
+        cbuf = (C.c_char * len(buf)).from_buffer(buf)
+        abi.check(self.lib.fdtd_snapshot_restore(self.h, C.cast(cbuf, C.c_void_p), len(buf)), "fdtd_snapshot_restore")

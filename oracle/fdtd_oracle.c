@@ -550,8 +550,8 @@ oracle_state *oracle_create(const fdtd_desc *d, char *err)
                              pow(cos(s->t.theta), 4));
         s->jres = (int)(sqrt((double)(s->xres * s->xres + s->yres * s->yres + s->zres * s->zres)) + 250);
         s->jdx = s->dx / s->corr;
-        s->je = calloc((size_t)s->jres, sizeof(double));
-        s->jh = calloc((size_t)s->jres, sizeof(double));
+        s->je = calloc((size_t)s->jres + 4, sizeof(double));   /* dval may touch data[res] */
+        s->jh = calloc((size_t)s->jres + 4, sizeof(double));
         s->jeps = malloc(sizeof(double) * (size_t)s->jres);
         s->jmu = malloc(sizeof(double) * (size_t)s->jres);
         for (i = 0; i < s->jres; i++) {
