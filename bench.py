@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Throughput of the B200 FDTD time step on the 512^3 rough Drude-silver surface.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one "step" = one full Yee time step of the whole grid): 512^3 cells,
+dx = 5 nm, dt = 0.5 x the 3D Courant limit, 16-cell CPML on all faces, a
+Gaussian-correlated rough surface (rms 10 nm, correlation 50 nm, seed 2024)
+with Drude silver (eps_inf 3.7, wp 1.38e16 rad/s, gamma 2.73e13 1/s) below and
+vacuum above, a p-polarised TSF plane wave at 30 deg incidence (600 nm pulse),
+three probes, and running DFTs at 500/600/700 nm on the NFFF box for a
+91 x 181 far-field grid.  Inputs are synthetic (seeded height map), built by
+gsvit_copy_b200.plan.rough_surface_scene.  Metric: Gcell-updates/s (cells x
+steps / device time), higher is better.
+
+Arms:
+  --impl b200       the CUDA library through its C ABI (default).  Prints one
+                    JSON line with value (device-timed steps, fields resident in
+                    HBM), e2e (the same job through the public Solver API with
+                    pinned host buffers: initial fields uploaded, K steps, probes
+                    and final E read back), the roofline of the dominant kernel,
+                    the clocks seen and a CPU baseline.
+  --impl reference  GSvit's own CPU stepping code (yee.c, boundary.c, source.c,
+                    farfield.c ... compiled from its sources into
+                    oracle/_ref/libgsvit_ref.so) on all host threads, on a
+                    bounded sample of the same workload (see SAMPLE below).
+
+Multi-GPU: the time step does not shard here; `--gpus N` under torchrun runs N
+independent replicas (one per rank and GPU), timed as the max over ranks, and
+`value` is the sum of all ranks' cell updates over that time (weak scaling).
+The field arrays (3.2 GB per set) are far larger than L2, so no L2 flush is
+needed between steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "Gcell-updates/s"
+UNIT = "Gcell/s"
+# bounded CPU sample of the workload: same scene recipe at 128^3 with the far
+# grid scaled with the edge length (46 x 91 points), so that the far-field
+# work per cell update matches the 512^3 case
+SAMPLE_RES = 128
+SAMPLE_ANGLES = (46, 91)
+SAMPLE_DESC = ("rough Drude-silver surface scene at 128^3 (dx 5 nm, 16-cell CPML, TSF 30 deg, "
+               "NFFF 3 wavelengths on a 46x91 far grid: far work per cell update as at 512^3)")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--res", type=int, default=512)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def workload_scene(res, nsteps_planned):
+    from gsvit_copy_b200 import plan
+    return plan.rough_surface_scene(res=res, nsteps=nsteps_planned)
+
+
+def sample_scene(nsteps_planned):
+    from gsvit_copy_b200 import plan
+    return plan.rough_surface_scene(res=SAMPLE_RES, nsteps=nsteps_planned, nfff_angles=SAMPLE_ANGLES)
+
+
+def config_block(res, scene):
+    return {
+        "workload": f"rough Drude-silver surface {res}^3, 16-cell CPML, TSF 30 deg p-pol 600 nm, "
+                    f"NFFF running DFT 3 wavelengths, 91x181 far grid, 3 probes",
+        "cells": scene.ncells,
+        "grid": [scene.xres, scene.yres, scene.zres],
+        "planned_steps": scene.nsteps,
+        "l2": "inputs larger than L2 (fields 3.2 GB per ping-pong set at 512^3); no flush",
+        "parallelism": "replicas",
+    }
+
+
+# ----------------------------------------------------------------- clocks
+
+CLOCK_FIELDS = ["index", "pci.bus_id", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+                "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+                "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while it runs (read only)."""
+
+    def __init__(self, bus_id=None):
+        self.bus_id = bus_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        import tempfile
+        fd, self.path = tempfile.mkstemp(prefix="clk", suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + ",".join(CLOCK_FIELDS), "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) != len(CLOCK_FIELDS):
+                    continue
+                if self.bus_id and self.bus_id.lower() not in p[1].lower() and p[1].lower() not in self.bus_id.lower():
+                    continue
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[2]) for r in rows if num(r[2]) is not None]
+        mx = [num(r[3]) for r in rows if num(r[3]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[6:10]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def bus_id_of(dev):
+    import torch
+    try:
+        p = torch.cuda.get_device_properties(dev)
+        dom, bus, d = getattr(p, "pci_domain_id", None), getattr(p, "pci_bus_id", None), getattr(p, "pci_device_id", None)
+        if bus is not None:
+            return "%08X:%02X:%02X" % (dom or 0, bus, d or 0)
+    except Exception:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------- peaks / ncu figures
+
+def hbm_peak():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(res):
+    """DRAM bytes per launch of the bulk kernel from the committed ncu summary of this workload."""
+    path = os.path.join(HERE, "profiles", f"bulk_kernel_rough{res}.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------- CPU sample
+
+def cpu_sample_run(steps=None, warmup=1, budget_s=15.0):
+    """Time GSvit's own CPU stepping code (oracle/_ref) on the bounded sample.
+    Returns (Gcell/s, threads, kind, steps timed)."""
+    from oracle import pyoracle
+    kind = "reference" if pyoracle.reference_available() else "port"
+    scene = sample_scene(4000)
+    cpu = pyoracle.CpuSolver(scene, "reference" if kind == "reference" else "oracle")
+    cpu.step(warmup)
+    if steps is None:
+        t = time.perf_counter()
+        cpu.step(1)
+        one = time.perf_counter() - t
+        steps = int(max(2, min(200, budget_s / max(one, 1e-6))))
+    t = time.perf_counter()
+    cpu.step(steps)
+    dt = time.perf_counter() - t
+    cpu.close()
+    threads = int(os.environ.get("OMP_NUM_THREADS", 0)) or os.cpu_count()
+    return scene.ncells * steps / dt / 1e9, threads, kind, steps
+
+
+def run_reference(a):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    value, threads, kind, steps = cpu_sample_run(steps=a.steps, warmup=a.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded height map)",
+        "config": {"workload": f"rough Drude-silver surface {a.res}^3 (sampled: {SAMPLE_DESC})",
+                   "sample_res": SAMPLE_RES},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{SAMPLE_DESC}, {steps} steps after {a.warmup} warm-up"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    line["ms_per_step"] = SAMPLE_RES ** 3 / (value * 1e9) * 1e3
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- GPU arm
+
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from gsvit_copy_b200 import abi
+    from gsvit_copy_b200.solver import Solver
+
+    rank, local, world = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device (the library has no CPU path)")
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    K, W = a.steps, a.warmup
+    scene = workload_scene(a.res, max(4000, K + W + 64))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    g = Solver(scene, device=local)
+    g.set_stream(stream.cuda_stream)
+
+    g.step(W)
+    g.sync()
+    torch.cuda.synchronize()
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(bus_id_of(local)) as clk:
+        e0.record(stream)
+        g.step(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    g.sync()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    clocks = clk.summary()
+    value = scene.ncells * K * world / (ms * 1e-3) / 1e9
+
+    # per-kernel profile of a few more steps (CUDA events around each launch)
+    prof = g.step_profile(8)
+    nprof = 8
+    bulk_s = prof["bulk_ms"] / nprof * 1e-3
+    peak, peak_kind = hbm_peak()
+    achieved = prof["bulk_bytes"] / bulk_s / 1e9 if bulk_s > 0 else None
+    roofline = {"kernel": "bulk_kernel (TMA-tiled fused H+E step of the interior box)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
+                "traffic": ncu_traffic(a.res), "algorithmic_bytes": prof["bulk_bytes"],
+                "ms_per_launch": prof["bulk_ms"] / nprof,
+                "step_share": prof["bulk_ms"] / prof["total_ms"] if prof["total_ms"] else None}
+    step_bytes = g.step_bytes()
+    step_gbs = step_bytes / (ms / K * 1e-3) / 1e9
+    gpu_launches = int(prof["launches_per_step"]) * K
+
+    # end to end through the public API with pinned host buffers
+    shape = g.shape
+    host = [torch.empty(shape, dtype=torch.float32, pin_memory=True) for _ in range(6)]
+    outE = [torch.empty(shape, dtype=torch.float32, pin_memory=True) for _ in range(3)]
+    import ctypes as C
+    ptrs = (C.POINTER(C.c_float) * 6)(*[C.cast(h.data_ptr(), C.POINTER(C.c_float)) for h in host])
+    abi.check(g.lib.fdtd_get_fields_f32(g.h, abi.EH, ptrs), "fdtd_get_fields_f32")
+    optrs = (C.POINTER(C.c_float) * 6)(*([C.cast(h.data_ptr(), C.POINTER(C.c_float)) for h in outE] + [None] * 3))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    abi.check(g.lib.fdtd_set_fields_f32(g.h, abi.EH, ptrs), "fdtd_set_fields_f32")
+    g.step(K)
+    pr = g.probes()
+    abi.check(g.lib.fdtd_get_fields_f32(g.h, abi.E_ALL, optrs), "fdtd_get_fields_f32")
+    g.sync()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    h2d = 6 * scene.ncells * 4
+    d2h = 3 * scene.ncells * 4 + pr.nbytes
+    e2e = {"value": scene.ncells * K * world / e2e_s / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+           "job": "upload 6 fields f32 from pinned host, K steps, read probes + final E (f32) to pinned host"}
+    g.close()
+    barrier()
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        v, thr, kind, n = cpu_sample_run(budget_s=a.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": kind,
+               "sample": f"{SAMPLE_DESC}, {n} steps after 1 warm-up, all host threads"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded Gaussian-correlated height map)",
+            "config": config_block(a.res, scene), "clocks": clocks, "e2e": e2e,
+            "gpu_launches": gpu_launches, "roofline": roofline,
+            "step_gbs_algorithmic": step_gbs, "step_bytes_algorithmic": step_bytes,
+            "kernel_ms_per_step": {k: prof[k] / nprof for k in ("bulk_ms", "slab_ms", "aux_ms", "nfff_ms", "total_ms")},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_b200(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -133,6 +133,7 @@ def load_library():
         "fdtd_step_graph": ([P, C.c_int, C.c_int], C.c_int),
         "fdtd_get_step": ([P, C.POINTER(C.c_int)], C.c_int),
         "fdtd_step_timed": ([P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),
+        "fdtd_step_profile": ([P, C.c_int, _dp], C.c_int),
         "fdtd_get_probes": ([P, _dp, C.c_size_t], C.c_int),
         "fdtd_nfff_spectrum": ([P, _dp, C.c_size_t], C.c_int),
         "fdtd_get_map": ([P, C.c_int, _ip, C.c_size_t], C.c_int),
@@ -154,7 +155,7 @@ def load_library():
 HEADER_SYMBOLS = [
     "fdtd_plan_create", "fdtd_plan_destroy", "fdtd_set_stream", "fdtd_sync",
     "fdtd_set_fields", "fdtd_get_fields", "fdtd_get_fields_f32", "fdtd_set_fields_f32",
-    "fdtd_step", "fdtd_step_graph", "fdtd_get_step", "fdtd_step_timed",
+    "fdtd_step", "fdtd_step_graph", "fdtd_get_step", "fdtd_step_timed", "fdtd_step_profile",
     "fdtd_get_probes", "fdtd_nfff_spectrum", "fdtd_get_map", "fdtd_get_nclasses",
     "fdtd_snapshot_size", "fdtd_snapshot_save", "fdtd_snapshot_restore",
     "fdtd_last_error", "fdtd_step_bytes",

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -16,6 +17,7 @@
 
 #include "../../include/gsvit_b200.h"
 #include "fdtd_internal.h"
+#include "fdtd_bulk.cuh"
 #include "fdtd_kernels.cuh"
 #include "plan_host.h"
 
@@ -86,7 +88,18 @@ struct fdtd_plan {
     const float **d_fieldptrs[2] = {nullptr, nullptr};   // device copies of fields[s]
     int *d_step = nullptr;
     int host_step = 0;
-    int ichunk = 0;
+    // work decomposition: general kernel (CPML slabs, grid edges) and TMA bulk kernel
+    SlabBox *d_boxes = nullptr;     // slab boxes (one thread per cell)
+    int nboxes = 0;
+    long long nslab_blocks = 0;
+    BulkItem *d_bulk = nullptr;
+    int nbulk = 0;
+    bool bulk_on = false;
+    BulkMaps bmaps[2];
+    int *d_err = nullptr;
+    int region[6] = {0, 0, 0, 0, 0, 0};   // bulk box Xlo Xhi Ylo Yhi Zlo Zhi
+    int tsf_cells = 0;                    // face cells of the TSF correction tables
+    double bulk_bytes = 0, slab_bytes = 0; // algorithmic HBM bytes per launch
     // NFFF
     bool nfff = false;
     int nfff_npoints = 0, nfff_nfreq = 0, nfff_ns = 0;
@@ -120,15 +133,29 @@ DevPlan plan_for(const fdtd_plan *P, int in)
     return d;
 }
 
+// the Yee/CPML/TSF/ADE part of one step: general items + bulk items
+int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
+{
+    DevPlan d = plan_for(P, in);
+    cudaError_t e;
+    if (P->bulk_on) {   // first: the slab E update reads H^{n+1/2} the bulk kernel wrote next to the slabs
+        e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, st);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
+    }
+    e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, st);
+    if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
+    return FDTD_OK;
+}
+
 int launch_step(fdtd_plan *P, cudaStream_t st)
 {
     const int in = P->cur;
     DevAux a = P->aux;
     a.fields = P->d_fieldptrs[in];
     launch_aux_step(a, st);
-    DevPlan d = plan_for(P, in);
-    cudaError_t e = launch_fused_step(d, P->ichunk, P->hp.has_ade, P->hp.maxpoles, st);
-    if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("fused step launch: ") + cudaGetErrorString(e));
+    if (P->tsf_cells) launch_tsf_faces(P->dp, P->tsf_cells, st);
+    int rc = launch_fused(P, in, st);
+    if (rc != FDTD_OK) return rc;
     if (P->nfff) {
         DevNfff n = P->nf;
         n.e = P->d_efieldptrs[1 - in];
@@ -203,7 +230,14 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
             P->snap.push_back({P->fields[s][c], n * sizeof(float)});
         }
     uint8_t *cls;
-    CA(upload(P->mem, &cls, hp.cls.data(), n), "class map");
+    {
+        const int pitch = (hp.zr + 15) / 16 * 16;   // TMA row pitch must be a multiple of 16 bytes
+        std::vector<uint8_t> padded((size_t)hp.xr * hp.yr * pitch, 0);
+        for (size_t row = 0; row < (size_t)hp.xr * hp.yr; row++)
+            std::memcpy(&padded[row * pitch], &hp.cls[row * hp.zr], hp.zr);
+        CA(upload(P->mem, &cls, padded.data(), padded.size()), "class map");
+        d.cpitch = pitch;
+    }
     d.cls = cls;
     DevClass *classes;
     CA(upload(P->mem, &classes, hp.classes.data(), hp.classes.size()), "class table");
@@ -279,6 +313,10 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
             uint8_t *m;
             CA(upload(P->mem, &m, hp.tmap[f].data(), hp.tmap[f].size()), "tsf map");
             d.tmap[f] = m;
+            CA(P->mem.alloc(&d.tcor_h[f], hp.tmap[f].size()), "tsf corrections");
+            CA(P->mem.alloc(&d.tcor_e[f], hp.tmap[f].size()), "tsf corrections");
+            d.tnb[f] = hp.tmap_dims[f][1];
+            P->tsf_cells += (int)hp.tmap[f].size();
         }
         d.corr = hp.corr;
         d.hcor = hp.dt / hp.dx / MU0;
@@ -437,14 +475,100 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
         P->ff.out = outp;
         bytes += (double)cell.size() * (9 * 4 + (double)f.nfreq * 6 * 16 * 2);
     }
-    // i-chunking: enough CTAs to fill the SMs a few times over
+    // work decomposition: the bulk box (outside every CPML slab, one extra
+    // plane on the low sides so that its halo row/column/plane is slab-free)
+    // goes to the TMA kernel when the k rows are 16-byte multiples; the rest
+    // (slabs, zeroed planes) to the general kernel
     {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        const int tiles = ((hp.zr + FDTD_TK - 1) / FDTD_TK) * ((hp.yr + FDTD_TJ - 1) / FDTD_TJ);
-        int want = (4 * sms + tiles - 1) / tiles;
-        int chunks = std::max(1, std::min(want, hp.xr / 16));
-        P->ichunk = (hp.xr + chunks - 1) / chunks;
+        const int X = hp.xr, Y = hp.yr, Z = hp.zr;
+        int lo[3], hi[3];
+        const int res[3] = {X, Y, Z};
+        for (int ax = 0; ax < 3; ax++) {
+            lo[ax] = hp.cp[2 * ax].enabled ? hp.cp[2 * ax].depth + 1 : 0;
+            hi[ax] = hp.cp[2 * ax + 1].enabled ? res[ax] - hp.cp[2 * ax + 1].depth : res[ax];
+        }
+        const char *nob = getenv("GSVIT_B200_NO_BULK");
+        P->bulk_on = (Z % 4 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
+        std::vector<SlabBox> boxes;
+        std::vector<BulkItem> blk;
+        long long nblk = 0;
+        auto add_box = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
+            if (i0 >= i1 || j0 >= j1 || k0 >= k1) return;
+            boxes.push_back({i0, i1, j0, j1, k0, k1, nblk});
+            nblk += ((long long)(i1 - i0) * (j1 - j0) * (k1 - k0) + 255) / 256;
+        };
+        auto chunks = [&](int a0, int a1, int tiles, int *len) {
+            int planes = a1 - a0;
+            int want = std::max(1, (8 * sms + tiles - 1) / std::max(tiles, 1));
+            int nch = std::max(1, std::min(want, planes / 24));
+            *len = (planes + nch - 1) / nch;
+        };
+        if (P->bulk_on) {
+            add_box(0, lo[0], 0, Y, 0, Z);
+            add_box(hi[0], X, 0, Y, 0, Z);
+            add_box(lo[0], hi[0], 0, lo[1], 0, Z);
+            add_box(lo[0], hi[0], hi[1], Y, 0, Z);
+            add_box(lo[0], hi[0], lo[1], hi[1], 0, lo[2]);
+            add_box(lo[0], hi[0], lo[1], hi[1], hi[2], Z);
+            int tiles = ((hi[1] - lo[1] + BULK_TILE - 1) / BULK_TILE) * ((hi[2] - lo[2] + BULK_TILE - 1) / BULK_TILE), len;
+            chunks(lo[0], hi[0], tiles, &len);
+            // chunk-major order: CTAs that run together share planes, so the
+            // halo rows/columns of neighbouring tiles are served from L2
+            for (int ib = lo[0]; ib < hi[0]; ib += len)
+                for (int j0 = lo[1]; j0 < hi[1]; j0 += BULK_TILE)
+                    for (int k0 = lo[2]; k0 < hi[2]; k0 += BULK_TILE)
+                        blk.push_back({j0, k0, ib, std::min(hi[0], ib + len), hi[1], hi[2], 0, 0});
+            for (int ax = 0; ax < 3; ax++) { P->region[2 * ax] = lo[ax]; P->region[2 * ax + 1] = hi[ax]; }
+        } else {
+            add_box(0, X, 0, Y, 0, Z);
+        }
+        if (nblk > 0x7fffffffLL) return bail(cudaErrorInvalidValue, "grid too large for the slab kernels");
+        {   // algorithmic bytes per launch: 24 B field reads + 24 B writes + 1 class byte per cell;
+            // (3 + 4 * poles) state arrays x (4 B read + 4 B write) per dispersive field component;
+            // 4 psi arrays x (4 B read + 4 B write) per CPML cell (slab kernels only)
+            auto cell_bytes = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
+                double b = 0;
+#pragma omp parallel for reduction(+ : b) schedule(static)
+                for (int i = i0; i < i1; i++)
+                    for (int j = j0; j < j1; j++)
+                        for (int k = k0; k < k1; k++) {
+                            const DevClass &c = hp.classes[hp.cls[((size_t)i * Y + j) * Z + k]];
+                            b += 49.0;
+                            if (c.flags & CF_ADE_BRANCH)
+                                b += (((c.flags & CF_ADE_X) ? 1 : 0) + ((c.flags & CF_ADE_Y) ? 1 : 0) + ((c.flags & CF_ADE_Z) ? 1 : 0)) *
+                                     (3 + 4 * hp.maxpoles) * 8.0;
+                        }
+                return b;
+            };
+            double total = 0;
+            for (auto &b : boxes) total += cell_bytes(b.i0, b.i1, b.j0, b.j1, b.k0, b.k1);
+            double psi = 0;
+            for (int f = 0; f < 6; f++)
+                if (hp.cp[f].enabled) {
+                    const int dep = hp.cp[f].depth;
+                    psi += ((f < 2) ? (double)dep * Y * Z : (f < 4) ? (double)X * dep * Z : (double)X * Y * dep) * 4 * 8.0;
+                }
+            P->slab_bytes = total + psi;
+            P->bulk_bytes = P->bulk_on ? cell_bytes(lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]) : 0;
+        }
+        CA(upload(P->mem, &P->d_boxes, boxes.data(), boxes.size()), "slab boxes");
+        P->nboxes = (int)boxes.size();
+        P->nslab_blocks = nblk;
+        CA(P->mem.alloc(&P->d_err, 1), "error word");
+        if (P->bulk_on) {
+            CA(upload(P->mem, &P->d_bulk, blk.data(), blk.size()), "work table");
+            P->nbulk = (int)blk.size();
+            void *fn = nullptr;
+            cudaDriverEntryPointQueryResult q;
+            CA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q), "driver entry point");
+            if (!fn || q != cudaDriverEntryPointSuccess) return bail(cudaErrorNotSupported, "cuTensorMapEncodeTiled");
+            for (int sset = 0; sset < 2; sset++)
+                if (bulk_make_maps(fn, d, P->fields[sset], cls, d.cpitch, &P->bmaps[sset]) != 0)
+                    return bail(cudaErrorInvalidValue, "tensor map encoding");
+            CA(bulk_configure(d.nclasses), "bulk kernel shared memory");
+        }
     }
     P->step_bytes = bytes;
     CA(cudaDeviceSynchronize(), "plan set-up");
@@ -478,6 +602,9 @@ int fdtd_sync(fdtd_plan *P)
     if (!P) return fail(FDTD_E_INVALID, "plan is NULL");
     CK(cudaSetDevice(P->device));
     CK(cudaStreamSynchronize(P->stream));
+    int err = 0;
+    CK(cudaMemcpy(&err, P->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail(FDTD_E_TIMEOUT, "a bounded wait of the bulk kernel expired");
     return FDTD_OK;
 }
 
@@ -615,11 +742,11 @@ int fdtd_step_timed(fdtd_plan *P, int nsteps, double *fused_ms, int *fused_launc
         DevAux a = P->aux;
         a.fields = P->d_fieldptrs[in];
         launch_aux_step(a, P->stream);
-        DevPlan d = plan_for(P, in);
+        if (P->tsf_cells) launch_tsf_faces(P->dp, P->tsf_cells, P->stream);
         CK(cudaEventRecord(ev[2 * s], P->stream));
-        cudaError_t e = launch_fused_step(d, P->ichunk, P->hp.has_ade, P->hp.maxpoles, P->stream);
+        int rc = launch_fused(P, in, P->stream);
         CK(cudaEventRecord(ev[2 * s + 1], P->stream));
-        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("fused step launch: ") + cudaGetErrorString(e));
+        if (rc != FDTD_OK) return rc;
         if (P->nfff) {
             DevNfff n = P->nf;
             n.e = P->d_efieldptrs[1 - in];
@@ -639,6 +766,66 @@ int fdtd_step_timed(fdtd_plan *P, int nsteps, double *fused_ms, int *fused_launc
     for (auto &e : ev) cudaEventDestroy(e);
     if (fused_ms) *fused_ms = tot;
     if (fused_launches) *fused_launches = nsteps;
+    return FDTD_OK;
+}
+
+int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
+{
+    if (!P || nsteps < 1 || !out) return fail(FDTD_E_INVALID, "bad argument");
+    CK(cudaSetDevice(P->device));
+    const int NE = 6;
+    std::vector<cudaEvent_t> ev((size_t)NE * nsteps);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    cudaStream_t st = P->stream;
+    for (int s = 0; s < nsteps; s++) {
+        cudaEvent_t *E = &ev[(size_t)NE * s];
+        const int in = P->cur;
+        DevAux a = P->aux;
+        a.fields = P->d_fieldptrs[in];
+        CK(cudaEventRecord(E[0], st));
+        launch_aux_step(a, st);
+        if (P->tsf_cells) launch_tsf_faces(P->dp, P->tsf_cells, st);
+        CK(cudaEventRecord(E[1], st));
+        DevPlan d = plan_for(P, in);
+        if (P->bulk_on) {
+            cudaError_t e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, st);
+            if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
+        }
+        CK(cudaEventRecord(E[2], st));
+        cudaError_t e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, st);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
+        CK(cudaEventRecord(E[3], st));
+        if (P->nfff) {
+            DevNfff n = P->nf;
+            n.e = P->d_efieldptrs[1 - in];
+            launch_nfff_accumulate(n, st);
+        }
+        CK(cudaEventRecord(E[4], st));
+        P->cur = 1 - in;
+        P->host_step++;
+    }
+    final_probes(P, st);
+    CK(cudaStreamSynchronize(st));
+    double aux = 0, bulk = 0, slab = 0, nf = 0, tot = 0;
+    for (int s = 0; s < nsteps; s++) {
+        cudaEvent_t *E = &ev[(size_t)NE * s];
+        float t01, t12, t23, t34, t04;
+        CK(cudaEventElapsedTime(&t01, E[0], E[1]));
+        CK(cudaEventElapsedTime(&t12, E[1], E[2]));
+        CK(cudaEventElapsedTime(&t23, E[2], E[3]));
+        CK(cudaEventElapsedTime(&t34, E[3], E[4]));
+        CK(cudaEventElapsedTime(&t04, E[0], E[4]));
+        aux += t01; bulk += t12; slab += t23; nf += t34; tot += t04;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    out[0] = bulk;
+    out[1] = P->bulk_bytes;
+    out[2] = slab;
+    out[3] = P->slab_bytes;
+    out[4] = aux;
+    out[5] = nf;
+    out[6] = tot;
+    out[7] = 1 + (P->tsf_cells ? 1 : 0) + (P->bulk_on ? 1 : 0) + 2 + (P->nfff ? 1 : 0);
     return FDTD_OK;
 }
 

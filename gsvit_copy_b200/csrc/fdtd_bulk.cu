@@ -1,0 +1,332 @@
+// fdtd_bulk.cu -- TMA-staged fused step for the bulk of the grid.
+//
+// The bulk region is every cell outside the CPML slabs (their H/E updates,
+// psi recursions and zeroed planes are done by the general kernel).  Inside
+// it a step is: ystep_h (yee.c:146-265) + TSF H (source.c:1464-1672), then
+// ystep_e with the ADE branch and the PEC rule (yee.c:530-1247) + TSF E
+// (source.c:547-771).  kappa is 1 everywhere here.
+//
+// A CTA owns 31 x 31 (j,k) cells of every plane of its i-chunk.  Its 8 warps
+// compute H on the 32 x 32 cells [j0-1, j0+31) x [k0-1, k0+31) -- the own
+// cells plus the row and column the E update needs from its neighbours --
+// with warp w on rows 4w..4w+3 and lane = column, then E on the own cells.
+// Thread 0 streams the planes through a 3-stage shared-memory ring with
+// cp.async.bulk.tensor (TMA) two planes ahead: E(p) box 36 x 33, H(p) box
+// 36 x 32 (floats, k innermost) and the class byte box 48 x 32, completion
+// on one mbarrier per stage.  Every wait is bounded; a CTA that gives up sets
+// the error word and returns after draining its copies.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "fdtd_bulk.cuh"
+#include "fdtd_device.cuh"
+
+namespace {
+
+constexpr int BROWS_E = 33, BROWS_H = 32, BW = 36, BWC = 48;
+constexpr int S = 3;
+constexpr int EBOX = BROWS_E * BW * 4;                     // 4752 B
+constexpr int EBOX_PAD = (EBOX + 127) / 128 * 128;         // 4864 B
+constexpr int HBOX = BROWS_H * BW * 4;                     // 4608 B
+constexpr int CBOX = BROWS_H * BWC;                        // 1536 B
+constexpr int STAGE = 3 * EBOX_PAD + 3 * HBOX + CBOX;      // 29952 B
+constexpr uint32_t STAGE_TX = 3 * EBOX + 3 * HBOX + CBOX;  // bytes the TMA delivers per stage
+constexpr int NTH = 256;
+constexpr long long WAIT_LIMIT = 1ll << 22;
+
+static_assert(EBOX_PAD % 128 == 0 && HBOX % 128 == 0 && CBOX % 128 == 0, "TMA boxes must stay 128-B aligned");
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void bar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool bar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait: false when the phase did not complete within the limit
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t parity)
+{
+    for (long long it = 0; it < WAIT_LIMIT; it++)
+        if (bar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ float *ebox(unsigned char *st, int c) { return reinterpret_cast<float *>(st + c * EBOX_PAD); }
+__device__ __forceinline__ float *hbox(unsigned char *st, int c)
+{
+    return reinterpret_cast<float *>(st + 3 * EBOX_PAD + c * HBOX);
+}
+__device__ __forceinline__ unsigned char *cbox(unsigned char *st) { return st + 3 * EBOX_PAD + 3 * HBOX; }
+
+// ------------------------------------------------------------- kernel
+
+template <bool ADE, int NPOLES>
+__global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ BulkMaps M,
+                                                      const BulkItem *items, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *stages = smem;
+    float4 *scls = reinterpret_cast<float4 *>(smem + S * STAGE);
+    float *hrow = reinterpret_cast<float *>(smem + S * STAGE + P.nclasses * 64);        // [8][2][32]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S * STAGE + P.nclasses * 64 + 8 * 2 * 32 * 4);
+
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const BulkItem it = items[blockIdx.x];
+    const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
+    const int xr = P.xr, yr = P.yr, zr = P.zr;
+    const int64_t si = P.si, sj = P.sj;
+    const int ka = (k0 - 1) & ~3, ka8 = (k0 - 1) & ~15;      // box origins (16-byte aligned x)
+    const int off = (k0 - 1) - ka, off8 = (k0 - 1) - ka8;
+    const int p0 = (ib > 0) ? ib - 1 : ib;                    // first plane (prologue H when ib > 0)
+    const int plast = min(ie, xr - 1);                        // last plane whose data is needed
+
+    for (int q = tid; q < P.nclasses * 4; q += NTH) scls[q] = reinterpret_cast<const float4 *>(P.classes)[q];
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) bar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    auto issue = [&](int p) {   // thread 0: all boxes of plane p into stage (p - p0) % S
+        const int s = (p - p0) % S;
+        unsigned char *st = stages + s * STAGE;
+        bar_expect_tx(&bars[s], STAGE_TX);
+        for (int c = 0; c < 3; c++) tma_load3(ebox(st, c), &M.e[c], ka, j0 - 1, p, &bars[s]);
+        for (int c = 0; c < 3; c++) tma_load3(hbox(st, c), &M.h[c], ka, j0 - 1, p, &bars[s]);
+        tma_load3(cbox(st), &M.cls, ka8, j0 - 1, p, &bars[s]);
+    };
+    if (tid == 0)
+        for (int p = p0; p <= plast && p < p0 + S; p++) issue(p);
+
+    // this thread's cells: rows rr = 4w + r (row 0 = j0-1), column lane (k = k0-1+lane)
+    const int k = k0 - 1 + lane;
+    const int ce = off + lane, ce8 = off8 + lane;
+    const bool kown = lane >= 1 && k < it.khi;
+    int jr[4];
+    bool own[4];
+    for (int r = 0; r < 4; r++) {
+        jr[r] = j0 - 1 + 4 * w + r;
+        own[r] = kown && (4 * w + r) >= 1 && jr[r] < it.jhi;
+    }
+    // TSF face membership by axis (source.c box faces)
+    const bool tsf = P.tsf_on != 0;
+
+    float e[4][3], h[4][3], him[4][2];
+    for (int r = 0; r < 4; r++) {
+        him[r][0] = him[r][1] = 0.f;
+        for (int a = 0; a < 3; a++) { e[r][a] = 0.f; h[r][a] = 0.f; }
+    }
+    bool failed = false;
+    for (int i = p0; i <= plast && i < ie; i++) {
+        const int s = (i - p0) % S;
+        const uint32_t par = (uint32_t)(((i - p0) / S) & 1);
+        const bool have_next = (i + 1 <= plast);
+        const int s1 = (i + 1 - p0) % S;
+        const uint32_t par1 = (uint32_t)(((i + 1 - p0) / S) & 1);
+        bool ok = bar_wait(&bars[s], par);
+        if (have_next) ok = ok && bar_wait(&bars[s1], par1);
+        if (__syncthreads_or(!ok)) { failed = true; break; }
+        unsigned char *st = stages + s * STAGE, *st1 = stages + s1 * STAGE;
+        const float *EX = ebox(st, 0), *EY = ebox(st, 1), *EZ = ebox(st, 2);
+        const float *HX = hbox(st, 0), *HY = hbox(st, 1), *HZ = hbox(st, 2);
+        const unsigned char *CL = cbox(st);
+        const float *EY1 = ebox(st1, 1), *EZ1 = ebox(st1, 2);
+        const bool prologue = (i < ib);
+        const bool il = (i == xr - 1);
+        // ---- H phase: 4 cells per thread
+        for (int r = 0; r < 4; r++) {
+            const int rr = 4 * w + r, j = jr[r];
+            const int b = rr * BW + ce;
+            const float ex = EX[b], ey = EY[b], ez = EZ[b];
+            e[r][0] = ex; e[r][1] = ey; e[r][2] = ez;
+            const float exj = EX[b + BW], ezj = EZ[b + BW];
+            const float exk = EX[b + 1], eyk = EY[b + 1];
+            const float eyi = have_next ? EY1[b] : 0.f, ezi = have_next ? EZ1[b] : 0.f;
+            const int cl = CL[rr * BWC + ce8];
+            const float4 hc = scls[cl * 4 + 2];
+            float hx = HX[b], hy = HY[b], hz = HZ[b];
+            const bool jl = (j == yr - 1), kl = (k == zr - 1);
+            if (!(jl || kl)) hx = hc.x * hx + hc.y * ((eyk - ey) - (ezj - ez));
+            if (!(il || kl)) hy = hc.x * hy + hc.y * ((ezi - ez) - (exk - ex));
+            if (!(il || jl)) hz = hc.x * hz + hc.y * ((exj - ex) - (eyi - ey));
+            if (tsf) tsf_add_h(P, i, j, k, hx, hy, hz);
+            h[r][0] = hx; h[r][1] = hy; h[r][2] = hz;
+            if (!prologue && own[r]) {
+                const int64_t c = (int64_t)i * si + (int64_t)j * sj + k;
+                P.fout[3][c] = hx;
+                P.fout[4][c] = hy;
+                P.fout[5][c] = hz;
+            }
+        }
+        if (!prologue) {
+            hrow[(w * 2 + 0) * 32 + lane] = h[3][2];
+            hrow[(w * 2 + 1) * 32 + lane] = h[3][0];
+        }
+        __syncthreads();
+        // ---- E phase on own cells
+        if (!prologue) {
+            float hyk[4], hxk[4];
+            for (int r = 0; r < 4; r++) {
+                hyk[r] = __shfl_up_sync(0xffffffffu, h[r][1], 1);
+                hxk[r] = __shfl_up_sync(0xffffffffu, h[r][0], 1);
+            }
+            for (int r = 0; r < 4; r++) {
+                if (!own[r]) continue;
+                const int rr = 4 * w + r, j = jr[r];
+                const float hzj = r ? h[r - 1][2] : hrow[((w - 1) * 2 + 0) * 32 + lane];
+                const float hxj = r ? h[r - 1][0] : hrow[((w - 1) * 2 + 1) * 32 + lane];
+                const int cl = CL[rr * BWC + ce8];
+                const float4 c0 = scls[cl * 4 + 0], c1 = scls[cl * 4 + 1];
+                const unsigned fl = __float_as_uint(c0.w);
+                const float curlx = (h[r][2] - hzj) - (h[r][1] - hyk[r]);
+                const float curly = (h[r][0] - hxk[r]) - (h[r][2] - him[r][1]);
+                const float curlz = (h[r][1] - him[r][0]) - (h[r][0] - hxj);
+                const bool gx = (j > 0 && k > 0), gy = (i > 0 && k > 0), gz = (i > 0 && j > 0);
+                float nx = e[r][0], ny = e[r][1], nz = e[r][2];
+                const int64_t c = (int64_t)i * si + (int64_t)j * sj + k;
+                if (ADE && (fl & CF_ADE_BRANCH)) {
+                    // ADE branch (yee.c:914-1108) without CPML: only the owned components
+                    const DevAde &A = P.ade[__float_as_int(scls[cl * 4 + 2].z)];
+                    const float curl[3] = {curlx, curly, curlz};
+                    const bool gd[3] = {gx, gy, gz};
+                    const unsigned cm[3] = {CF_ADE_X, CF_ADE_Y, CF_ADE_Z};
+                    float ne[3] = {nx, ny, nz};
+                    for (int a = 0; a < 3; a++) {
+                        if (!(fl & cm[a])) continue;
+                        const float eo = e[r][a];
+                        const float dp = P.dp[a][c], dpp = P.dpp[a][c], ep = P.ep[a][c];
+                        float p[2] = {0.f, 0.f}, pp[2] = {0.f, 0.f};
+                        for (int n = 0; n < NPOLES; n++) { p[n] = P.p_[a][n][c]; pp[n] = P.pp_[a][n][c]; }
+                        float v = eo;
+                        if (gd[a]) {
+                            v = A.c0dx * curl[a] + A.c1 * (-A.a0 * dpp + A.one_m_a1 * dp);
+                            for (int n = 0; n < NPOLES; n++) v += A.c1 * (-A.bp0[n] * pp[n] + A.one_m_bp1[n] * p[n]);
+                            v += A.c2 * ep + A.c3 * eo;
+                        }
+                        ne[a] = v;
+                        P.dp[a][c] = A.a0 * dpp + A.a1 * dp + A.a2 * (ep + 2.f * eo + v);
+                        for (int n = 0; n < NPOLES; n++) {
+                            P.p_[a][n][c] = A.bp0[n] * pp[n] + A.bp1[n] * p[n] + A.bp2[n] * ep + A.bp3[n] * eo + A.bp4[n] * v;
+                            P.pp_[a][n][c] = p[n];
+                        }
+                        P.ep[a][c] = eo;
+                        P.dpp[a][c] = dp;
+                    }
+                    if (gx && !(fl & CF_ADE_X)) ne[0] = c0.x * nx + c1.x * curlx;
+                    if (gy && !(fl & CF_ADE_Y)) ne[1] = c0.y * ny + c1.y * curly;
+                    if (gz && !(fl & CF_ADE_Z)) ne[2] = c0.z * nz + c1.z * curlz;
+                    nx = ne[0]; ny = ne[1]; nz = ne[2];
+                } else {
+                    if (gx) nx = c0.x * nx + c1.x * curlx;
+                    if (gy) ny = c0.y * ny + c1.y * curly;
+                    if (gz) nz = c0.z * nz + c1.z * curlz;
+                }
+                if (fl & CF_PEC_X) nx = 0.f;
+                if (fl & CF_PEC_Y) ny = 0.f;
+                if (fl & CF_PEC_Z) nz = 0.f;
+                if (tsf) tsf_add_e(P, i, j, k, nx, ny, nz);
+                P.fout[0][c] = nx;
+                P.fout[1][c] = ny;
+                P.fout[2][c] = nz;
+            }
+        }
+        for (int r = 0; r < 4; r++) { him[r][0] = h[r][1]; him[r][1] = h[r][2]; }
+        __syncthreads();   // stage s is free
+        if (tid == 0 && i + S <= plast) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(i + S);
+        }
+    }
+    if (failed) {
+        if (tid == 0) {
+            atomicExch(err, 1);
+            for (int s = 0; s < S; s++)     // drain: one more bounded wait per stage
+                bar_wait(&bars[s], 0);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+size_t bulk_smem_bytes(int nclasses) { return (size_t)S * STAGE + (size_t)nclasses * 64 + 8 * 2 * 32 * 4 + S * 8; }
+
+cudaError_t bulk_configure(int nclasses)
+{
+    size_t smem = bulk_smem_bytes(nclasses);
+    cudaError_t e;
+    e = cudaFuncSetAttribute(bulk_kernel<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(bulk_kernel<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(bulk_kernel<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t launch_bulk(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade,
+                        int npoles, cudaStream_t st)
+{
+    if (nitems <= 0) return cudaSuccess;
+    size_t smem = bulk_smem_bytes(p.nclasses);
+    if (!ade)
+        bulk_kernel<false, 0><<<nitems, NTH, smem, st>>>(p, m, items, err);
+    else if (npoles == 0)
+        bulk_kernel<true, 0><<<nitems, NTH, smem, st>>>(p, m, items, err);
+    else
+        bulk_kernel<true, 2><<<nitems, NTH, smem, st>>>(p, m, items, err);
+    return cudaGetLastError();
+}
+
+// Tensor maps of one field set: 3D (k, j, i) float boxes of 36 x 33 (E) and
+// 36 x 32 (H); class bytes 48 x 32 over a row pitch padded to 16 bytes.
+int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, BulkMaps *out)
+{
+    auto enc = reinterpret_cast<CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                             const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                             CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                             CUtensorMapFloatOOBfill)>(encode_fn);
+    const cuuint64_t dims[3] = {(cuuint64_t)p.zr, (cuuint64_t)p.yr, (cuuint64_t)p.xr};
+    const cuuint64_t strides[2] = {(cuuint64_t)p.zr * 4, (cuuint64_t)p.zr * 4 * (cuuint64_t)p.yr};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const cuuint32_t boxe[3] = {BW, BROWS_E, 1}, boxh[3] = {BW, BROWS_H, 1}, boxc[3] = {BWC, BROWS_H, 1};
+    for (int c = 0; c < 3; c++) {
+        if (enc(&out->e[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, f[c], dims, strides, boxe, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return -1;
+        if (enc(&out->h[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, f[3 + c], dims, strides, boxh, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return -1;
+    }
+    const cuuint64_t cdims[3] = {(cuuint64_t)p.zr, (cuuint64_t)p.yr, (cuuint64_t)p.xr};
+    const cuuint64_t cstr[2] = {(cuuint64_t)cls_pitch, (cuuint64_t)cls_pitch * (cuuint64_t)p.yr};
+    if (enc(&out->cls, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void *)cls, cdims, cstr, boxc, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return -1;
+    return 0;
+}

@@ -1,0 +1,27 @@
+// fdtd_bulk.cuh -- TMA-staged bulk kernel (fdtd_bulk.cu).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fdtd_internal.h"
+
+// tensor maps of the input field set and of the class map
+struct BulkMaps {
+    CUtensorMap e[3];
+    CUtensorMap h[3];
+    CUtensorMap cls;
+};
+
+// one CTA: own cells [j0, min(j0+31, jhi)) x [k0, min(k0+31, khi)) of planes [ib, ie)
+struct BulkItem {
+    int j0, k0, ib, ie, jhi, khi, pad0, pad1;
+};
+
+#define BULK_TILE 31
+
+size_t bulk_smem_bytes(int nclasses);
+cudaError_t bulk_configure(int nclasses);
+cudaError_t launch_bulk(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade,
+                        int npoles, cudaStream_t st);
+int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, BulkMaps *out);

@@ -14,6 +14,7 @@
 //               grid arrays touched only by dispersive cells.
 #pragma once
 #include <stdint.h>
+#include <vector_types.h>
 
 #define FDTD_MAX_CLASSES 256
 #define FDTD_MAX_ADE 8
@@ -27,15 +28,20 @@
 #define CF_PEC_Y      0x020u
 #define CF_PEC_Z      0x040u
 
-struct DevClass {
-    float ca[3];    // ordinary update E = ca*E + cb*curl (get_cabs, yee.c:1397-1493)
-    float cb[3];    // same cb, also used by the boundary_estep CPML corrections
-    float cba[3];   // CPML cb inside the ADE branch (yee.c:950-1057), from the ADE material
-    float da, db;   // H update (yee.c:219-243) and CPML-H db (get_db, yee.c:1620-1647)
-    float tsfe;     // (dt/dx)/epsilon(cell) of the TSF-E correction (source.c:548,566)
+struct alignas(16) DevClass {
+    // float4 0: ordinary update E = ca*E + cb*curl (get_cabs, yee.c:1397-1493)
+    float ca[3];
     uint32_t flags;
+    // float4 1: cb, also used by the boundary_estep CPML corrections; TSF-E factor
+    float cb[3];
+    float tsfe;     // (dt/dx)/epsilon(cell) of the TSF-E correction (source.c:548,566)
+    // float4 2: H update (yee.c:219-243) and CPML-H db (get_db, yee.c:1620-1647)
+    float da, db;
     int32_t ade;    // ADE coefficient set
-    float pad[2];
+    float pad0;
+    // float4 3: CPML cb inside the ADE branch (yee.c:950-1057), from the ADE material
+    float cba[3];
+    float pad1;
 };
 
 struct DevAde {      // calculate_ade_a/bp/c (plan.c:2737-2763), rounded to float
@@ -53,7 +59,8 @@ struct DevPlan {
     // fields: [0..2] = E x,y,z, [3..5] = H x,y,z
     const float *fin[6];
     float *fout[6];
-    const uint8_t *cls;
+    const uint8_t *cls;             // class map, rows padded to cpitch bytes
+    int cpitch;
     const DevClass *classes;
     int nclasses;
     // ADE
@@ -73,6 +80,8 @@ struct DevPlan {
     int t0[3], t1[3];               // box corners i0 j0 k0 / in jn kn
     int tskip[6];
     const uint8_t *tmap[6];         // per face cell: bit0 apply (mat_too_close_check), bit1 PEC at the face cell
+    float2 *tcor_h[6], *tcor_e[6];  // this step's TSF corrections per face cell (two components each)
+    int tnb[6];                     // inner extent of the face tables
     double corr, hcor;
     double tax, tay, taz;           // propagation direction sin(t)cos(p), sin(t)sin(p), cos(t)
     int trx_origin, try_origin, trz_origin;  // dcomp corner (source.c:54-107), or flags for the rx=0 quirk

@@ -1,7 +1,8 @@
 // fdtd_kernels.cu -- sm_100a kernels of one GSvit FDTD time step.
 //
-// One step = aux_step (1D TSF grid, 1 CTA) -> fused_step (H and E of the
-// whole grid in one pass) -> nfff_accumulate (running DFT on the NFFF box).
+// One step = aux_step (1D TSF grid, 1 CTA) -> bulk kernel (fdtd_bulk.cu,
+// fused H+E over the slab-free box) -> slab_h -> slab_e (the CPML slabs and
+// grid edges, one thread per cell) -> nfff_accumulate (running DFT).
 //
 // fused_step marches along i (the slowest axis of the reference layout
 // data[i][j][k]) over a (j,k) tile.  For plane i it first forms H^{n+1/2}(i)
@@ -18,184 +19,31 @@
 // byte through HBM (49 B); halo reads are served by L1/L2.
 #include <cuda_runtime.h>
 
+#include "fdtd_device.cuh"
 #include "fdtd_kernels.cuh"
 
 namespace {
 
 enum { X0 = 0, XN = 1, Y0 = 2, YN = 3, Z0 = 4, ZN = 5 };
 
-// ---------------------------------------------------------------- TSF (FP64)
+// ------------------------------------------------------------ cell updates
 
-// dcomp of source.c:54-107 with the reference call (i0=0, i1=xres, ...): the
-// corner offsets and the rx = 0 branch are resolved on the host.
-__device__ __forceinline__ double dcomp(const DevPlan &P, int i, int j, int k)
+
+#define FULLMASK 0xffffffffu
+
+// CPML psi_H update and corrections (boundary.c:347-519, face order x0 y0 z0
+// xn yn zn), TSF H corrections (source.c:1476-1672) and the outer H planes
+// zeroed by boundary_hstep (boundary.c:418-420, 455-457, 490-492), applied to
+// H after ystep_h.  `owner` cells write their psi_H.
+__device__ __noinline__ float3 h_special(const DevPlan &P, int i, int j, int k, bool owner, float db, float dey_i,
+                                         float dez_i, float dex_j, float dez_j, float dex_k, float dey_k, float3 hin)
 {
-    double rx = P.trx_zero ? 0.0 : (double)(i - P.trx_origin);
-    double ry = (double)(j - P.try_origin);
-    double rz = (double)(k - P.trz_origin);
-    double s = __dadd_rn(__dadd_rn(__dmul_rn(P.tax, rx), __dmul_rn(P.tay, ry)), __dmul_rn(P.taz, rz));
-    return __dmul_rn(P.corr, __dadd_rn(10.0, s));
-}
-
-// sv_dline_get_dval, dline.c:89-111 (4-point cubic, linear near the ends)
-__device__ __forceinline__ double dval(const double *data, int res, double x)
-{
-    double fl = floor(x);
-    int l = (int)fl;
-    double a = x - fl;
-    if (x >= 1 && x < (res - 1)) {
-        double w1 = a + 1, w2 = a, w3 = 1 - a, w4 = 2 - a;
-        w1 = 4 - 8 * w1 + 5 * w1 * w1 - w1 * w1 * w1;
-        w2 = 1 - 2 * w2 * w2 + w2 * w2 * w2;
-        w3 = 1 - 2 * w3 * w3 + w3 * w3 * w3;
-        w4 = 4 - 8 * w4 + 5 * w4 * w4 - w4 * w4 * w4;
-        return w1 * data[l - 1] + w2 * data[l] + w3 * data[l + 1] + w4 * data[l + 2];
-    } else if ((x < 1 && x >= 0) || (x >= (res - 1) && x < res))
-        return (1 - a) * data[l] + a * data[l + 1];
-    return 0;
-}
-
-__device__ __forceinline__ uint8_t tflag(const DevPlan &P, int f, int a, int b)
-{
-    int nb = (f < 4) ? (P.t1[2] - P.t0[2] + 1) : (P.t1[1] - P.t0[1] + 1);
-    return P.tmap[f][a * nb + b];
-}
-
-// TSF corrections of the H cell (i,j,k), source.c:1476-1672
-__device__ void tsf_h(const DevPlan &P, int i, int j, int k, float &hx, float &hy, float &hz)
-{
-    const int i0 = P.t0[0], j0 = P.t0[1], k0 = P.t0[2], in = P.t1[0], jn = P.t1[1], kn = P.t1[2];
-    const double hc = P.hcor;
-    // i faces: j in [j0,jn], k in [k0,kn]
-    if (j >= j0 && j <= jn && k >= k0 && k <= kn) {
-        if (i == i0 - 1 && (tflag(P, X0, j - j0, k - k0) & 1)) {
-            double ve = dval(P.aux_e, P.jres, dcomp(P, i0, j, k));
-            if (k < kn) hy -= (float)(hc * (ve * P.gez));
-            if (j < jn) hz += (float)(hc * (ve * P.gey));
-        }
-        if (i == in && (tflag(P, XN, j - j0, k - k0) & 1)) {
-            double ve = dval(P.aux_e, P.jres, dcomp(P, in, j, k));
-            if (k < kn) hy += (float)(hc * (ve * P.gez));
-            if (j < jn) hz -= (float)(hc * (ve * P.gey));
-        }
-    }
-    if (i >= i0 && i <= in && k >= k0 && k <= kn) {
-        if (j == j0 - 1 && (tflag(P, Y0, i - i0, k - k0) & 1)) {
-            double ve = dval(P.aux_e, P.jres, dcomp(P, i, j0, k));
-            if (k < kn) hx += (float)(hc * (ve * P.gez));
-            if (i < in) hz -= (float)(hc * (ve * P.gex));
-        }
-        if (j == jn && (tflag(P, YN, i - i0, k - k0) & 1)) {
-            double ve = dval(P.aux_e, P.jres, dcomp(P, i, jn, k));
-            if (k < kn) hx -= (float)(hc * (ve * P.gez));
-            if (i < in) hz += (float)(hc * (ve * P.gex));
-        }
-    }
-    if (i >= i0 && i <= in && j >= j0 && j <= jn) {
-        if (k == k0 - 1) {
-            uint8_t fl = tflag(P, Z0, i - i0, j - j0);
-            if (fl & 1) {
-                double ve = dval(P.aux_e, P.jres, dcomp(P, i, j, k0));
-                if (j < jn && !(fl & 2)) hx -= (float)(hc * (ve * P.gey));
-                if (i < in && !(fl & 2)) hy += (float)(hc * (ve * P.gex));
-            }
-        }
-        if (k == kn && (tflag(P, ZN, i - i0, j - j0) & 1)) {
-            double ve = dval(P.aux_e, P.jres, dcomp(P, i, j, kn));
-            if (j < jn) hx += (float)(hc * (ve * P.gey));
-            if (i < in) hy -= (float)(hc * (ve * P.gex));
-        }
-    }
-}
-
-// TSF corrections of the E cell (i,j,k), source.c:547-771
-__device__ void tsf_e(const DevPlan &P, int i, int j, int k, float tsfe, float &ex, float &ey, float &ez)
-{
-    const int i0 = P.t0[0], j0 = P.t0[1], k0 = P.t0[2], in = P.t1[0], jn = P.t1[1], kn = P.t1[2];
-    const double ce = (double)tsfe;
-    if (j >= j0 && j <= jn && k >= k0 && k <= kn) {
-        if (i == i0 && (tflag(P, X0, j - j0, k - k0) & 1)) {
-            double vh = dval(P.aux_h, P.jres, dcomp(P, i0 - 1, j, k));
-            if (j < jn) ey += (float)(ce * (vh * P.ghz));
-            if (k < kn) ez -= (float)(ce * (vh * P.ghy));
-        }
-        if (i == in && (tflag(P, XN, j - j0, k - k0) & 1)) {
-            double vh = dval(P.aux_h, P.jres, dcomp(P, in, j, k));
-            if (j < jn) ey -= (float)(ce * (vh * P.ghz));
-            if (k < kn) ez += (float)(ce * (vh * P.ghy));
-        }
-    }
-    if (i >= i0 && i <= in && k >= k0 && k <= kn) {
-        if (j == j0 && (tflag(P, Y0, i - i0, k - k0) & 1)) {
-            double vh = dval(P.aux_h, P.jres, dcomp(P, i, j0 - 1, k));
-            if (i < in) ex -= (float)(ce * (vh * P.ghz));
-            if (k < kn) ez += (float)(ce * (vh * P.ghx));
-        }
-        if (j == jn && (tflag(P, YN, i - i0, k - k0) & 1)) {
-            double vh = dval(P.aux_h, P.jres, dcomp(P, i, jn, k));
-            if (i < in) ex += (float)(ce * (vh * P.ghz));
-            if (k < kn) ez -= (float)(ce * (vh * P.ghx));
-        }
-    }
-    if (i >= i0 && i <= in && j >= j0 && j <= jn) {
-        if (k == k0) {
-            uint8_t fl = tflag(P, Z0, i - i0, j - j0);
-            if (fl & 1) {
-                double vh = dval(P.aux_h, P.jres, dcomp(P, i, j, k0 - 1));
-                if (i < in && !(fl & 2)) ex += (float)(ce * (vh * P.ghy));
-                if (j < jn && !(fl & 2)) ey -= (float)(ce * (vh * P.ghx));
-            }
-        }
-        if (k == kn && (tflag(P, ZN, i - i0, j - j0) & 1)) {
-            double vh = dval(P.aux_h, P.jres, dcomp(P, i, j, kn));
-            if (i < in) ex -= (float)(ce * (vh * P.ghy));
-            if (j < jn) ey += (float)(ce * (vh * P.ghx));
-        }
-    }
-}
-
-// ------------------------------------------------------------------- H cell
-
-struct EOwn {           // E^n at the cell and its +1 neighbours, read once
-    float ex, ey, ez;
-    float ey_k1, ex_k1, ez_j1, ex_j1, ez_i1, ey_i1;
-};
-
-__device__ __forceinline__ void load_e(const DevPlan &P, int64_t c, int i, int j, int k, EOwn &e)
-{
-    const float *EX = P.fin[0], *EY = P.fin[1], *EZ = P.fin[2];
-    e.ex = __ldg(EX + c); e.ey = __ldg(EY + c); e.ez = __ldg(EZ + c);
-    const bool kl = (k == P.zr - 1), jl = (j == P.yr - 1), il = (i == P.xr - 1);
-    e.ey_k1 = kl ? 0.f : __ldg(EY + c + 1);
-    e.ex_k1 = kl ? 0.f : __ldg(EX + c + 1);
-    e.ez_j1 = jl ? 0.f : __ldg(EZ + c + P.sj);
-    e.ex_j1 = jl ? 0.f : __ldg(EX + c + P.sj);
-    e.ez_i1 = il ? 0.f : __ldg(EZ + c + P.si);
-    e.ey_i1 = il ? 0.f : __ldg(EY + c + P.si);
-}
-
-// H^{n+1/2} of cell (i,j,k): ystep_h + TSF + CPML (+ the zeroed outer planes).
-// `owner` cells also write their psi_H.
-__device__ void h_cell(const DevPlan &P, const DevClass *cls, int i, int j, int k, bool owner, const EOwn &e,
-                       float h[3])
-{
-    const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
-    const DevClass &C = cls[__ldg(P.cls + c)];
-    float hx = __ldg(P.fin[3] + c), hy = __ldg(P.fin[4] + c), hz = __ldg(P.fin[5] + c);
+    float hx = hin.x, hy = hin.y, hz = hin.z;
     const int xr = P.xr, yr = P.yr, zr = P.zr;
     const bool il = (i == xr - 1), jl = (j == yr - 1), kl = (k == zr - 1);
-    const float ikx = __ldg(P.ikh[0] + i), iky = __ldg(P.ikh[1] + j), ikz = __ldg(P.ikh[2] + k);
-    const float dey_i = e.ey_i1 - e.ey, dez_i = e.ez_i1 - e.ez;   // E differences along x
-    const float dex_j = e.ex_j1 - e.ex, dez_j = e.ez_j1 - e.ez;   // along y
-    const float dex_k = e.ex_k1 - e.ex, dey_k = e.ey_k1 - e.ey;   // along z
-    // ystep_h, yee.c:246-256
-    if (!(jl || kl)) hx = C.da * hx + C.db * (dey_k * ikz - dez_j * iky);
-    if (!(il || kl)) hy = C.da * hy + C.db * (dez_i * ikx - dex_k * ikz);
-    if (!(il || jl)) hz = C.da * hz + C.db * (dex_j * iky - dey_i * ikx);
-    if (P.tsf_on) tsf_h(P, i, j, k, hx, hy, hz);
-    // CPML H, boundary.c:347-519; face order x0 y0 z0 xn yn zn
+    if (P.tsf_on) tsf_add_h(P, i, j, k, hx, hy, hz);
     const bool jin = (j >= 1 && j < yr - 1), kin = (k >= 1 && k < zr - 1), iin = (i >= 1 && i < xr - 1);
-    const float dbdx = C.db * P.dx;
+    const float dbdx = db * P.dx;
     const float idx_ = 1.0f / P.dx;
     if (P.cp_on[X0] && i < P.cp_d[X0] - 1 && jin && kin) {
         const int64_t q = ((int64_t)i * yr + j) * zr + k;
@@ -263,36 +111,60 @@ __device__ void h_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
             if (owner) { P.psih_out[ZN][1][q] = pyz; P.psih_out[ZN][0][q] = pxz; }
         }
     }
-    // outer H planes zeroed by boundary_hstep (boundary.c:418-420, 455-457, 490-492)
     if ((P.cp_on[XN] && il && jin && kin) || (P.cp_on[YN] && jl && iin && kin) || (P.cp_on[ZN] && kl && iin && jin))
         hx = hy = hz = 0.f;
-    h[0] = hx; h[1] = hy; h[2] = hz;
+    return make_float3(hx, hy, hz);
 }
 
-// ------------------------------------------------------------------- E cell
-
-template <bool ADE, int NPOLES>
-__device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int k, const EOwn &e, const float h[3],
-                       float hx_jm, float hz_jm, float hx_km, float hy_km, float hy_im, float hz_im)
+// H^{n+1/2}(i) at one cell from E^n and the six E differences (ystep_h,
+// yee.c:246-256, then h_special where the cell lies in a slab or on a face).
+__device__ __forceinline__ void h_update(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k,
+                                         bool special, bool owner, float dey_i, float dez_i, float dex_j, float dez_j,
+                                         float dex_k, float dey_k, float h[3])
 {
+    const float4 hc = scls[cls * 4 + 2];     // da, db
+    const bool il = (i == P.xr - 1), jl = (j == P.yr - 1), kl = (k == P.zr - 1);
+    float ikx = 1.f, iky = 1.f, ikz = 1.f;
+    if (special) { ikx = __ldg(P.ikh[0] + i); iky = __ldg(P.ikh[1] + j); ikz = __ldg(P.ikh[2] + k); }
+    if (!(jl || kl)) h[0] = hc.x * h[0] + hc.y * (dey_k * ikz - dez_j * iky);
+    if (!(il || kl)) h[1] = hc.x * h[1] + hc.y * (dez_i * ikx - dex_k * ikz);
+    if (!(il || jl)) h[2] = hc.x * h[2] + hc.y * (dex_j * iky - dey_i * ikx);
+    if (special) {
+        const float3 o = h_special(P, i, j, k, owner, hc.y, dey_i, dez_i, dex_j, dez_j, dex_k, dey_k,
+                                   make_float3(h[0], h[1], h[2]));
+        h[0] = o.x; h[1] = o.y; h[2] = o.z;
+    }
+}
+
+// E^{n+1}(i) of one cell on the general path: ADE branch with its CPML
+// (yee.c:914-1108), ordinary update (yee.c:1113-1128), PEC rule
+// (yee.c:1138-1237), boundary_estep zero planes, psi_E and corrections
+// (boundary.c:691-884) and TSF E (source.c:547-771).
+template <bool ADE, int NPOLES>
+__device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k,
+                                         float3 eo3, float3 h3, float hx_jm, float hz_jm, float hx_km, float hy_km,
+                                         float hy_im, float hz_im)
+{
+    const float eo[3] = {eo3.x, eo3.y, eo3.z};
+    const float h[3] = {h3.x, h3.y, h3.z};
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
-    const DevClass &C = cls[__ldg(P.cls + c)];
-    const unsigned fl = C.flags;
+    const float4 c0 = scls[cls * 4 + 0], c1 = scls[cls * 4 + 1], c2 = scls[cls * 4 + 2], c3 = scls[cls * 4 + 3];
+    const unsigned fl = __float_as_uint(c0.w);
+    const float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z}, cba[3] = {c3.x, c3.y, c3.z};
+    const int ade_set = __float_as_int(c2.z);
     const int xr = P.xr, yr = P.yr, zr = P.zr;
     const float ikx = __ldg(P.ike[0] + i), iky = __ldg(P.ike[1] + j), ikz = __ldg(P.ike[2] + k);
     const float hx = h[0], hy = h[1], hz = h[2];
     const bool gx = (j > 0 && k > 0), gy = (i > 0 && k > 0), gz = (i > 0 && j > 0);
-    // H differences along each axis (only formed where the neighbour exists)
     const float dhz_i = i > 0 ? hz - hz_im : 0.f, dhy_i = i > 0 ? hy - hy_im : 0.f;
     const float dhz_j = j > 0 ? hz - hz_jm : 0.f, dhx_j = j > 0 ? hx - hx_jm : 0.f;
     const float dhx_k = k > 0 ? hx - hx_km : 0.f, dhy_k = k > 0 ? hy - hy_km : 0.f;
     const float curlx = dhz_j * iky - dhy_k * ikz;
     const float curly = dhx_k * ikz - dhz_i * ikx;
     const float curlz = dhy_i * ikx - dhx_j * iky;
-    float nx = e.ex, ny = e.ey, nz = e.ez;
+    float nx = eo[0], ny = eo[1], nz = eo[2];
     const float idx_ = 1.0f / P.dx;
-    // CPML psi_E values carried from the ADE-branch update to boundary_estep
-    float px0[2], pxn[2], py0[2], pyn[2], pz0[2], pzn[2];
+    float px0[2] = {0, 0}, pxn[2] = {0, 0}, py0[2] = {0, 0}, pyn[2] = {0, 0}, pz0[2] = {0, 0}, pzn[2] = {0, 0};
     const bool inx0 = P.cp_on[X0] && i >= 1 && i < P.cp_d[X0];
     const bool iny0 = P.cp_on[Y0] && j >= 1 && j < P.cp_d[Y0];
     const bool inz0 = P.cp_on[Z0] && k >= 1 && k < P.cp_d[Z0];
@@ -310,12 +182,9 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
         if (inzn) { qzn = ((int64_t)i * yr + j) * P.cp_d[ZN] + (k - (zr - P.cp_d[ZN])); pzn[0] = P.psie[ZN][0][qzn]; pzn[1] = P.psie[ZN][1][qzn]; }
     }
     if (ADE && (fl & CF_ADE_BRANCH)) {
-        // ADE (Drude + critical points) branch, yee.c:914-1108
-        const DevAde &A = P.ade[C.ade];
-        const bool ax = (fl & CF_ADE_X) != 0, ay = (fl & CF_ADE_Y) != 0, az = (fl & CF_ADE_Z) != 0;
-        float dp[3], dpp[3], ep[3], p[3][2], pp[3][2];
-        const float eo[3] = {e.ex, e.ey, e.ez};
-        const bool comp[3] = {ax, ay, az};
+        const DevAde &A = P.ade[ade_set];
+        const bool comp[3] = {(fl & CF_ADE_X) != 0, (fl & CF_ADE_Y) != 0, (fl & CF_ADE_Z) != 0};
+        float dp[3] = {0, 0, 0}, dpp[3] = {0, 0, 0}, ep[3] = {0, 0, 0}, p[3][2], pp[3][2];
         for (int a = 0; a < 3; a++) {
             if (!comp[a]) continue;
             dp[a] = P.dp[a][c]; dpp[a] = P.dpp[a][c]; ep[a] = P.ep[a][c];
@@ -331,9 +200,8 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
             v += A.c2 * ep[a] + A.c3 * eo[a];
             ne[a] = v;
         }
-        // CPML inside the ADE branch, yee.c:950-1057 (first psi_E update)
-        if (!zero) {
-            if (inx0 && i > 1) {   // x0: corrections scaled by cb == 0 (yee.c:577)
+        if (!zero) {   // CPML inside the ADE branch, first psi_E update
+            if (inx0 && i > 1) {   // x0 corrections are scaled by cb == 0 (yee.c:577)
                 const float be = __ldg(P.be[X0] + i), ce = __ldg(P.ce[X0] + i);
                 px0[0] = be * px0[0] + ce * dhz_i * idx_;
                 px0[1] = be * px0[1] + ce * dhy_i * idx_;
@@ -342,48 +210,47 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
                 const float be = __ldg(P.be[Y0] + j), ce = __ldg(P.ce[Y0] + j);
                 py0[0] = be * py0[0] + ce * dhz_j * idx_;
                 py0[1] = be * py0[1] + ce * dhx_j * idx_;
-                if ((i > 0 && k > 0) && ax) ne[0] += P.dx * C.cba[0] * py0[0];
-                if ((i > 0 && k > 0) && az) ne[2] -= P.dx * C.cba[2] * py0[1];
+                if ((i > 0 && k > 0) && comp[0]) ne[0] += P.dx * cba[0] * py0[0];
+                if ((i > 0 && k > 0) && comp[2]) ne[2] -= P.dx * cba[2] * py0[1];
             }
             if (inz0 && k > 1) {
                 const float be = __ldg(P.be[Z0] + k), ce = __ldg(P.ce[Z0] + k);
-                pz0[1] = be * pz0[1] + ce * dhx_k * idx_;   // peyz
-                pz0[0] = be * pz0[0] + ce * dhy_k * idx_;   // pexz
-                if ((i > 0 && j > 0) && ay) ne[1] += P.dx * C.cba[1] * pz0[1];
-                if ((i > 0 && j > 0) && ax) ne[0] -= P.dx * C.cba[0] * pz0[0];
+                pz0[1] = be * pz0[1] + ce * dhx_k * idx_;
+                pz0[0] = be * pz0[0] + ce * dhy_k * idx_;
+                if ((i > 0 && j > 0) && comp[1]) ne[1] += P.dx * cba[1] * pz0[1];
+                if ((i > 0 && j > 0) && comp[0]) ne[0] -= P.dx * cba[0] * pz0[0];
             }
             if (inxn) {
                 const int ir = i - (xr - P.cp_d[XN]);
                 const float be = __ldg(P.be[XN] + ir), ce = __ldg(P.ce[XN] + ir);
                 pxn[0] = be * pxn[0] + ce * dhz_i * idx_;
                 pxn[1] = be * pxn[1] + ce * dhy_i * idx_;
-                if ((j > 0 && k > 0) && ay) ne[1] -= P.dx * C.cba[1] * pxn[0];
-                if ((j > 0 && k > 0) && az) ne[2] += P.dx * C.cba[2] * pxn[1];
+                if ((j > 0 && k > 0) && comp[1]) ne[1] -= P.dx * cba[1] * pxn[0];
+                if ((j > 0 && k > 0) && comp[2]) ne[2] += P.dx * cba[2] * pxn[1];
             }
             if (inyn) {
                 const int jr = j - (yr - P.cp_d[YN]);
                 const float be = __ldg(P.be[YN] + jr), ce = __ldg(P.ce[YN] + jr);
                 pyn[0] = be * pyn[0] + ce * dhz_j * idx_;
                 pyn[1] = be * pyn[1] + ce * dhx_j * idx_;
-                if ((i > 0 && k > 0) && ax) ne[0] += P.dx * C.cba[0] * pyn[0];
-                if ((i > 0 && k > 0) && az) ne[2] -= P.dx * C.cba[2] * pyn[1];
+                if ((i > 0 && k > 0) && comp[0]) ne[0] += P.dx * cba[0] * pyn[0];
+                if ((i > 0 && k > 0) && comp[2]) ne[2] -= P.dx * cba[2] * pyn[1];
             }
             if (inzn) {
                 const int kr = k - (zr - P.cp_d[ZN]);
                 const float be = __ldg(P.be[ZN] + kr), ce = __ldg(P.ce[ZN] + kr);
                 pzn[1] = be * pzn[1] + ce * dhx_k * idx_;
                 pzn[0] = be * pzn[0] + ce * dhy_k * idx_;
-                if ((i > 0 && j > 0) && ay) ne[1] += P.dx * C.cba[1] * pzn[1];
-                if ((i > 0 && j > 0) && ax) ne[0] -= P.dx * C.cba[0] * pzn[0];
+                if ((i > 0 && j > 0) && comp[1]) ne[1] += P.dx * cba[1] * pzn[1];
+                if ((i > 0 && j > 0) && comp[0]) ne[0] -= P.dx * cba[0] * pzn[0];
             }
         }
-        // polarisation recursions (only components the branch owns are ever read back)
-        for (int a = 0; a < 3; a++) {
+        for (int a = 0; a < 3; a++) {   // polarisation recursions of the owned components
             if (!comp[a]) continue;
-            const float en = ne[a];
-            P.dp[a][c] = A.a0 * dpp[a] + A.a1 * dp[a] + A.a2 * (ep[a] + 2.f * eo[a] + en);
+            const float e1 = ne[a];
+            P.dp[a][c] = A.a0 * dpp[a] + A.a1 * dp[a] + A.a2 * (ep[a] + 2.f * eo[a] + e1);
             for (int n = 0; n < NPOLES; n++) {
-                P.p_[a][n][c] = A.bp0[n] * pp[a][n] + A.bp1[n] * p[a][n] + A.bp2[n] * ep[a] + A.bp3[n] * eo[a] + A.bp4[n] * en;
+                P.p_[a][n][c] = A.bp0[n] * pp[a][n] + A.bp1[n] * p[a][n] + A.bp2[n] * ep[a] + A.bp3[n] * eo[a] + A.bp4[n] * e1;
                 P.pp_[a][n][c] = p[a][n];
             }
             P.ep[a][c] = eo[a];
@@ -391,15 +258,12 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
         }
         nx = ne[0]; ny = ne[1]; nz = ne[2];
     }
-    // ordinary update of the components left (yee.c:1113-1128)
-    if (gx && !(ADE && (fl & CF_ADE_X))) nx = C.ca[0] * e.ex + C.cb[0] * curlx;
-    if (gy && !(ADE && (fl & CF_ADE_Y))) ny = C.ca[1] * e.ey + C.cb[1] * curly;
-    if (gz && !(ADE && (fl & CF_ADE_Z))) nz = C.ca[2] * e.ez + C.cb[2] * curlz;
-    // PEC rule (yee.c:1138-1237)
+    if (gx && !(ADE && (fl & CF_ADE_X))) nx = ca[0] * eo[0] + cb[0] * curlx;
+    if (gy && !(ADE && (fl & CF_ADE_Y))) ny = ca[1] * eo[1] + cb[1] * curly;
+    if (gz && !(ADE && (fl & CF_ADE_Z))) nz = ca[2] * eo[2] + cb[2] * curlz;
     if (fl & CF_PEC_X) nx = 0.f;
     if (fl & CF_PEC_Y) ny = 0.f;
     if (fl & CF_PEC_Z) nz = 0.f;
-    // boundary_estep: zeroed planes and psi_E (second update for ADE cells), boundary.c:691-884
     if (zero) {
         nx = ny = nz = 0.f;
     } else {
@@ -410,18 +274,18 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
             px0[0] = be * px0[0] + ce * dhz_i * idx_;
             px0[1] = be * px0[1] + ce * dhy_i * idx_;
             if (j > 0 && k > 0) {
-                if (ty) ny -= dx * C.cb[1] * px0[0];
-                if (tz) nz += dx * C.cb[2] * px0[1];
+                if (ty) ny -= dx * cb[1] * px0[0];
+                if (tz) nz += dx * cb[2] * px0[1];
+                P.psie[X0][0][qx0] = px0[0]; P.psie[X0][1][qx0] = px0[1];
             }
-            if (j > 0 && k > 0) { P.psie[X0][0][qx0] = px0[0]; P.psie[X0][1][qx0] = px0[1]; }
         }
         if (iny0) {
             const float be = __ldg(P.be[Y0] + j), ce = __ldg(P.ce[Y0] + j);
             py0[0] = be * py0[0] + ce * dhz_j * idx_;
             py0[1] = be * py0[1] + ce * dhx_j * idx_;
             if (i > 0 && k > 0) {
-                if (tx) nx += dx * C.cb[0] * py0[0];
-                if (tz) nz -= dx * C.cb[2] * py0[1];
+                if (tx) nx += dx * cb[0] * py0[0];
+                if (tz) nz -= dx * cb[2] * py0[1];
                 P.psie[Y0][0][qy0] = py0[0]; P.psie[Y0][1][qy0] = py0[1];
             }
         }
@@ -430,8 +294,8 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
             pz0[1] = be * pz0[1] + ce * dhx_k * idx_;
             pz0[0] = be * pz0[0] + ce * dhy_k * idx_;
             if (i > 0 && j > 0) {
-                if (ty) ny += dx * C.cb[1] * pz0[1];
-                if (tz) nx -= dx * C.cb[0] * pz0[0];     // gated by ztbc in the reference (boundary.c:758-759)
+                if (ty) ny += dx * cb[1] * pz0[1];
+                if (tz) nx -= dx * cb[0] * pz0[0];     // gated by ztbc in the reference (boundary.c:758-759)
                 P.psie[Z0][0][qz0] = pz0[0]; P.psie[Z0][1][qz0] = pz0[1];
             }
         }
@@ -441,8 +305,8 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
             pxn[0] = be * pxn[0] + ce * dhz_i * idx_;
             pxn[1] = be * pxn[1] + ce * dhy_i * idx_;
             if (j > 0 && k > 0) {
-                if (ty) ny -= dx * C.cb[1] * pxn[0];
-                if (tz) nz += dx * C.cb[2] * pxn[1];
+                if (ty) ny -= dx * cb[1] * pxn[0];
+                if (tz) nz += dx * cb[2] * pxn[1];
                 P.psie[XN][0][qxn] = pxn[0]; P.psie[XN][1][qxn] = pxn[1];
             }
         }
@@ -452,8 +316,8 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
             pyn[0] = be * pyn[0] + ce * dhz_j * idx_;
             pyn[1] = be * pyn[1] + ce * dhx_j * idx_;
             if (i > 0 && k > 0) {
-                if (tx) nx += dx * C.cb[0] * pyn[0];
-                if (tz) nz -= dx * C.cb[2] * pyn[1];
+                if (tx) nx += dx * cb[0] * pyn[0];
+                if (tz) nz -= dx * cb[2] * pyn[1];
                 P.psie[YN][0][qyn] = pyn[0]; P.psie[YN][1][qyn] = pyn[1];
             }
         }
@@ -463,87 +327,163 @@ __device__ void e_cell(const DevPlan &P, const DevClass *cls, int i, int j, int 
             pzn[1] = be * pzn[1] + ce * dhx_k * idx_;
             pzn[0] = be * pzn[0] + ce * dhy_k * idx_;
             if (i > 0 && j > 0) {
-                if (ty) ny += dx * C.cb[1] * pzn[1];
-                if (tx) nx -= dx * C.cb[0] * pzn[0];
+                if (ty) ny += dx * cb[1] * pzn[1];
+                if (tx) nx -= dx * cb[0] * pzn[0];
                 P.psie[ZN][0][qzn] = pzn[0]; P.psie[ZN][1][qzn] = pzn[1];
             }
         }
     }
-    if (P.tsf_on) tsf_e(P, i, j, k, C.tsfe, nx, ny, nz);
-    P.fout[0][c] = nx;
-    P.fout[1][c] = ny;
-    P.fout[2][c] = nz;
+    if (P.tsf_on) tsf_add_e(P, i, j, k, nx, ny, nz);
+    return make_float3(nx, ny, nz);
 }
 
-// ------------------------------------------------------------ fused kernel
+// ------------------------------------------------------------ slab kernels
+
+// One thread per cell of the slab boxes (the CPML slabs and every cell the
+// bulk kernel does not own).  slab_h forms H^{n+1/2} with the full special
+// path; slab_e then forms E^{n+1} from the H^{n+1/2} that slab_h and the bulk
+// kernel wrote.  Both read E^n/H^n from the input set only.
+
+__device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &i, int &j, int &k)
+{
+    int b = 0;
+    while (b + 1 < nboxes && (long long)blockIdx.x >= boxes[b + 1].first_block) b++;
+    const SlabBox B = boxes[b];
+    long long t = ((long long)blockIdx.x - B.first_block) * blockDim.x + threadIdx.x;
+    const int nk = B.k1 - B.k0, nj = B.j1 - B.j0;
+    if (t >= (long long)(B.i1 - B.i0) * nj * nk) return false;
+    k = B.k0 + (int)(t % nk);
+    t /= nk;
+    j = B.j0 + (int)(t % nj);
+    i = B.i0 + (int)(t / nj);
+    return true;
+}
+
+__global__ void __launch_bounds__(256) slab_h_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
+{
+    int i, j, k;
+    if (!box_cell(boxes, nboxes, i, j, k)) return;
+    const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
+    const float *EX = P.fin[0], *EY = P.fin[1], *EZ = P.fin[2];
+    const float ex = __ldg(EX + c), ey = __ldg(EY + c), ez = __ldg(EZ + c);
+    const bool il = (i == P.xr - 1), jl = (j == P.yr - 1), kl = (k == P.zr - 1);
+    const float eyk = kl ? 0.f : __ldg(EY + c + 1), exk = kl ? 0.f : __ldg(EX + c + 1);
+    const float ezj = jl ? 0.f : __ldg(EZ + c + P.sj), exj = jl ? 0.f : __ldg(EX + c + P.sj);
+    const float ezi = il ? 0.f : __ldg(EZ + c + P.si), eyi = il ? 0.f : __ldg(EY + c + P.si);
+    float h[3] = {__ldg(P.fin[3] + c), __ldg(P.fin[4] + c), __ldg(P.fin[5] + c)};
+    const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
+    h_update(P, cl, cls_at(P, i, j, k), i, j, k, true, true, eyi - ey, ezi - ez, exj - ex, ezj - ez, exk - ex, eyk - ey, h);
+    P.fout[3][c] = h[0];
+    P.fout[4][c] = h[1];
+    P.fout[5][c] = h[2];
+}
 
 template <bool ADE, int NPOLES>
-__global__ void __launch_bounds__(FDTD_TK * FDTD_TJ, 2) fused_step_kernel(const DevPlan P, int ichunk)
+__global__ void __launch_bounds__(256) slab_e_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
 {
-    constexpr int TK = FDTD_TK, TJ = FDTD_TJ;
-    __shared__ float sh[3][TJ + 1][TK + 1];          // H^{n+1/2}(i) with the j0-1 row and k0-1 column
-    __shared__ DevClass scls[FDTD_MAX_CLASSES];
-    const int tid = threadIdx.x;
-    const int tk = tid % TK, tj = tid / TK;
-    const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
-    const int k = k0 + tk, j = j0 + tj;
-    const bool own = (k < P.zr) && (j < P.yr);
-    const int ib = blockIdx.z * ichunk;
-    const int ie = min(P.xr, ib + ichunk);
-    {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(P.classes);
-        uint32_t *dst = reinterpret_cast<uint32_t *>(scls);
-        const int words = P.nclasses * (int)(sizeof(DevClass) / 4);
-        for (int w = tid; w < words; w += TK * TJ) dst[w] = src[w];
-    }
-    // halo cell owned by this thread: row j0-1 (tid < TK) or column k0-1
-    int hj = -1, hk = -1;
-    if (tid < TK) { hj = j0 - 1; hk = k0 + tid; }
-    else if (tid < TK + TJ) { hj = j0 + (tid - TK); hk = k0 - 1; }
-    const bool halo = hj >= 0 && hk >= 0 && hj < P.yr && hk < P.zr;
-    __syncthreads();
+    int i, j, k;
+    if (!box_cell(boxes, nboxes, i, j, k)) return;
+    const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
+    const float *HX = P.fout[3], *HY = P.fout[4], *HZ = P.fout[5];   // H^{n+1/2}, written this step
+    const float3 eo = make_float3(__ldg(P.fin[0] + c), __ldg(P.fin[1] + c), __ldg(P.fin[2] + c));
+    const float3 h = make_float3(HX[c], HY[c], HZ[c]);
+    const float hx_jm = j > 0 ? HX[c - P.sj] : 0.f, hz_jm = j > 0 ? HZ[c - P.sj] : 0.f;
+    const float hx_km = k > 0 ? HX[c - 1] : 0.f, hy_km = k > 0 ? HY[c - 1] : 0.f;
+    const float hy_im = i > 0 ? HY[c - P.si] : 0.f, hz_im = i > 0 ? HZ[c - P.si] : 0.f;
+    const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
+    const float3 en = e_special<ADE, NPOLES>(P, cl, cls_at(P, i, j, k), i, j, k, eo, h, hx_jm, hz_jm, hx_km, hy_km, hy_im, hz_im);
+    P.fout[0][c] = en.x;
+    P.fout[1][c] = en.y;
+    P.fout[2][c] = en.z;
+}
 
-    float hy_im = 0.f, hz_im = 0.f;   // H^{n+1/2}(i-1) at this thread's cell
-    if (ib > 0 && own) {
-        EOwn e;
-        float h[3];
-        load_e(P, (int64_t)(ib - 1) * P.si + (int64_t)j * P.sj + k, ib - 1, j, k, e);
-        h_cell(P, scls, ib - 1, j, k, false, e, h);
-        hy_im = h[1];
-        hz_im = h[2];
+// ------------------------------------------------------------ TSF face tables
+
+// This step's TSF corrections for every face cell (source.c:547-771 and
+// 1476-1672): the 1D grid value at corr*dcomp(cell) by the cubic
+// interpolation of dline.c:89-111 (FP64), projected by gex..ghz, scaled by
+// dt/(dx mu0) for H or (dt/dx)/epsilon(cell) for E, gated by TSF_SKIP, the
+// source-skip map and (k0 face) the PEC test.  Runs after aux_step.
+__global__ void tsf_face_kernel(const __grid_constant__ DevPlan P, int total)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int i0 = P.t0[0], j0 = P.t0[1], k0 = P.t0[2], in = P.t1[0], jn = P.t1[1], kn = P.t1[2];
+    const int ni = in - i0 + 1, nj = jn - j0 + 1, nk = kn - k0 + 1;
+    const int sz[3] = {nj * nk, ni * nk, ni * nj};
+    int f = 0, off = t;
+    while (f < 6 && off >= sz[f / 2]) { off -= sz[f / 2]; f++; }
+    if (f >= 6) return;
+    const int a = off / P.tnb[f], b = off % P.tnb[f];
+    const uint8_t fl = P.tmap[f][off];
+    const double hc = P.hcor;
+    float2 dh = make_float2(0.f, 0.f), de = make_float2(0.f, 0.f);
+    const float4 *cls4 = reinterpret_cast<const float4 *>(P.classes);
+    if (fl & 1) {
+        int ei, ej, ek;   // E cell; dH / dE are the dcomp positions of the H and E corrections
+        double dH, dE;
+        if (f < 2) {
+            const int j = j0 + a, k = k0 + b;
+            if (f == 0) { ei = i0; dH = tsf_dcomp(P, i0, j, k); dE = tsf_dcomp(P, i0 - 1, j, k); }
+            else { ei = in; dH = tsf_dcomp(P, in, j, k); dE = dH; }
+            ej = j; ek = k;
+        } else if (f < 4) {
+            const int i = i0 + a, k = k0 + b;
+            if (f == 2) { ej = j0; dH = tsf_dcomp(P, i, j0, k); dE = tsf_dcomp(P, i, j0 - 1, k); }
+            else { ej = jn; dH = tsf_dcomp(P, i, jn, k); dE = dH; }
+            ei = i; ek = k;
+        } else {
+            const int i = i0 + a, j = j0 + b;
+            if (f == 4) { ek = k0; dH = tsf_dcomp(P, i, j, k0); dE = tsf_dcomp(P, i, j, k0 - 1); }
+            else { ek = kn; dH = tsf_dcomp(P, i, j, kn); dE = dH; }
+            ei = i; ej = j;
+        }
+        const double ve = tsf_dval(P.aux_e, P.jres, dH);
+        const double vh = tsf_dval(P.aux_h, P.jres, dE);
+        const double ce = (double)cls4[cls_at(P, ei, ej, ek) * 4 + 1].w;
+        const bool pec = (fl & 2) != 0;
+        switch (f) {
+        case 0:
+            if (ek < kn) dh.x = -(float)(hc * (ve * P.gez));
+            if (ej < jn) dh.y = (float)(hc * (ve * P.gey));
+            if (ej < jn) de.x = (float)(ce * (vh * P.ghz));
+            if (ek < kn) de.y = -(float)(ce * (vh * P.ghy));
+            break;
+        case 1:
+            if (ek < kn) dh.x = (float)(hc * (ve * P.gez));
+            if (ej < jn) dh.y = -(float)(hc * (ve * P.gey));
+            if (ej < jn) de.x = -(float)(ce * (vh * P.ghz));
+            if (ek < kn) de.y = (float)(ce * (vh * P.ghy));
+            break;
+        case 2:
+            if (ek < kn) dh.x = (float)(hc * (ve * P.gez));
+            if (ei < in) dh.y = -(float)(hc * (ve * P.gex));
+            if (ei < in) de.x = -(float)(ce * (vh * P.ghz));
+            if (ek < kn) de.y = (float)(ce * (vh * P.ghx));
+            break;
+        case 3:
+            if (ek < kn) dh.x = -(float)(hc * (ve * P.gez));
+            if (ei < in) dh.y = (float)(hc * (ve * P.gex));
+            if (ei < in) de.x = (float)(ce * (vh * P.ghz));
+            if (ek < kn) de.y = -(float)(ce * (vh * P.ghx));
+            break;
+        case 4:
+            if (ej < jn && !pec) dh.x = -(float)(hc * (ve * P.gey));
+            if (ei < in && !pec) dh.y = (float)(hc * (ve * P.gex));
+            if (ei < in && !pec) de.x = (float)(ce * (vh * P.ghy));
+            if (ej < jn && !pec) de.y = -(float)(ce * (vh * P.ghx));
+            break;
+        default:
+            if (ej < jn) dh.x = (float)(hc * (ve * P.gey));
+            if (ei < in) dh.y = -(float)(hc * (ve * P.gex));
+            if (ei < in) de.x = -(float)(ce * (vh * P.ghy));
+            if (ej < jn) de.y = (float)(ce * (vh * P.ghx));
+            break;
+        }
     }
-    for (int i = ib; i < ie; i++) {
-        EOwn e;
-        float h[3] = {0.f, 0.f, 0.f};
-        const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
-        if (own) {
-            load_e(P, c, i, j, k, e);
-            h_cell(P, scls, i, j, k, true, e, h);
-            sh[0][tj + 1][tk + 1] = h[0];
-            sh[1][tj + 1][tk + 1] = h[1];
-            sh[2][tj + 1][tk + 1] = h[2];
-            P.fout[3][c] = h[0];
-            P.fout[4][c] = h[1];
-            P.fout[5][c] = h[2];
-        }
-        if (halo) {
-            EOwn eh;
-            float hh[3];
-            load_e(P, (int64_t)i * P.si + (int64_t)hj * P.sj + hk, i, hj, hk, eh);
-            h_cell(P, scls, i, hj, hk, false, eh, hh);
-            sh[0][hj - j0 + 1][hk - k0 + 1] = hh[0];
-            sh[1][hj - j0 + 1][hk - k0 + 1] = hh[1];
-            sh[2][hj - j0 + 1][hk - k0 + 1] = hh[2];
-        }
-        __syncthreads();
-        if (own) {
-            e_cell<ADE, NPOLES>(P, scls, i, j, k, e, h, sh[0][tj][tk + 1], sh[2][tj][tk + 1], sh[0][tj + 1][tk],
-                                sh[1][tj + 1][tk], hy_im, hz_im);
-        }
-        hy_im = h[1];
-        hz_im = h[2];
-        __syncthreads();
-    }
+    P.tcor_h[f][off] = dh;
+    P.tcor_e[f][off] = de;
+    (void)a; (void)b;
 }
 
 // ------------------------------------------------------------ 1D aux grid
@@ -698,16 +638,22 @@ void launch_aux_step(const DevAux &a, cudaStream_t st) { aux_step_kernel<<<1, 10
 
 void launch_probe_capture(const DevAux &a, cudaStream_t st) { probe_capture_kernel<<<1, 256, 0, st>>>(a); }
 
-cudaError_t launch_fused_step(const DevPlan &p, int ichunk, bool ade, int npoles, cudaStream_t st)
+void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st)
 {
-    dim3 grid((p.zr + FDTD_TK - 1) / FDTD_TK, (p.yr + FDTD_TJ - 1) / FDTD_TJ, (p.xr + ichunk - 1) / ichunk);
-    dim3 block(FDTD_TK * FDTD_TJ);
+    if (total > 0) tsf_face_kernel<<<(total + 255) / 256, 256, 0, st>>>(p, total);
+}
+
+cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
+                              cudaStream_t st)
+{
+    if (nblocks <= 0) return cudaSuccess;
+    slab_h_kernel<<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     if (!ade)
-        fused_step_kernel<false, 0><<<grid, block, 0, st>>>(p, ichunk);
+        slab_e_kernel<false, 0><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     else if (npoles == 0)
-        fused_step_kernel<true, 0><<<grid, block, 0, st>>>(p, ichunk);
+        slab_e_kernel<true, 0><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     else
-        fused_step_kernel<true, 2><<<grid, block, 0, st>>>(p, ichunk);
+        slab_e_kernel<true, 2><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     return cudaGetLastError();
 }
 

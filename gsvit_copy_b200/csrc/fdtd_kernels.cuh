@@ -5,9 +5,6 @@
 
 #include "fdtd_internal.h"
 
-// fused tile: TK cells along k (contiguous, one warp per j row), TJ rows along j
-#define FDTD_TK 32
-#define FDTD_TJ 16
 
 struct DevAux {                 // 1D auxiliary grid of the TSF source (1dpool.c)
     double *e, *h;              // res values each
@@ -38,9 +35,17 @@ struct DevNfff {
     double inv2dx;
 };
 
+// a box of cells handled one thread per cell; blocks [first_block, next box's first_block)
+struct SlabBox {
+    int i0, i1, j0, j1, k0, k1;
+    long long first_block;
+};
+
 void launch_aux_step(const DevAux &a, cudaStream_t st);
 void launch_probe_capture(const DevAux &a, cudaStream_t st);
-cudaError_t launch_fused_step(const DevPlan &p, int ichunk, bool ade, int npoles, cudaStream_t st);
+void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st);
+cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
+                              cudaStream_t st);
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st);
 
 struct DevFarfield {

@@ -76,6 +76,12 @@ class Solver:
         abi.check(self.lib.fdtd_step_timed(self.h, n, C.byref(ms), C.byref(cnt)), "fdtd_step_timed")
         return ms.value, cnt.value
 
+    def step_profile(self, n: int) -> dict:
+        out = (C.c_double * 8)()
+        abi.check(self.lib.fdtd_step_profile(self.h, n, out), "fdtd_step_profile")
+        keys = ["bulk_ms", "bulk_bytes", "slab_ms", "slab_bytes", "aux_ms", "nfff_ms", "total_ms", "launches_per_step"]
+        return dict(zip(keys, list(out)))
+
     @property
     def step_count(self) -> int:
         s = C.c_int()

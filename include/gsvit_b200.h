@@ -226,6 +226,14 @@ int fdtd_get_step(const fdtd_plan *plan, int *step);
  * for the roofline of the dominant kernel). */
 int fdtd_step_timed(fdtd_plan *plan, int nsteps, double *fused_ms, int *fused_launches);
 
+/* Per-kernel profile of nsteps steps (CUDA events around every launch):
+ * out[0..1] = bulk kernel total ms / algorithmic bytes per launch,
+ * out[2..3] = slab kernels (H+E) total ms / algorithmic bytes per launch,
+ * out[4] = 1D aux grid + TSF face tables total ms, out[5] = NFFF running DFT
+ * total ms, out[6] = all kernels of the steps total ms, out[7] = kernel
+ * launches per step. */
+int fdtd_step_profile(fdtd_plan *plan, int nsteps, double out[8]);
+
 /* ---- outputs ------------------------------------------------------------- */
 
 /* Probe series: out[(p*nsteps + step)*6 + c], c = Ex,Ey,Ez,Hx,Hy,Hz, for the
