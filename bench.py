@@ -187,12 +187,12 @@ def hbm_peak():
 
 
 def ncu_traffic(res):
-    """DRAM bytes per launch of the bulk kernel from the committed ncu summary of this workload."""
-    path = os.path.join(HERE, "profiles", f"bulk_kernel_rough{res}.txt")
+    """DRAM bytes per launch of the bulk kernel from the committed ncu launch list of this workload."""
+    path = os.path.join(HERE, "profiles", f"launches_rough{res}.txt")
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_launch:"):
+                if line.startswith("bulk_kernel dram_bytes_per_launch:"):
                     return float(line.split(":", 1)[1].split()[0])
     except OSError:
         pass

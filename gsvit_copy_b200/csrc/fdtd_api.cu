@@ -866,7 +866,9 @@ int fdtd_get_map(fdtd_plan *P, int which, int32_t *out, size_t out_len)
     case FDTD_MAP_CLASS: {
         std::vector<uint8_t> tmp(n);
         CK(cudaSetDevice(P->device));
-        CK(cudaMemcpy(tmp.data(), P->dp.cls, n, cudaMemcpyDeviceToHost));
+        // rows of zres bytes at a pitch of cpitch bytes on the device
+        CK(cudaMemcpy2D(tmp.data(), P->hp.zr, P->dp.cls, P->dp.cpitch, P->hp.zr, (size_t)P->hp.xr * P->hp.yr,
+                        cudaMemcpyDeviceToHost));
         for (size_t c = 0; c < n; c++) out[c] = tmp[c];
         break;
     }

@@ -48,13 +48,18 @@ def test_random_state_parity(kind):
 
 @pytest.mark.parametrize("kind", KINDS)
 def test_tsf_driven_parity_and_farfield(kind):
-    s = plan.small_scene(kind, nsteps=300)
+    """Plane-wave pulse through the TSF box for 200 steps (the scattered wave
+    still fills the box; later the fields decay to a residual of ~1e-3 of the
+    peak and a relative norm of them measures FP32 rounding only).  Fields are
+    also compared at step 100, and probes / far field over the whole run."""
+    s = plan.small_scene(kind, nsteps=200)
     g, o = _pair(s)
-    g.step(300)
-    o.step(300)
-    fg, fo = g.fields(), o.fields()
-    errs = [rel_l2(a, b) for a, b in zip(fg, fo)]
-    assert max(errs) < TOL, errs
+    for n in (100, 100):
+        g.step(n)
+        o.step(n)
+        fg, fo = g.fields(), o.fields()
+        errs = [rel_l2(a, b) for a, b in zip(fg, fo)]
+        assert max(errs) < TOL, (o.step_count, errs)
     assert rel_l2(g.probes(), o.probes()) < TOL
     spec = g.nfff_spectrum()
     ref = series_spectrum(o.nfff_series(), s.nfff["omega"], s.dt)
@@ -88,3 +93,16 @@ def test_snapshot_restore_bitwise():
     g.step(30)
     for x, y in zip(first, g.fields(dtype=np.float32)):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("kind", ["lintab", "full"])
+def test_class_map_readback(kind):
+    """The per-cell class map (pitched rows on the device) reads back with one
+    id per cell, every id in use, and a single class on the plain interior."""
+    s = plan.small_scene(kind)
+    g = Solver(s)
+    m = g.map(abi.MAP_CLASS)
+    n = g.nclasses
+    assert m.min() >= 0 and m.max() < n
+    assert len(np.unique(m)) == n
+    assert len(np.unique(m[11:13, 9:11, 2:4])) == 1
