@@ -32,6 +32,7 @@ EX, EY, EZ, HX, HY, HZ = 0x01, 0x02, 0x04, 0x08, 0x10, 0x20
 E_ALL, H_ALL = EX | EY | EZ, HX | HY | HZ
 EH = E_ALL | H_ALL
 MAP_MAT, MAP_BNDS, MAP_SOURCESKIP, MAP_CLASS = 0, 1, 2, 3
+STATIC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
@@ -131,6 +132,7 @@ def load_library():
         "fdtd_get_fields_f32": ([P, C.c_int, C.POINTER(_fp)], C.c_int),
         "fdtd_step": ([P, C.c_int], C.c_int),
         "fdtd_step_graph": ([P, C.c_int, C.c_int], C.c_int),
+        "fdtd_step_static_scratch": ([P, C.c_int], C.c_int),
         "fdtd_get_step": ([P, C.POINTER(C.c_int)], C.c_int),
         "fdtd_step_timed": ([P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),
         "fdtd_step_profile": ([P, C.c_int, _dp], C.c_int),
@@ -155,7 +157,7 @@ def load_library():
 HEADER_SYMBOLS = [
     "fdtd_plan_create", "fdtd_plan_destroy", "fdtd_set_stream", "fdtd_sync",
     "fdtd_set_fields", "fdtd_get_fields", "fdtd_get_fields_f32", "fdtd_set_fields_f32",
-    "fdtd_step", "fdtd_step_graph", "fdtd_get_step", "fdtd_step_timed", "fdtd_step_profile",
+    "fdtd_step", "fdtd_step_graph", "fdtd_step_static_scratch", "fdtd_get_step", "fdtd_step_timed", "fdtd_step_profile",
     "fdtd_get_probes", "fdtd_nfff_spectrum", "fdtd_get_map", "fdtd_get_nclasses",
     "fdtd_snapshot_size", "fdtd_snapshot_save", "fdtd_snapshot_restore",
     "fdtd_last_error", "fdtd_step_bytes",

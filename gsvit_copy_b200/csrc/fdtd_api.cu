@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -672,6 +673,83 @@ int fdtd_step(fdtd_plan *P, int nsteps)
         if (rc != FDTD_OK) return rc;
         P->host_step++;
     }
+    final_probes(P, P->stream);
+    CK(cudaGetLastError());
+    return FDTD_OK;
+}
+
+}  // extern "C"
+
+// Scratch of fdtd_step_static_scratch: this step's TSF face correction tables,
+// one per device (the module's copy on each device), never allocated.
+static __device__ __align__(256) unsigned char g_static_scratch[FDTD_STATIC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kStaticDevices = 64;
+std::mutex g_static_mu;
+void *g_static_addr[kStaticDevices] = {};
+
+// Device address of g_static_scratch on `device` (current), looked up once.
+int static_scratch_addr(int device, unsigned char **out)
+{
+    if (device < 0 || device >= kStaticDevices) return fail(FDTD_E_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(FDTD_E_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+        g_static_addr[device] = p;
+    }
+    *out = static_cast<unsigned char *>(g_static_addr[device]);
+    return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_step_static_scratch(fdtd_plan *P, int nsteps)
+{
+    if (!P || nsteps < 0) return fail(FDTD_E_INVALID, "bad argument");
+    CK(cudaSetDevice(P->device));
+    unsigned char *base = nullptr;
+    int rc = static_scratch_addr(P->device, &base);
+    if (rc != FDTD_OK) return rc;
+    // carve the twelve tables (H and E corrections of six faces) out of the array
+    float2 *th[6] = {}, *te[6] = {};
+    size_t used = 0;
+    if (P->tsf_cells) {
+        for (int f = 0; f < 6; f++) {
+            const size_t bytes = (P->hp.tmap[f].size() * sizeof(float2) + 255) & ~(size_t)255;
+            if (used + 2 * bytes > FDTD_STATIC_SCRATCH_BYTES)
+                return fail(FDTD_E_UNSUPPORTED, "the TSF face tables of this plan need more than the "
+                                                "FDTD_STATIC_SCRATCH_BYTES (32 MiB) of static scratch");
+            th[f] = reinterpret_cast<float2 *>(base + used);
+            te[f] = reinterpret_cast<float2 *>(base + used + bytes);
+            used += 2 * bytes;
+        }
+    }
+    float2 *keep_h[6], *keep_e[6];
+    for (int f = 0; f < 6; f++) {
+        keep_h[f] = P->dp.tcor_h[f];
+        keep_e[f] = P->dp.tcor_e[f];
+        if (P->tsf_cells) {
+            P->dp.tcor_h[f] = th[f];
+            P->dp.tcor_e[f] = te[f];
+        }
+    }
+    rc = FDTD_OK;
+    for (int s = 0; s < nsteps && rc == FDTD_OK; s++) {
+        rc = launch_step(P, P->stream);
+        if (rc == FDTD_OK) P->host_step++;
+    }
+    for (int f = 0; f < 6; f++) {
+        P->dp.tcor_h[f] = keep_h[f];
+        P->dp.tcor_e[f] = keep_e[f];
+    }
+    if (rc != FDTD_OK) return rc;
     final_probes(P, P->stream);
     CK(cudaGetLastError());
     return FDTD_OK;
