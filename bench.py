@@ -306,6 +306,10 @@ def run_b200(a):
                 "traffic": ncu_traffic(a.res), "algorithmic_bytes": prof["bulk_bytes"],
                 "ms_per_launch": prof["bulk_ms"] / nprof,
                 "step_share": prof["bulk_ms"] / prof["total_ms"] if prof["total_ms"] else None}
+    # far-field integration of the accumulated running DFTs (once per run)
+    t0 = time.perf_counter()
+    spec = g.nfff_spectrum()
+    ff_ms = (time.perf_counter() - t0) * 1e3
     step_bytes = g.step_bytes()
     step_gbs = step_bytes / (ms / K * 1e-3) / 1e9
     gpu_launches = int(prof["launches_per_step"]) * K
@@ -350,6 +354,8 @@ def run_b200(a):
             "gpu_launches": gpu_launches, "roofline": roofline,
             "step_gbs_algorithmic": step_gbs, "step_bytes_algorithmic": step_bytes,
             "kernel_ms_per_step": {k: prof[k] / nprof for k in ("bulk_ms", "slab_ms", "aux_ms", "nfff_ms", "total_ms")},
+            "farfield_finalize_ms": ff_ms,
+            "farfield_points": int(spec.shape[0]),
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

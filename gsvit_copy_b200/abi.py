@@ -76,7 +76,7 @@ class Nfff(C.Structure):
         ("i0", C.c_int32), ("j0", C.c_int32), ("k0", C.c_int32),
         ("in_", C.c_int32), ("jn", C.c_int32), ("kn", C.c_int32),
         ("skip", C.c_int32 * 6), ("skip_lo", (C.c_int32 * 2) * 6), ("skip_hi", (C.c_int32 * 2) * 6),
-        ("npoints", C.c_int32), ("nfreq", C.c_int32),
+        ("npoints", C.c_int32), ("nfreq", C.c_int32), ("series", C.c_int32), ("reserved", C.c_int32),
         ("points", _ip), ("istart", _ip), ("omega", _dp),
     ]
 
@@ -138,6 +138,8 @@ def load_library():
         "fdtd_step_profile": ([P, C.c_int, _dp], C.c_int),
         "fdtd_get_probes": ([P, _dp, C.c_size_t], C.c_int),
         "fdtd_nfff_spectrum": ([P, _dp, C.c_size_t], C.c_int),
+        "fdtd_nfff_ndata": ([P, C.POINTER(C.c_int)], C.c_int),
+        "fdtd_nfff_series": ([P, _dp, C.c_size_t], C.c_int),
         "fdtd_get_map": ([P, C.c_int, _ip, C.c_size_t], C.c_int),
         "fdtd_get_nclasses": ([P, C.POINTER(C.c_int)], C.c_int),
         "fdtd_snapshot_size": ([P, C.POINTER(C.c_size_t)], C.c_int),
@@ -158,7 +160,7 @@ HEADER_SYMBOLS = [
     "fdtd_plan_create", "fdtd_plan_destroy", "fdtd_set_stream", "fdtd_sync",
     "fdtd_set_fields", "fdtd_get_fields", "fdtd_get_fields_f32", "fdtd_set_fields_f32",
     "fdtd_step", "fdtd_step_graph", "fdtd_step_static_scratch", "fdtd_get_step", "fdtd_step_timed", "fdtd_step_profile",
-    "fdtd_get_probes", "fdtd_nfff_spectrum", "fdtd_get_map", "fdtd_get_nclasses",
+    "fdtd_get_probes", "fdtd_nfff_spectrum", "fdtd_nfff_ndata", "fdtd_nfff_series", "fdtd_get_map", "fdtd_get_nclasses",
     "fdtd_snapshot_size", "fdtd_snapshot_save", "fdtd_snapshot_restore",
     "fdtd_last_error", "fdtd_step_bytes",
 ]

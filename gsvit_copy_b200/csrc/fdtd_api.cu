@@ -8,6 +8,7 @@
 // fdtd_step_graph replays them from a CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -108,6 +109,9 @@ struct fdtd_plan {
     const float **d_efieldptrs[2] = {nullptr, nullptr};
     DevFarfield ff;
     std::vector<double> omega;
+    bool nfff_series = false;             // time-domain series of farfield.c, exact
+    DevNfffSeries ns;
+    int nfff_ndata = 0;
     // graphs per parity
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_steps = 0;
@@ -148,6 +152,23 @@ int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
     return FDTD_OK;
 }
 
+// NFFF work of a step: running DFT and/or the exact time-domain series,
+// both reading the E set this step wrote
+void launch_nfff(fdtd_plan *P, int in, cudaStream_t st)
+{
+    if (!P->nfff) return;
+    if (P->nfff_nfreq > 0) {
+        DevNfff n = P->nf;
+        n.e = P->d_efieldptrs[1 - in];
+        launch_nfff_accumulate(n, st);
+    }
+    if (P->nfff_series) {
+        DevNfffSeries q = P->ns;
+        q.e = P->d_efieldptrs[1 - in];
+        launch_nfff_series(q, st);
+    }
+}
+
 int launch_step(fdtd_plan *P, cudaStream_t st)
 {
     const int in = P->cur;
@@ -157,11 +178,7 @@ int launch_step(fdtd_plan *P, cudaStream_t st)
     if (P->tsf_cells) launch_tsf_faces(P->dp, P->tsf_cells, st);
     int rc = launch_fused(P, in, st);
     if (rc != FDTD_OK) return rc;
-    if (P->nfff) {
-        DevNfff n = P->nf;
-        n.e = P->d_efieldptrs[1 - in];
-        launch_nfff_accumulate(n, st);
-    }
+    launch_nfff(P, in, st);
     P->cur = 1 - in;
     return FDTD_OK;
 }
@@ -251,23 +268,21 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
         d.ade = ade;
         d.nade = (int)hp.ades.size();
         for (int a = 0; a < 3; a++) {
-            CA(P->mem.alloc(&d.ep[a], n), "ADE state");
-            CA(P->mem.alloc(&d.dp[a], n), "ADE state");
-            CA(P->mem.alloc(&d.dpp[a], n), "ADE state");
-            P->snap.push_back({d.ep[a], n * 4}); P->snap.push_back({d.dp[a], n * 4}); P->snap.push_back({d.dpp[a], n * 4});
+            CA(P->mem.alloc(&d.q[a], n), "ADE state");
+            P->snap.push_back({d.q[a], n * 4});
             for (int q = 0; q < hp.maxpoles; q++) {
-                CA(P->mem.alloc(&d.p_[a][q], n), "ADE state");
-                CA(P->mem.alloc(&d.pp_[a][q], n), "ADE state");
-                P->snap.push_back({d.p_[a][q], n * 4}); P->snap.push_back({d.pp_[a][q], n * 4});
+                CA(P->mem.alloc(&d.pc[a][q], n), "ADE state");
+                CA(P->mem.alloc(&d.qc[a][q], n), "ADE state");
+                P->snap.push_back({d.pc[a][q], n * 4}); P->snap.push_back({d.qc[a][q], n * 4});
             }
         }
-        size_t nd = 0;   // dispersive cells: per owned component E^{n-1}, P_D, P_D^{n-1} (+4 per pole) read+written
+        size_t nd = 0;   // dispersive components: Q read + written, E^{n-1} read (12 B), + 16 B per pole (p, q)
         for (size_t c = 0; c < n; c++) {
             const DevClass &k = hp.classes[hp.cls[c]];
             if (k.flags & CF_ADE_BRANCH)
                 nd += ((k.flags & CF_ADE_X) ? 1 : 0) + ((k.flags & CF_ADE_Y) ? 1 : 0) + ((k.flags & CF_ADE_Z) ? 1 : 0);
         }
-        bytes += (double)nd * (3 + 4 * hp.maxpoles) * 8.0;
+        bytes += (double)nd * (12.0 + 16.0 * hp.maxpoles);
     }
     // CPML
     for (int f = 0; f < 6; f++) {
@@ -383,7 +398,7 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
         P->d_fieldptrs[s] = fp;
     }
     // NFFF running DFT over the box faces (farfield.c:207-404 loops), skip rules included
-    if (desc->nfff.enabled && desc->nfff.npoints > 0 && desc->nfff.nfreq > 0) {
+    if (desc->nfff.enabled && desc->nfff.npoints > 0 && (desc->nfff.nfreq > 0 || desc->nfff.series)) {
         const fdtd_nfff &f = desc->nfff;
         if (f.i0 < 1 || f.j0 < 1 || f.k0 < 1 || f.in > hp.xr - 2 || f.jn > hp.yr - 2 || f.kn > hp.zr - 2 || f.in <= f.i0 ||
             f.jn <= f.j0 || f.kn <= f.k0)
@@ -419,19 +434,13 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
         P->nfff_npoints = f.npoints;
         P->nfff_nfreq = f.nfreq;
         P->nfff_ns = (int)cell.size();
-        P->omega.assign(f.omega, f.omega + f.nfreq);
-        std::vector<double> odt(f.nfreq);
-        for (int q = 0; q < f.nfreq; q++) odt[q] = f.omega[q] * hp.dt;
+        if (f.nfreq > 0) P->omega.assign(f.omega, f.omega + f.nfreq);
         int32_t *dcell, *dnstr, *dijk, *dpts, *dist;
         int8_t *dface;
-        double *dodt, *dom;
-        double2 *acc, *outp;
         CA(upload(P->mem, &dcell, cell.data(), cell.size()), "nfff");
         CA(upload(P->mem, &dnstr, nstr.data(), nstr.size()), "nfff");
         CA(upload(P->mem, &dijk, ijk.data(), ijk.size()), "nfff");
         CA(upload(P->mem, &dface, face.data(), face.size()), "nfff");
-        CA(upload(P->mem, &dodt, odt.data(), odt.size()), "nfff");
-        CA(upload(P->mem, &dom, f.omega, (size_t)f.nfreq), "nfff");
         CA(upload(P->mem, &dpts, f.points, (size_t)3 * f.npoints), "nfff");
         std::vector<int32_t> ist(f.npoints);
         {
@@ -444,37 +453,97 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
             }
         }
         CA(upload(P->mem, &dist, ist.data(), ist.size()), "nfff");
-        const size_t nacc = (size_t)f.nfreq * 6 * cell.size();
-        CA(P->mem.alloc(&acc, nacc), "nfff accumulators");
-        P->snap.push_back({acc, nacc * sizeof(double2)});
-        CA(P->mem.alloc(&outp, (size_t)f.npoints * f.nfreq * 3), "nfff output");
         for (int s = 0; s < 2; s++) {
             const float **fp;
             CA(P->mem.alloc(&fp, 3), "field pointer table");
             CA(cudaMemcpy(fp, P->fields[s], sizeof(float *) * 3, cudaMemcpyHostToDevice), "field pointer table");
             P->d_efieldptrs[s] = fp;
         }
-        P->nf.ns = (int)cell.size();
-        P->nf.nfreq = f.nfreq;
-        P->nf.cell = dcell;
-        P->nf.nstride = dnstr;
-        P->nf.acc = acc;
-        P->nf.omega_dt = dodt;
-        P->nf.step = P->d_step;
-        P->nf.inv2dx = 1.0 / (2.0 * hp.dx);
-        P->ff.npoints = f.npoints;
-        P->ff.nfreq = f.nfreq;
-        P->ff.ns = (int)cell.size();
-        P->ff.points = dpts;
-        P->ff.istart = dist;
-        P->ff.cell_ijk = dijk;
-        P->ff.face = dface;
-        P->ff.acc = acc;
-        P->ff.omega = dom;
-        P->ff.dt = hp.dt;
-        P->ff.dx = hp.dx;
-        P->ff.out = outp;
-        bytes += (double)cell.size() * (9 * 4 + (double)f.nfreq * 6 * 16 * 2);
+        if (f.nfreq > 0) {
+            std::vector<double> odt(f.nfreq);
+            for (int q = 0; q < f.nfreq; q++) odt[q] = f.omega[q] * hp.dt;
+            double *dodt, *dom;
+            double2 *acc, *outp;
+            CA(upload(P->mem, &dodt, odt.data(), odt.size()), "nfff");
+            CA(upload(P->mem, &dom, f.omega, (size_t)f.nfreq), "nfff");
+            const size_t nacc = (size_t)f.nfreq * 6 * cell.size();
+            CA(P->mem.alloc(&acc, nacc), "nfff accumulators");
+            P->snap.push_back({acc, nacc * sizeof(double2)});
+            CA(P->mem.alloc(&outp, (size_t)f.npoints * f.nfreq * 3), "nfff output");
+            // exp(-i omega R dt) over every retarded index R the box can produce:
+            // R <= 1 + (largest point-to-box-corner distance) / (c dt)
+            double dmax = 0;
+            for (int q = 0; q < f.npoints; q++)
+                for (int corner = 0; corner < 8; corner++) {
+                    const double cx = (corner & 1) ? f.in : f.i0, cy = (corner & 2) ? f.jn : f.j0, cz = (corner & 4) ? f.kn : f.k0;
+                    const double ux = f.points[3 * q] - cx, uy = f.points[3 * q + 1] - cy, uz = f.points[3 * q + 2] - cz;
+                    dmax = std::max(dmax, std::sqrt(ux * ux + uy * uy + uz * uz));
+                }
+            const int ntw = (int)(1.0 + dmax * hp.dx / (C0 * hp.dt)) + 2;
+            std::vector<double2> tw((size_t)f.nfreq * ntw);
+            for (int q = 0; q < f.nfreq; q++)
+                for (int R = 0; R < ntw; R++) {
+                    const double ph = f.omega[q] * (double)R * hp.dt;
+                    tw[(size_t)q * ntw + R] = make_double2(std::cos(ph), -std::sin(ph));
+                }
+            double2 *dtw, *part;
+            CA(upload(P->mem, &dtw, tw.data(), tw.size()), "far-field twiddles");
+            int nsm = 148;
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+            const int ptiles = (f.npoints + 127) / 128;
+            int groups = (4 * nsm + ptiles - 1) / ptiles;
+            groups = std::max(1, std::min(groups, std::max(1, (int)cell.size() / 256)));
+            CA(P->mem.alloc(&part, (size_t)groups * f.npoints * f.nfreq * 3), "far-field partial sums");
+            P->nf.ns = (int)cell.size();
+            P->nf.nfreq = f.nfreq;
+            P->nf.cell = dcell;
+            P->nf.nstride = dnstr;
+            P->nf.acc = acc;
+            P->nf.omega_dt = dodt;
+            P->nf.step = P->d_step;
+            P->nf.inv2dx = 1.0 / (2.0 * hp.dx);
+            P->ff.npoints = f.npoints;
+            P->ff.nfreq = f.nfreq;
+            P->ff.ns = (int)cell.size();
+            P->ff.points = dpts;
+            P->ff.istart = dist;
+            P->ff.cell_ijk = dijk;
+            P->ff.face = dface;
+            P->ff.acc = acc;
+            P->ff.omega = dom;
+            P->ff.dt = hp.dt;
+            P->ff.dx = hp.dx;
+            P->ff.out = outp;
+            P->ff.ntw = ntw;
+            P->ff.tw = dtw;
+            P->ff.groups = groups;
+            P->ff.part = part;
+        }
+        if (f.series) {
+            // farfield.c:63-64
+            P->nfff_ndata = (int)(2000 + 2 * desc->nsteps +
+                                  std::sqrt((double)(hp.xr * hp.xr + hp.yr * hp.yr + hp.zr * hp.zr)) / (C0 * hp.dt / hp.dx));
+            const size_t nser = (size_t)f.npoints * 3 * P->nfff_ndata;
+            double *ser;
+            CA(P->mem.alloc(&ser, nser), "far-field series");
+            CA(cudaMemset(ser, 0, nser * sizeof(double)), "far-field series");
+            P->snap.push_back({ser, nser * sizeof(double)});
+            P->nfff_series = true;
+            P->ns.ns = (int)cell.size();
+            P->ns.npoints = f.npoints;
+            P->ns.ndata = P->nfff_ndata;
+            P->ns.cell = dcell;
+            P->ns.nstride = dnstr;
+            P->ns.cell_ijk = dijk;
+            P->ns.face = dface;
+            P->ns.points = dpts;
+            P->ns.istart = dist;
+            P->ns.series = ser;
+            P->ns.step = P->d_step;
+            P->ns.dx = hp.dx;
+            P->ns.dt = hp.dt;
+        }
+        if (f.nfreq > 0) bytes += (double)cell.size() * (9 * 4 + (double)f.nfreq * 6 * 16 * 2);
     }
     // work decomposition: the bulk box (outside every CPML slab, one extra
     // plane on the low sides so that its halo row/column/plane is slab-free)
@@ -527,7 +596,7 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
         }
         if (nblk > 0x7fffffffLL) return bail(cudaErrorInvalidValue, "grid too large for the slab kernels");
         {   // algorithmic bytes per launch: 24 B field reads + 24 B writes + 1 class byte per cell;
-            // (3 + 4 * poles) state arrays x (4 B read + 4 B write) per dispersive field component;
+            // 12 B (Q read + write, E^{n-1} read) + 16 B per pole per dispersive field component;
             // 4 psi arrays x (4 B read + 4 B write) per CPML cell (slab kernels only)
             auto cell_bytes = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
                 double b = 0;
@@ -539,7 +608,7 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
                             b += 49.0;
                             if (c.flags & CF_ADE_BRANCH)
                                 b += (((c.flags & CF_ADE_X) ? 1 : 0) + ((c.flags & CF_ADE_Y) ? 1 : 0) + ((c.flags & CF_ADE_Z) ? 1 : 0)) *
-                                     (3 + 4 * hp.maxpoles) * 8.0;
+                                     (12.0 + 16.0 * hp.maxpoles);
                         }
                 return b;
             };
@@ -825,11 +894,7 @@ int fdtd_step_timed(fdtd_plan *P, int nsteps, double *fused_ms, int *fused_launc
         int rc = launch_fused(P, in, P->stream);
         CK(cudaEventRecord(ev[2 * s + 1], P->stream));
         if (rc != FDTD_OK) return rc;
-        if (P->nfff) {
-            DevNfff n = P->nf;
-            n.e = P->d_efieldptrs[1 - in];
-            launch_nfff_accumulate(n, P->stream);
-        }
+        launch_nfff(P, in, P->stream);
         P->cur = 1 - in;
         P->host_step++;
     }
@@ -873,11 +938,7 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
         cudaError_t e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
         CK(cudaEventRecord(E[3], st));
-        if (P->nfff) {
-            DevNfff n = P->nf;
-            n.e = P->d_efieldptrs[1 - in];
-            launch_nfff_accumulate(n, st);
-        }
+        launch_nfff(P, in, st);
         CK(cudaEventRecord(E[4], st));
         P->cur = 1 - in;
         P->host_step++;
@@ -903,7 +964,7 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
     out[4] = aux;
     out[5] = nf;
     out[6] = tot;
-    out[7] = 1 + (P->tsf_cells ? 1 : 0) + (P->bulk_on ? 1 : 0) + 2 + (P->nfff ? 1 : 0);
+    out[7] = 1 + (P->tsf_cells ? 1 : 0) + (P->bulk_on ? 1 : 0) + 2 + (P->nfff_nfreq > 0 ? 1 : 0) + (P->nfff_series ? 1 : 0);
     return FDTD_OK;
 }
 
@@ -922,13 +983,33 @@ int fdtd_get_probes(fdtd_plan *P, double *out, size_t out_len)
 int fdtd_nfff_spectrum(fdtd_plan *P, double *out, size_t out_len)
 {
     if (!P || !out) return fail(FDTD_E_INVALID, "NULL argument");
-    if (!P->nfff) return fail(FDTD_E_STATE, "the plan has no NFFF box / frequencies");
+    if (!P->nfff || P->nfff_nfreq <= 0) return fail(FDTD_E_STATE, "the plan has no NFFF box / frequencies");
     size_t need = (size_t)P->nfff_npoints * P->nfff_nfreq * 3 * 2;
     if (out_len < need) return fail(FDTD_E_INVALID, "spectrum buffer too small");
     CK(cudaSetDevice(P->device));
     launch_farfield_finalize(P->ff, P->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, P->ff.out, need * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+    CK(cudaStreamSynchronize(P->stream));
+    return FDTD_OK;
+}
+
+int fdtd_nfff_ndata(const fdtd_plan *P, int *ndata)
+{
+    if (!P || !ndata) return fail(FDTD_E_INVALID, "NULL argument");
+    if (!P->nfff_series) return fail(FDTD_E_STATE, "the plan was created without nfff.series");
+    *ndata = P->nfff_ndata;
+    return FDTD_OK;
+}
+
+int fdtd_nfff_series(fdtd_plan *P, double *out, size_t out_len)
+{
+    if (!P || !out) return fail(FDTD_E_INVALID, "NULL argument");
+    if (!P->nfff_series) return fail(FDTD_E_STATE, "the plan was created without nfff.series");
+    const size_t need = (size_t)P->nfff_npoints * 3 * P->nfff_ndata;
+    if (out_len < need) return fail(FDTD_E_INVALID, "series buffer too small");
+    CK(cudaSetDevice(P->device));
+    CK(cudaMemcpyAsync(out, P->ns.series, need * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
     CK(cudaStreamSynchronize(P->stream));
     return FDTD_OK;
 }

@@ -220,23 +220,23 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
                     for (int a = 0; a < 3; a++) {
                         if (!(fl & cm[a])) continue;
                         const float eo = e[r][a];
-                        const float dp = P.dp[a][c], dpp = P.dpp[a][c], ep = P.ep[a][c];
-                        float p[2] = {0.f, 0.f}, pp[2] = {0.f, 0.f};
-                        for (int n = 0; n < NPOLES; n++) { p[n] = P.p_[a][n][c]; pp[n] = P.pp_[a][n][c]; }
+                        // difference-form state (DevAde); E^{n-1} is the output set before this step writes it
+                        const float qd = P.q[a][c], ep = P.fout[a][c];
+                        float pc[2] = {0.f, 0.f}, qc[2] = {0.f, 0.f};
+                        for (int n = 0; n < NPOLES; n++) { pc[n] = P.pc[a][n][c]; qc[n] = P.qc[a][n][c]; }
                         float v = eo;
                         if (gd[a]) {
-                            v = A.c0dx * curl[a] + A.c1 * (-A.a0 * dpp + A.one_m_a1 * dp);
-                            for (int n = 0; n < NPOLES; n++) v += A.c1 * (-A.bp0[n] * pp[n] + A.one_m_bp1[n] * p[n]);
+                            v = A.c0dx * curl[a] + A.qe * qd;
+                            for (int n = 0; n < NPOLES; n++) v += A.qpe[n] * qc[n] + A.pe[n] * pc[n];
                             v += A.c2 * ep + A.c3 * eo;
                         }
                         ne[a] = v;
-                        P.dp[a][c] = A.a0 * dpp + A.a1 * dp + A.a2 * (ep + 2.f * eo + v);
+                        P.q[a][c] = A.ma0 * qd + A.a2 * (ep + 2.f * eo + v);
                         for (int n = 0; n < NPOLES; n++) {
-                            P.p_[a][n][c] = A.bp0[n] * pp[n] + A.bp1[n] * p[n] + A.bp2[n] * ep + A.bp3[n] * eo + A.bp4[n] * v;
-                            P.pp_[a][n][c] = p[n];
+                            const float qn = A.rp[n] * pc[n] + A.rq[n] * qc[n] + A.bp2[n] * ep + A.bp3[n] * eo + A.bp4[n] * v;
+                            P.qc[a][n][c] = qn;
+                            P.pc[a][n][c] = pc[n] + qn;
                         }
-                        P.ep[a][c] = eo;
-                        P.dpp[a][c] = dp;
                     }
                     if (gx && !(fl & CF_ADE_X)) ne[0] = c0.x * nx + c1.x * curlx;
                     if (gy && !(fl & CF_ADE_Y)) ne[1] = c0.y * ny + c1.y * curly;

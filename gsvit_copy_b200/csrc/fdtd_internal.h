@@ -44,12 +44,27 @@ struct alignas(16) DevClass {
     float pad1;
 };
 
-struct DevAde {      // calculate_ade_a/bp/c (plan.c:2737-2763), rounded to float
-    float c0dx;      // ade_c0 / dx
-    float c1, c2, c3;
-    float a0, a1, a2, one_m_a1;
-    float bp0[2], bp1[2], bp2[2], bp3[2], bp4[2];
-    float one_m_bp1[2];
+// ADE coefficients of calculate_ade_a/bp/c (plan.c:2737-2763), recast for the
+// difference form of the polarisation state: per component the kernels keep
+// Q = P_D^n - P_D^{n-1} and, per critical-point pole, p = P_cp^n and
+// q = P_cp^n - P_cp^{n-1}; E^{n-1} is the output field set before it is
+// overwritten.  The reference's
+//   E^{n+1} = c0 curl + c1 (-a0 P^{n-1} + (1-a1) P^n) + ... + c2 E^{n-1} + c3 E^n,
+//   P^{n+1} = a0 P^{n-1} + a1 P^n + a2 (E^{n-1} + 2 E^n + E^{n+1})
+// becomes, with a0 + a1 = 1 exactly,
+//   E^{n+1} = c0 curl + c1 a0 Q + sum_p [c1 bp0 q + c1 (1 - bp0 - bp1) p] + c2 E^{n-1} + c3 E^n,
+//   Q' = -a0 Q + a2 (E^{n-1} + 2 E^n + E^{n+1}),
+//   q' = (bp0 + bp1 - 1) p - bp0 q + bp2 E^{n-1} + bp3 E^n + bp4 E^{n+1},  p' = p + q'.
+// The same recursion, but FP32 no longer subtracts two nearly equal P values
+// (P grows like the time integral of Q), so it tracks the FP64 reference.
+struct DevAde {
+    float c0dx;          // ade_c0 / dx
+    float c2, c3;
+    float qe;            // c1 * a0
+    float ma0, a2;       // Q recursion
+    float pe[2], qpe[2]; // c1 (1 - bp0 - bp1), c1 bp0
+    float rp[2], rq[2];  // q recursion: bp0 + bp1 - 1, -bp0
+    float bp2[2], bp3[2], bp4[2];
 };
 
 struct DevPlan {
@@ -66,8 +81,8 @@ struct DevPlan {
     // ADE
     int nade;
     const DevAde *ade;
-    float *ep[3], *dp[3], *dpp[3];
-    float *pp_[3][2], *p_[3][2];
+    float *q[3];                    // Drude current Q per component
+    float *pc[3][2], *qc[3][2];     // critical-point poles: p and q per component
     // CPML: face order x0 xn y0 yn z0 zn
     int cp_on[6], cp_d[6];
     const float *be[6], *ce[6], *bh[6], *ch[6];

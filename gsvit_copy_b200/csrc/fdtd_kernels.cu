@@ -184,19 +184,20 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
     if (ADE && (fl & CF_ADE_BRANCH)) {
         const DevAde &A = P.ade[ade_set];
         const bool comp[3] = {(fl & CF_ADE_X) != 0, (fl & CF_ADE_Y) != 0, (fl & CF_ADE_Z) != 0};
-        float dp[3] = {0, 0, 0}, dpp[3] = {0, 0, 0}, ep[3] = {0, 0, 0}, p[3][2], pp[3][2];
+        // difference-form state (see DevAde); E^{n-1} is the output set before this write
+        float qd[3] = {0, 0, 0}, ep[3] = {0, 0, 0}, pc[3][2], qc[3][2];
         for (int a = 0; a < 3; a++) {
             if (!comp[a]) continue;
-            dp[a] = P.dp[a][c]; dpp[a] = P.dpp[a][c]; ep[a] = P.ep[a][c];
-            for (int n = 0; n < NPOLES; n++) { p[a][n] = P.p_[a][n][c]; pp[a][n] = P.pp_[a][n][c]; }
+            qd[a] = P.q[a][c]; ep[a] = P.fout[a][c];
+            for (int n = 0; n < NPOLES; n++) { pc[a][n] = P.pc[a][n][c]; qc[a][n] = P.qc[a][n][c]; }
         }
         const float curl[3] = {curlx, curly, curlz};
         const bool gd[3] = {gx, gy, gz};
         float ne[3] = {nx, ny, nz};
         for (int a = 0; a < 3; a++) {
             if (!(comp[a] && gd[a])) continue;
-            float v = A.c0dx * curl[a] + A.c1 * (-A.a0 * dpp[a] + A.one_m_a1 * dp[a]);
-            for (int n = 0; n < NPOLES; n++) v += A.c1 * (-A.bp0[n] * pp[a][n] + A.one_m_bp1[n] * p[a][n]);
+            float v = A.c0dx * curl[a] + A.qe * qd[a];
+            for (int n = 0; n < NPOLES; n++) v += A.qpe[n] * qc[a][n] + A.pe[n] * pc[a][n];
             v += A.c2 * ep[a] + A.c3 * eo[a];
             ne[a] = v;
         }
@@ -248,13 +249,12 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
         for (int a = 0; a < 3; a++) {   // polarisation recursions of the owned components
             if (!comp[a]) continue;
             const float e1 = ne[a];
-            P.dp[a][c] = A.a0 * dpp[a] + A.a1 * dp[a] + A.a2 * (ep[a] + 2.f * eo[a] + e1);
+            P.q[a][c] = A.ma0 * qd[a] + A.a2 * (ep[a] + 2.f * eo[a] + e1);
             for (int n = 0; n < NPOLES; n++) {
-                P.p_[a][n][c] = A.bp0[n] * pp[a][n] + A.bp1[n] * p[a][n] + A.bp2[n] * ep[a] + A.bp3[n] * eo[a] + A.bp4[n] * e1;
-                P.pp_[a][n][c] = p[a][n];
+                const float qn = A.rp[n] * pc[a][n] + A.rq[n] * qc[a][n] + A.bp2[n] * ep[a] + A.bp3[n] * eo[a] + A.bp4[n] * e1;
+                P.qc[a][n][c] = qn;
+                P.pc[a][n][c] = pc[a][n] + qn;
             }
-            P.ep[a][c] = eo[a];
-            P.dpp[a][c] = dp[a];
         }
         nx = ne[0]; ny = ne[1]; nz = ne[2];
     }
@@ -565,70 +565,160 @@ __global__ void nfff_accumulate_kernel(const DevNfff N)
 
 // ------------------------------------------------------------ far-field integration
 
-// F_hat_n(omega) = sum_s A_s exp(-i omega (1 + R_ns - istart_n) dt) *
+// F_hat_n(omega) = sum_s A_s exp(-i omega (R_ns - istart_n) dt) *
 //   [(-c' + b e^{i omega dt} + c' e^{2 i omega dt}) Ehat_s + sgn_f a e^{i omega dt} Dhat_s]
-// with r, cos(theta), a, b, c, R of farfield.c:175-405 (the DFT of the
-// reference time-domain series).  One block per (point, frequency).
-__global__ void farfield_finalize_kernel(const DevFarfield F)
+// with r, cos(theta), a, b, c and the retarded index R = (int)(1 + r/(c dt)) of
+// farfield.c:175-405: the DFT of the reference time-domain series.
+//
+// Tiled over (far points x surface-cell groups): a CTA owns 128 far points
+// (one per thread) and one group of surface cells, staged 32 at a time in
+// shared memory with their accumulators for NF frequencies (read once per
+// CTA instead of once per point).  exp(-i omega R dt) comes from a table over
+// R; exp(+i omega istart dt), the face area and the sum over groups are
+// applied by farfield_reduce_kernel.  FP64 throughout.
+template <int NF>
+__global__ void __launch_bounds__(128) farfield_partial_kernel(const DevFarfield F, int f0)
 {
-    const int pf = blockIdx.x;
-    const int p = pf / F.nfreq, f = pf % F.nfreq;
-    const double x = F.points[3 * p], y = F.points[3 * p + 1], z = F.points[3 * p + 2];
-    const double om = F.omega[f], dt = F.dt, dx = F.dx;
+    constexpr int CH = 32;
+    __shared__ double2 sacc[CH][NF][6];
+    __shared__ int4 sgeo[CH];
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = p < F.npoints;
+    const int per = (F.ns + F.groups - 1) / F.groups;
+    const int s0 = blockIdx.y * per, s1 = min(F.ns, s0 + per);
     const double C0 = 299792458.0, PI = 3.14159265358979323846;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    double sw, cw, s2, c2;
-    sincos(om * dt, &sw, &cw);
-    sincos(2.0 * om * dt, &s2, &c2);
-    for (int s = threadIdx.x; s < F.ns; s += blockDim.x) {
-        const int fc = F.face[s];
-        const double ci = F.cell_ijk[3 * s], cj = F.cell_ijk[3 * s + 1], ck = F.cell_ijk[3 * s + 2];
-        const double rx = x - ci, ry = y - cj, rz = z - ck;
-        const double rc = sqrt(rx * rx + ry * ry + rz * rz);
-        // angle(): normal of the face (farfield.c:44-54)
-        double dot;
-        if (fc == 0) dot = -rx; else if (fc == 1) dot = rx; else if (fc == 2) dot = -ry;
-        else if (fc == 3) dot = ry; else if (fc == 4) dot = -rz; else dot = rz;
-        const double ct = dot / sqrt((rx * rx + ry * ry + rz * rz) * 1.0);
-        const double area = dx * dx;
-        const double r = rc * dx;
-        const int R = (int)(1.0 + r / (C0 * dt));
-        const double a = 1.0 / (4.0 * PI * r);
-        const double b = -1.0 / (4.0 * PI) * ct / (r * r);
-        const double cc = -1.0 / (4.0 * PI) * ct / (C0 * r);
-        const double cp = cc / 2.0 / dt;
-        const double sg = (fc & 1) ? 1.0 : -1.0;
-        // K = -c' + b e^{i w dt} + c' e^{2 i w dt};  L = sg * a * e^{i w dt}
-        const double Kr = -cp + b * cw + cp * c2, Ki = b * sw + cp * s2;
-        const double Lr = sg * a * cw, Li = sg * a * sw;
-        double ph_s, ph_c;
-        sincos(-om * (double)(R - F.istart[p]) * dt, &ph_s, &ph_c);
-        for (int q = 0; q < 3; q++) {
-            const double2 Eh = F.acc[((size_t)f * 6 + q) * F.ns + s];
-            const double2 Dh = F.acc[((size_t)f * 6 + 3 + q) * F.ns + s];
-            const double tr = Kr * Eh.x - Ki * Eh.y + Lr * Dh.x - Li * Dh.y;
-            const double ti = Kr * Eh.y + Ki * Eh.x + Lr * Dh.y + Li * Dh.x;
-            acc[2 * q] += area * (ph_c * tr - ph_s * ti);
-            acc[2 * q + 1] += area * (ph_c * ti + ph_s * tr);
+    const double dt = F.dt, dx = F.dx, c0dt = C0 * dt;
+    double x = 0, y = 0, z = 0;
+    if (live) { x = F.points[3 * p]; y = F.points[3 * p + 1]; z = F.points[3 * p + 2]; }
+    double cw[NF], sw[NF], c2[NF], s2[NF];
+    for (int f = 0; f < NF; f++) {
+        const double om = F.omega[f0 + f];
+        sincos(om * dt, &sw[f], &cw[f]);
+        sincos(2.0 * om * dt, &s2[f], &c2[f]);
+    }
+    double acc[NF][3][2];
+    for (int f = 0; f < NF; f++)
+        for (int q = 0; q < 3; q++) acc[f][q][0] = acc[f][q][1] = 0.0;
+    for (int base = s0; base < s1; base += CH) {
+        const int n = min(CH, s1 - base);
+        __syncthreads();
+        for (int q = threadIdx.x; q < n; q += blockDim.x)
+            sgeo[q] = make_int4(F.cell_ijk[3 * (base + q)], F.cell_ijk[3 * (base + q) + 1], F.cell_ijk[3 * (base + q) + 2],
+                                F.face[base + q]);
+        for (int t = threadIdx.x; t < n * NF * 6; t += blockDim.x) {
+            const int q = t % n, fq = t / n;
+            sacc[q][fq / 6][fq % 6] = F.acc[((size_t)(f0 + fq / 6) * 6 + fq % 6) * F.ns + base + q];
+        }
+        __syncthreads();
+        if (!live) continue;
+        for (int q = 0; q < n; q++) {
+            const int4 g = sgeo[q];
+            const double rx = x - g.x, ry = y - g.y, rz = z - g.z;
+            const double rc = sqrt(rx * rx + ry * ry + rz * rz);
+            double dot;   // angle(): normal of the face (farfield.c:44-54)
+            switch (g.w) {
+            case 0: dot = -rx; break;
+            case 1: dot = rx; break;
+            case 2: dot = -ry; break;
+            case 3: dot = ry; break;
+            case 4: dot = -rz; break;
+            default: dot = rz; break;
+            }
+            const double ct = dot / rc;
+            const double r = rc * dx;
+            const int R = min((int)(1.0 + r / c0dt), F.ntw - 1);
+            const double ir = 1.0 / r;
+            const double a = ir / (4.0 * PI);
+            const double b = -ct / (4.0 * PI) * ir * ir;
+            const double cp = -ct / (4.0 * PI * C0) * ir / (2.0 * dt);
+            const double sg = (g.w & 1) ? 1.0 : -1.0;
+            for (int f = 0; f < NF; f++) {
+                const double2 w = F.tw[(size_t)(f0 + f) * F.ntw + R];
+                const double Kr = -cp + b * cw[f] + cp * c2[f], Ki = b * sw[f] + cp * s2[f];
+                const double Lr = sg * a * cw[f], Li = sg * a * sw[f];
+                for (int c = 0; c < 3; c++) {
+                    const double2 Eh = sacc[q][f][c], Dh = sacc[q][f][3 + c];
+                    const double tr = Kr * Eh.x - Ki * Eh.y + Lr * Dh.x - Li * Dh.y;
+                    const double ti = Kr * Eh.y + Ki * Eh.x + Lr * Dh.y + Li * Dh.x;
+                    acc[f][c][0] += w.x * tr - w.y * ti;
+                    acc[f][c][1] += w.x * ti + w.y * tr;
+                }
+            }
         }
     }
-    // block reduction: warp shuffles then shared memory
-    __shared__ double red[32][6];
-    for (int q = 0; q < 6; q++)
-        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0)
-        for (int q = 0; q < 6; q++) red[warp][q] = acc[q];
-    __syncthreads();
-    if (warp == 0) {
-        const int nw = blockDim.x >> 5;
-        for (int q = 0; q < 6; q++) {
-            double v = lane < nw ? red[lane][q] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0) acc[q] = v;
+    if (live)
+        for (int f = 0; f < NF; f++)
+            for (int c = 0; c < 3; c++)
+                F.part[(((size_t)blockIdx.y * F.npoints + p) * F.nfreq + f0 + f) * 3 + c] = make_double2(acc[f][c][0], acc[f][c][1]);
+}
+
+// out = area * exp(+i omega istart dt) * sum over groups (fixed order)
+__global__ void farfield_reduce_kernel(const DevFarfield F)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= F.npoints * F.nfreq * 3) return;
+    const int p = t / (F.nfreq * 3), f = (t / 3) % F.nfreq;
+    double re = 0, im = 0;
+    for (int g = 0; g < F.groups; g++) {
+        const double2 v = F.part[(size_t)g * F.npoints * F.nfreq * 3 + t];
+        re += v.x;
+        im += v.y;
+    }
+    double sn, cs;
+    sincos(F.omega[f] * (double)F.istart[p] * F.dt, &sn, &cs);
+    const double area = F.dx * F.dx;
+    F.out[t] = make_double2(area * (cs * re - sn * im), area * (cs * im + sn * re));
+}
+
+// The reference's far-field series, farfield.c:207-404, for every (surface
+// cell, far point): r and cos(theta) as dist()/angle() (farfield.c:33-56),
+// nn = (int)(step + 1 + r/(c dt)) - istart with the reference's operation
+// order (the sum can round across an integer, so nn is formed exactly as
+// there), three taps per component when 3 <= nn < ndata.  FP64 atomics.
+__global__ void nfff_series_kernel(const DevNfffSeries S)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S.ns) return;
+    const int step = *S.step - 1;
+    const double C0 = 299792458.0, PI = 3.14159265358979323846;
+    const double dx = S.dx, dt = S.dt;
+    const int fc = S.face[s];
+    const double ci = S.cell_ijk[3 * s], cj = S.cell_ijk[3 * s + 1], ck = S.cell_ijk[3 * s + 2];
+    const int64_t cc = S.cell[s], st = S.nstride[s];
+    double ev[3], dv[3];
+    for (int a = 0; a < 3; a++) {
+        const float *E = S.e[a];
+        ev[a] = (double)E[cc];
+        dv[a] = (double)E[cc + st] - (double)E[cc - st];
+    }
+    const double size = __dmul_rn(dx, dx);
+    const double pos = (fc & 1) ? 1.0 : -1.0;
+    for (int p = blockIdx.y; p < S.npoints; p += gridDim.y) {
+        const double x = S.points[3 * p], y = S.points[3 * p + 1], z = S.points[3 * p + 2];
+        const double ux = x - ci, uy = y - cj, uz = z - ck;
+        const double rc = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy)), __dmul_rn(uz, uz)));
+        double dot;
+        switch (fc) {
+        case 0: dot = -ux; break;
+        case 1: dot = ux; break;
+        case 2: dot = -uy; break;
+        case 3: dot = uy; break;
+        case 4: dot = -uz; break;
+        default: dot = uz; break;
         }
-        if (lane == 0)
-            for (int q = 0; q < 3; q++) F.out[((size_t)p * F.nfreq + f) * 3 + q] = make_double2(acc[2 * q], acc[2 * q + 1]);
+        const double ct = dot / rc;
+        const double r = __dmul_rn(rc, dx);
+        const int nn = (int)__dadd_rn((double)(step + 1), __ddiv_rn(r, __dmul_rn(C0, dt))) - S.istart[p];
+        if (nn < 3 || nn >= S.ndata) continue;
+        const double a1 = 1.0 / (4.0 * PI * r);
+        const double b1 = -1.0 / (4.0 * PI) * ct / (r * r);
+        const double c1 = -1.0 / (4.0 * PI) * ct / (C0 * r);
+        for (int a = 0; a < 3; a++) {
+            double *F = S.series + ((size_t)p * 3 + a) * S.ndata;
+            atomicAdd(F + nn, -c1 / 2.0 / dt * ev[a] * size);
+            atomicAdd(F + nn - 1, (pos * a1 * dv[a] / 2.0 / dx + b1 * ev[a]) * size);
+            atomicAdd(F + nn - 2, c1 / 2.0 / dt * ev[a] * size);
+        }
     }
 }
 
@@ -666,5 +756,22 @@ void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st)
 void launch_farfield_finalize(const DevFarfield &f, cudaStream_t st)
 {
     if (f.npoints <= 0 || f.nfreq <= 0) return;
-    farfield_finalize_kernel<<<f.npoints * f.nfreq, 256, 0, st>>>(f);
+    const dim3 grid((f.npoints + 127) / 128, f.groups);
+    for (int f0 = 0; f0 < f.nfreq; f0 += 4) {
+        switch (f.nfreq - f0) {
+        case 1: farfield_partial_kernel<1><<<grid, 128, 0, st>>>(f, f0); break;
+        case 2: farfield_partial_kernel<2><<<grid, 128, 0, st>>>(f, f0); break;
+        case 3: farfield_partial_kernel<3><<<grid, 128, 0, st>>>(f, f0); break;
+        default: farfield_partial_kernel<4><<<grid, 128, 0, st>>>(f, f0); break;
+        }
+    }
+    const int nt = f.npoints * f.nfreq * 3;
+    farfield_reduce_kernel<<<(nt + 255) / 256, 256, 0, st>>>(f);
+}
+
+void launch_nfff_series(const DevNfffSeries &s, cudaStream_t st)
+{
+    if (s.ns <= 0 || s.npoints <= 0) return;
+    const dim3 grid((s.ns + 255) / 256, (unsigned)min(s.npoints, 65535));
+    nfff_series_kernel<<<grid, 256, 0, st>>>(s);
 }

@@ -58,5 +58,28 @@ struct DevFarfield {
     const double *omega;        // nfreq
     double dt, dx;
     double2 *out;               // [(p*nfreq + f)*3 + c]
+    // tiled finalize
+    int ntw;                    // twiddle entries per frequency
+    const double2 *tw;          // [f*ntw + R] = exp(-i omega R dt)
+    int groups;                 // surface-cell groups of the partial sums
+    double2 *part;              // [((g*npoints + p)*nfreq + f)*3 + c] (scratch)
 };
+
+// The reference's own time-domain far-field series (farfield.c:175-405),
+// accumulated exactly: three taps per (surface cell, far point) and step.
+struct DevNfffSeries {
+    int ns, npoints, ndata;
+    const int32_t *cell;        // linear index of the surface cell
+    const int32_t *nstride;     // +/- stride along the face normal
+    const int32_t *cell_ijk;    // 3*ns
+    const int8_t *face;         // ns
+    const int32_t *points;      // 3*npoints
+    const int32_t *istart;      // npoints
+    const float *const *e;      // 3 E field pointers (the set written by this step)
+    double *series;             // [(p*3 + c)*ndata + m]
+    const int *step;            // device step counter (already advanced)
+    double dx, dt;
+};
+void launch_nfff_series(const DevNfffSeries &s, cudaStream_t st);
+
 void launch_farfield_finalize(const DevFarfield &f, cudaStream_t st);

@@ -322,13 +322,16 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
         DevAde a;
         std::memset(&a, 0, sizeof(a));
         a.c0dx = (float)(q.ade_c0 / dx);
-        a.c1 = (float)q.ade_c1; a.c2 = (float)q.ade_c2; a.c3 = (float)q.ade_c3;
-        a.a0 = (float)q.ade_a0; a.a1 = (float)q.ade_a1; a.a2 = (float)q.ade_a2;
-        a.one_m_a1 = (float)(1 - q.ade_a1);
+        a.c2 = (float)q.ade_c2; a.c3 = (float)q.ade_c3;
+        a.qe = (float)(q.ade_c1 * q.ade_a0);
+        a.ma0 = (float)(-q.ade_a0);
+        a.a2 = (float)q.ade_a2;
         for (int p = 0; p < 2; p++) {
-            a.bp0[p] = (float)q.ade_bp0[p]; a.bp1[p] = (float)q.ade_bp1[p]; a.bp2[p] = (float)q.ade_bp2[p];
-            a.bp3[p] = (float)q.ade_bp3[p]; a.bp4[p] = (float)q.ade_bp4[p];
-            a.one_m_bp1[p] = (float)(1 - q.ade_bp1[p]);
+            a.pe[p] = (float)(q.ade_c1 * ((1.0 - q.ade_bp0[p]) - q.ade_bp1[p]));
+            a.qpe[p] = (float)(q.ade_c1 * q.ade_bp0[p]);
+            a.rp[p] = (float)((q.ade_bp0[p] + q.ade_bp1[p]) - 1.0);
+            a.rq[p] = (float)(-q.ade_bp0[p]);
+            a.bp2[p] = (float)q.ade_bp2[p]; a.bp3[p] = (float)q.ade_bp3[p]; a.bp4[p] = (float)q.ade_bp4[p];
             if (q.ade_bp2[p] != 0 || q.ade_bp3[p] != 0 || q.ade_bp4[p] != 0) hp->maxpoles = 2;
         }
         ade_slot[m] = (int)hp->ades.size();

@@ -324,6 +324,7 @@ class Scene:
                 ist = np.ascontiguousarray(f["istart"], dtype=np.int32)
                 keep.append(ist)
                 d.nfff.istart = abi.as_ptr(ist, C.c_int32)
+            d.nfff.series = 1 if f.get("series") else 0
             om = np.ascontiguousarray(f.get("omega", np.zeros(0)), dtype=np.float64)
             keep.append(om)
             d.nfff.nfreq = len(om)

@@ -106,6 +106,16 @@ class Solver:
                   "fdtd_nfff_spectrum")
         return out[..., 0] + 1j * out[..., 1]
 
+    def nfff_series(self) -> np.ndarray:
+        """Time-domain far-field series (npoints, 3, ndata) of a plan with nfff["series"]."""
+        nd = C.c_int()
+        abi.check(self.lib.fdtd_nfff_ndata(self.h, C.byref(nd)), "fdtd_nfff_ndata")
+        npt = len(self.scene.nfff["points"])
+        out = np.zeros((npt, 3, nd.value))
+        abi.check(self.lib.fdtd_nfff_series(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), out.size),
+                  "fdtd_nfff_series")
+        return out
+
     def map(self, which: int) -> np.ndarray:
         out = np.empty(self.shape, dtype=np.int32)
         abi.check(self.lib.fdtd_get_map(self.h, which, out.ctypes.data_as(C.POINTER(C.c_int32)), out.size),

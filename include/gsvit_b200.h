@@ -144,7 +144,12 @@ typedef struct fdtd_nfff {
     int32_t skip_lo[6][2];              /* per face: min of the 2 tangential indices */
     int32_t skip_hi[6][2];              /* per face: max of the 2 tangential indices */
     int32_t npoints;
-    int32_t nfreq;
+    int32_t nfreq;                      /* running-DFT frequencies (0 = none)  */
+    int32_t series;                     /* 1 = also accumulate the reference's
+                                         * time-domain series (farfield.c:175-405)
+                                         * exactly: cost O(npoints x surface) per
+                                         * step, meant for few far points      */
+    int32_t reserved;
     const int32_t *points;              /* 3*npoints far-point cells (ri,rj,rk) */
     const int32_t *istart;              /* npoints; NULL = farfield.c:76-91 rule */
     const double *omega;                /* nfreq angular frequencies (rad/s)  */
@@ -264,6 +269,14 @@ int fdtd_get_probes(fdtd_plan *plan, double *out, size_t out_len);
  * time-domain far-field series F_c of farfield.c:175-405 (c = x,y,z),
  * out[((p*nfreq + f)*3 + c)*2 + {0,1}] = {re, im}. */
 int fdtd_nfff_spectrum(fdtd_plan *plan, double *out, size_t out_len);
+
+/* Length of the time-domain far-field series of a plan created with
+ * nfff.series = 1: ndata = 2000 + 2*nsteps + |res|/(c dt/dx) (farfield.c:63-64). */
+int fdtd_nfff_ndata(const fdtd_plan *plan, int *ndata);
+
+/* The time-domain far-field series itself (rpoints[n].ex/ey/ez->data of
+ * farfield.c), FP64: out[(p*3 + c)*ndata + m]. */
+int fdtd_nfff_series(fdtd_plan *plan, double *out, size_t out_len);
 
 /* Read back a derived integer map (FDTD_MAP_*) as N int32 values. */
 int fdtd_get_map(fdtd_plan *plan, int which, int32_t *out, size_t out_len);

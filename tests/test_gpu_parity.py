@@ -66,6 +66,22 @@ def test_tsf_driven_parity_and_farfield(kind):
     assert rel_l2(spec, ref) < TOL, rel_l2(spec, ref)
 
 
+@pytest.mark.parametrize("kind", KINDS)
+def test_farfield_series_mode(kind):
+    """nfff.series: the reference's time-domain far-field series, exactly as
+    farfield.c forms it, beside the running DFT of the same run."""
+    s = plan.small_scene(kind, nsteps=200)
+    s.nfff["series"] = True
+    g, o = _pair(s)
+    g.step(200)
+    o.step(200)
+    ser, ref = g.nfff_series(), o.nfff_series()
+    assert ser.shape == ref.shape
+    assert rel_l2(ser, ref) < TOL, rel_l2(ser, ref)
+    spec = g.nfff_spectrum()
+    assert rel_l2(spec, series_spectrum(ref, s.nfff["omega"], s.dt)) < TOL
+
+
 def test_graph_matches_eager_bitwise():
     s = plan.small_scene("full", nsteps=64)
     a = Solver(s)
