@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
     float4 *scls = reinterpret_cast<float4 *>(smem + S * STAGE);
     float *hrow = reinterpret_cast<float *>(smem + S * STAGE + P.nclasses * 64);        // [8][2][32]
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S * STAGE + P.nclasses * 64 + 8 * 2 * 32 * 4);
+    DevAde *sade = reinterpret_cast<DevAde *>(smem + S * STAGE + P.nclasses * 64 + 8 * 2 * 32 * 4 + S * 8);
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const BulkItem it = items[blockIdx.x];
@@ -107,6 +108,9 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
     const int plast = min(ie, xr - 1);                        // last plane whose data is needed
 
     for (int q = tid; q < P.nclasses * 4; q += NTH) scls[q] = reinterpret_cast<const float4 *>(P.classes)[q];
+    if (ADE)
+        for (int q = tid; q < P.nade * (int)(sizeof(DevAde) / 4); q += NTH)
+            reinterpret_cast<float *>(sade)[q] = reinterpret_cast<const float *>(P.ade)[q];
     if (tid == 0) {
         for (int s = 0; s < S; s++) bar_init(&bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -159,6 +163,23 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
         const float *EY1 = ebox(st1, 1), *EZ1 = ebox(st1, 2);
         const bool prologue = (i < ib);
         const bool il = (i == xr - 1);
+        // Drude state of this plane's own cells (Q and E^{n-1}), requested before
+        // the H phase so that the loads overlap it
+        float aq[4][3], aep[4][3];
+        if (ADE && NPOLES == 0) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const unsigned fl = (!prologue && own[r]) ? __float_as_uint(scls[CL[(4 * w + r) * BWC + ce8] * 4].w) : 0u;
+                const int64_t c = (int64_t)i * si + (int64_t)jr[r] * sj + k;
+                const unsigned cm[3] = {CF_ADE_X, CF_ADE_Y, CF_ADE_Z};
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    const bool need = (fl & CF_ADE_BRANCH) && (fl & cm[a]);
+                    aq[r][a] = need ? P.q[a][c] : 0.f;
+                    aep[r][a] = need ? P.fout[a][c] : 0.f;
+                }
+            }
+        }
         // ---- H phase: 4 cells per thread
         for (int r = 0; r < 4; r++) {
             const int rr = 4 * w + r, j = jr[r];
@@ -212,7 +233,7 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
                 const int64_t c = (int64_t)i * si + (int64_t)j * sj + k;
                 if (ADE && (fl & CF_ADE_BRANCH)) {
                     // ADE branch (yee.c:914-1108) without CPML: only the owned components
-                    const DevAde &A = P.ade[__float_as_int(scls[cl * 4 + 2].z)];
+                    const DevAde &A = sade[__float_as_int(scls[cl * 4 + 2].z)];
                     const float curl[3] = {curlx, curly, curlz};
                     const bool gd[3] = {gx, gy, gz};
                     const unsigned cm[3] = {CF_ADE_X, CF_ADE_Y, CF_ADE_Z};
@@ -221,7 +242,7 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
                         if (!(fl & cm[a])) continue;
                         const float eo = e[r][a];
                         // difference-form state (DevAde); E^{n-1} is the output set before this step writes it
-                        const float qd = P.q[a][c], ep = P.fout[a][c];
+                        const float qd = (NPOLES == 0) ? aq[r][a] : P.q[a][c], ep = (NPOLES == 0) ? aep[r][a] : P.fout[a][c];
                         float pc[2] = {0.f, 0.f}, qc[2] = {0.f, 0.f};
                         for (int n = 0; n < NPOLES; n++) { pc[n] = P.pc[a][n][c]; qc[n] = P.qc[a][n][c]; }
                         float v = eo;
@@ -275,7 +296,7 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
 
 }  // namespace
 
-size_t bulk_smem_bytes(int nclasses) { return (size_t)S * STAGE + (size_t)nclasses * 64 + 8 * 2 * 32 * 4 + S * 8; }
+size_t bulk_smem_bytes(int nclasses) { return (size_t)S * STAGE + (size_t)nclasses * 64 + 8 * 2 * 32 * 4 + S * 8 + FDTD_MAX_ADE * sizeof(DevAde); }
 
 cudaError_t bulk_configure(int nclasses)
 {
