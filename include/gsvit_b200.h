@@ -224,19 +224,25 @@ int fdtd_step(fdtd_plan *plan, int nsteps);
 int fdtd_step_graph(fdtd_plan *plan, int nsteps, int chunk);
 
 /* Same as fdtd_step, with its scratch in static device memory.  No
- * counterpart in the reference.  The only scratch of a step is the pair of
- * TSF face correction tables per face (written by one kernel of the step and
- * read by the Yee kernels of the same step); this entry point places them in
- * one file-scope static device array of FDTD_STATIC_SCRATCH_BYTES instead of
- * the plan's own buffers, and calls no allocator.
+ * counterpart in the reference.  It is meant for callers that cannot call
+ * cudaMalloc where they step: applications whose device memory belongs to
+ * another allocator (a framework's caching allocator or a fixed budget), and
+ * loops where cudaMalloc's implicit device-wide synchronisation would stall
+ * other streams.  The only scratch of a step is the pair of TSF face
+ * correction tables per face (written by one kernel of the step and read by
+ * the Yee kernels of the same step); this entry point places them in one
+ * file-scope static device array of FDTD_STATIC_SCRATCH_BYTES instead of
+ * plan-owned buffers, and calls no allocator.  The caller still owns the plan
+ * (inputs and outputs); every GPU that loads the library holds the 32 MiB
+ * array until the process exits.
  *  - The first call on a device does set-up: it looks up the array's device
  *    address (with that device current) and keeps it.  Make that first call
  *    before any stream capture.
  *  - A plan whose tables need more than FDTD_STATIC_SCRATCH_BYTES (2 x 8 bytes
  *    per TSF face cell, each table rounded up to 256 bytes) is rejected with
  *    FDTD_E_UNSUPPORTED; the fields are left untouched.
- *  - Nothing in the array has to start at zero: every entry a step reads was
- *    written earlier in that step.
+ *  - The array keeps whatever the last call left in it.  Nothing in it has to
+ *    start at zero: every entry a step reads was written earlier in that step.
  *  - There is one array per device.  Calls that overlap in time on the same
  *    device (plans on different streams or host threads) race on it. */
 #define FDTD_STATIC_SCRATCH_BYTES (32u * 1024u * 1024u)

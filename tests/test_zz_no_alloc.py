@@ -1,6 +1,9 @@
-"""fdtd_step_static_scratch (step with its TSF face tables in static device
-memory) against fdtd_step, through the C ABI.  Collected last on purpose: it
-must give the same bits whether or not other plans ran in the process before."""
+"""fdtd_step_static_scratch, the step for callers that cannot call cudaMalloc
+where they step (their device memory belongs to another allocator, or
+cudaMalloc's device-wide synchronisation would stall other streams): its TSF
+face tables live in a static device array.  Checked against fdtd_step through
+the C ABI on two calls in a row.  Collected last on purpose, and it must give
+the same bits whether it runs alone or after other plans in the process."""
 import ctypes as C
 
 import numpy as np
