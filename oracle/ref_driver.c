@@ -414,3 +414,74 @@ int ref_get_aux(const ref_state *r, double *e, double *h)
 }
 
 int ref_get_step(const ref_state *r) { return r->set->sc.step_act; }
+
+#ifdef GSVIT_DROPIN
+/* ------------------------------------------------------------------------
+ * Drop-in check (test infrastructure): the same planned SvPool / SvSet, but
+ * stepped through the GPU branch of svit.c:204-256 -- sv_pool_allocate_gpus
+ * (pool.c:76-81) and the sv_pool_gpu_* family, here provided by
+ * gsvit_copy_b200/dropin/gpu_b200.c over libgsvit_b200.  Built only into
+ * oracle/_ref/libgsvit_dropin.so, with UCUDA defined for every object.
+ */
+int dropin_start(ref_state *r)
+{
+    SvPool *mp = r->mp;
+    SvSet *set = r->set;
+    int p;
+    /* point outputs as the planner leaves them (set->so, output.c:110-120) */
+    set->so.npnts = r->nprobes;
+    set->so.pnts = (SvOutputPar *)g_malloc0(sizeof(SvOutputPar) * (r->nprobes > 0 ? r->nprobes : 1));
+    for (p = 0; p < r->nprobes; p++) {
+        set->so.pnts[p].i = r->probes[3 * p];
+        set->so.pnts[p].j = r->probes[3 * p + 1];
+        set->so.pnts[p].k = r->probes[3 * p + 2];
+    }
+    if (r->nprobes > 0) {
+        mp->out->outpointdata = (gdouble **)g_malloc(sizeof(gdouble *) * r->nprobes);
+        for (p = 0; p < r->nprobes; p++)
+            mp->out->outpointdata[p] = (gdouble *)g_malloc0(sizeof(gdouble) * 6 * (size_t)(r->nsteps > 0 ? r->nsteps : 1));
+    }
+    set->plan.gpumode = SV_GPUMODE_FULL;
+    set->sc.ugpu[0] = 0;
+    sv_pool_allocate_gpus(mp, set);
+    if (!mp->gpu) return -1;
+    if (sv_pool_gpu_init(mp, set)) return -1;
+    return sv_pool_gpu_copyto(mp, set, SV_SYNC_ALL) ? -1 : 0;
+}
+
+/* the GPU branch of the loop, svit.c:240-256 */
+int dropin_step(ref_state *r, int nsteps)
+{
+    SvPool *mp = r->mp;
+    SvSet *set = r->set;
+    int it, rc = 0;
+    for (it = 0; it < nsteps; it++) {
+        rc |= sv_pool_gpu_boundary_copy(mp, set);
+        rc |= sv_pool_gpu_ystep_h(mp, set);
+        rc |= sv_pool_gpu_apply_source_hstep(mp, set);
+        rc |= sv_pool_gpu_boundary_hstep(mp, set);
+        rc |= sv_pool_gpu_ystep_e(mp, set);
+        rc |= sv_pool_gpu_apply_source_estep(mp, set);
+        rc |= sv_pool_gpu_boundary_estep(mp, set);
+        rc |= sv_pool_gpu_getsum(mp, set);
+        rc |= sv_pool_gpu_apply_farfield(mp, set);
+        rc |= sv_pool_gpu_apply_pfarfield(mp, set);
+        rc |= sv_pool_gpu_getpoints(mp, set);
+        rc |= sv_pool_gpu_getforce(mp, set);
+        set->sc.step_act++;
+    }
+    return rc ? -1 : 0;
+}
+
+/* sv_pool_gpu_copyfrom at output time (svit.c:251-253) */
+int dropin_finish(ref_state *r) { return sv_pool_gpu_copyfrom(r->mp, r->set, SV_SYNC_EH) ? -1 : 0; }
+
+/* the point outputs written by copyfrom, as out[(p*nsteps + step)*6 + c] */
+int dropin_get_probes(const ref_state *r, double *out)
+{
+    int p;
+    for (p = 0; p < r->nprobes; p++)
+        memcpy(out + (size_t)p * r->nsteps * 6, r->mp->out->outpointdata[p], sizeof(double) * 6 * (size_t)r->nsteps);
+    return 0;
+}
+#endif

@@ -62,6 +62,9 @@ static inline gchar *g_strdup(const gchar *s) { if (!s) return NULL; size_t n = 
 
 /* local/random sources only (outside the path driven here) */
 typedef struct _GRand { unsigned long long s; } GRand;
+/* opaque thread-queue types named by gpu.h (compiled with UCUDA for the drop-in build only) */
+typedef struct _GQueue GQueue;
+typedef struct _GMutex GMutex;
 static inline GRand *g_rand_new(void) { GRand *r = (GRand *)g_malloc(sizeof(GRand)); r->s = 88172645463325252ULL; return r; }
 static inline GRand *g_rand_new_with_seed(guint32 seed) { GRand *r = g_rand_new(); r->s ^= seed; return r; }
 static inline void g_rand_set_seed(GRand *r, guint32 seed) { r->s = 88172645463325252ULL ^ seed; }

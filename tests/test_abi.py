@@ -126,3 +126,36 @@ def test_null_arguments():
     assert lib.fdtd_step(None, 1) == -1
     assert lib.fdtd_sync(None) == -1
     assert lib.fdtd_plan_destroy(None) == 0
+
+
+DROPIN_SO = os.path.join(ROOT, "oracle", "_ref", "libgsvit_dropin.so")
+GSVIT_GPU_FAMILY = ["sv_gpu_new", "sv_pool_gpu_init", "sv_pool_gpu_apply_source_hstep", "sv_pool_gpu_apply_source_estep",
+                    "sv_pool_gpu_ystep_h", "sv_pool_gpu_ystep_e", "sv_pool_gpu_copyto", "sv_pool_gpu_copyfrom",
+                    "sv_pool_gpu_getsum", "sv_pool_gpu_boundary_copy", "sv_pool_gpu_boundary_hstep",
+                    "sv_pool_gpu_boundary_estep", "sv_pool_gpu_apply_farfield", "sv_pool_gpu_getpoints",
+                    "sv_pool_gpu_getforce", "sv_pool_gpu_apply_pfarfield"]
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN_SO), reason="drop-in test build not present")
+def test_dropin_exports_gsvit_gpu_family():
+    """The drop-in for src3d/gpu.c defines sv_gpu_new and every sv_pool_gpu_*
+    function GSvit's loop calls (pool.h:98-128) and links libgsvit_b200."""
+    out = subprocess.run(["nm", "-D", "--defined-only", DROPIN_SO], capture_output=True, text=True, check=True).stdout
+    defined = set(re.findall(r"\bT (sv_\w+)", out))
+    assert not [s for s in GSVIT_GPU_FAMILY if s not in defined]
+    deps = subprocess.run(["readelf", "-d", DROPIN_SO], capture_output=True, text=True, check=True).stdout
+    assert "libgsvit_b200.so" in deps
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN_SO), reason="drop-in test build not present")
+def test_dropin_build_cpu_branch_is_gsvit():
+    """Compiled with UCUDA (SvPool then carries its gpu member), GSvit's CPU
+    branch in the drop-in build still gives the bits of the plain build."""
+    from oracle.pyoracle import CpuSolver
+    from tests import _dropin
+    s = plan.small_scene("full", nsteps=20)
+    a, b = _dropin.DropinRun(s, gpu=False), CpuSolver(s, "reference")
+    a.step(20)
+    b.step(20)
+    for x, y in zip(a.fields(), b.fields()):
+        assert np.array_equal(x, y)
