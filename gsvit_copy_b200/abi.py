@@ -147,6 +147,15 @@ def load_library():
         "fdtd_snapshot_restore": ([P, P, C.c_size_t], C.c_int),
         "fdtd_last_error": ([], C.c_char_p),
         "fdtd_step_bytes": ([P, C.POINTER(C.c_double)], C.c_int),
+        "fdtd_batch_create": ([C.POINTER(Desc), C.c_int, C.c_int, C.POINTER(P)], C.c_int),
+        "fdtd_batch_destroy": ([P], C.c_int),
+        "fdtd_batch_size": ([P, C.POINTER(C.c_int)], C.c_int),
+        "fdtd_batch_plan": ([P, C.c_int, C.POINTER(P)], C.c_int),
+        "fdtd_batch_step": ([P, C.c_int], C.c_int),
+        "fdtd_batch_step_graph": ([P, C.c_int, C.c_int], C.c_int),
+        "fdtd_batch_sync": ([P], C.c_int),
+        "fdtd_batch_tune": ([P, C.c_int, _dp, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "fdtd_batch_config": ([P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -163,6 +172,8 @@ HEADER_SYMBOLS = [
     "fdtd_get_probes", "fdtd_nfff_spectrum", "fdtd_nfff_ndata", "fdtd_nfff_series", "fdtd_get_map", "fdtd_get_nclasses",
     "fdtd_snapshot_size", "fdtd_snapshot_save", "fdtd_snapshot_restore",
     "fdtd_last_error", "fdtd_step_bytes",
+    "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_size", "fdtd_batch_plan", "fdtd_batch_step",
+    "fdtd_batch_step_graph", "fdtd_batch_sync", "fdtd_batch_tune", "fdtd_batch_config",
 ]
 
 

@@ -100,6 +100,9 @@ struct fdtd_plan {
     BulkMaps bmaps[2];
     int *d_err = nullptr;
     int region[6] = {0, 0, 0, 0, 0, 0};   // bulk box Xlo Xhi Ylo Yhi Zlo Zhi
+    std::vector<SlabBox> h_boxes;         // host copies of the work lists (batched launches)
+    std::vector<BulkItem> h_bulk;
+    int bulk_len = 0;                     // planes per bulk item
     int tsf_cells = 0;                    // face cells of the TSF correction tables
     double bulk_bytes = 0, slab_bytes = 0; // algorithmic HBM bytes per launch
     // NFFF
@@ -192,6 +195,26 @@ int final_probes(fdtd_plan *P, cudaStream_t st)
     return FDTD_OK;
 }
 
+// Bulk work items of a plan: (j,k) tiles of the bulk box, planes cut into
+// chunks of `len`, chunk-major so that CTAs that run together share planes in
+// L2 (the halo rows/columns of neighbouring tiles are then served from L2).
+std::vector<BulkItem> bulk_items(const int lo[3], const int hi[3], int len, int inst)
+{
+    std::vector<BulkItem> blk;
+    for (int ib = lo[0]; ib < hi[0]; ib += len)
+        for (int j0 = lo[1]; j0 < hi[1]; j0 += BULK_TILE)
+            for (int k0 = lo[2]; k0 < hi[2]; k0 += BULK_TILE)
+                blk.push_back({j0, k0, ib, std::min(hi[0], ib + len), hi[1], hi[2], inst, 0});
+    return blk;
+}
+
+int bulk_tiles(const int lo[3], const int hi[3])
+{
+    return ((hi[1] - lo[1] + BULK_TILE - 1) / BULK_TILE) * ((hi[2] - lo[2] + BULK_TILE - 1) / BULK_TILE);
+}
+
+int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool pole_arrays);
+
 template <class T>
 cudaError_t upload(DevBuf &m, T **dst, const T *src, size_t count)
 {
@@ -206,7 +229,15 @@ extern "C" {
 
 const char *fdtd_last_error(void) { return g_err.c_str(); }
 
-int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
+int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out) { return plan_create_impl(desc, device, out, false); }
+
+}  // extern "C"
+
+namespace {
+
+// pole_arrays: allocate the critical-point state even for a Drude-only plan,
+// so that a batched launch may run it with the two-pole kernel variant
+int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool pole_arrays)
 {
     if (!out) return fail(FDTD_E_INVALID, "out is NULL");
     *out = nullptr;
@@ -222,6 +253,7 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
         return fail(rc, err);
     }
     HostPlan &hp = P->hp;
+    if (pole_arrays && hp.has_ade) hp.maxpoles = 2;
     P->device = device;
     cudaError_t ce = cudaSetDevice(device);
     if (ce != cudaSuccess) { delete P; return fail(FDTD_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce)); }
@@ -566,7 +598,7 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
         long long nblk = 0;
         auto add_box = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
             if (i0 >= i1 || j0 >= j1 || k0 >= k1) return;
-            boxes.push_back({i0, i1, j0, j1, k0, k1, nblk});
+            boxes.push_back({i0, i1, j0, j1, k0, k1, nblk, 0, 0});
             nblk += ((long long)(i1 - i0) * (j1 - j0) * (k1 - k0) + 255) / 256;
         };
         auto chunks = [&](int a0, int a1, int tiles, int *len) {
@@ -582,14 +614,10 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
             add_box(lo[0], hi[0], hi[1], Y, 0, Z);
             add_box(lo[0], hi[0], lo[1], hi[1], 0, lo[2]);
             add_box(lo[0], hi[0], lo[1], hi[1], hi[2], Z);
-            int tiles = ((hi[1] - lo[1] + BULK_TILE - 1) / BULK_TILE) * ((hi[2] - lo[2] + BULK_TILE - 1) / BULK_TILE), len;
-            chunks(lo[0], hi[0], tiles, &len);
-            // chunk-major order: CTAs that run together share planes, so the
-            // halo rows/columns of neighbouring tiles are served from L2
-            for (int ib = lo[0]; ib < hi[0]; ib += len)
-                for (int j0 = lo[1]; j0 < hi[1]; j0 += BULK_TILE)
-                    for (int k0 = lo[2]; k0 < hi[2]; k0 += BULK_TILE)
-                        blk.push_back({j0, k0, ib, std::min(hi[0], ib + len), hi[1], hi[2], 0, 0});
+            int len;
+            chunks(lo[0], hi[0], bulk_tiles(lo, hi), &len);
+            blk = bulk_items(lo, hi, len, 0);
+            P->bulk_len = len;
             for (int ax = 0; ax < 3; ax++) { P->region[2 * ax] = lo[ax]; P->region[2 * ax + 1] = hi[ax]; }
         } else {
             add_box(0, X, 0, Y, 0, Z);
@@ -624,6 +652,8 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
             P->bulk_bytes = P->bulk_on ? cell_bytes(lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]) : 0;
         }
         CA(upload(P->mem, &P->d_boxes, boxes.data(), boxes.size()), "slab boxes");
+        P->h_boxes = boxes;
+        P->h_bulk = blk;
         P->nboxes = (int)boxes.size();
         P->nslab_blocks = nblk;
         CA(P->mem.alloc(&P->d_err, 1), "error word");
@@ -637,7 +667,8 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
             for (int sset = 0; sset < 2; sset++)
                 if (bulk_make_maps(fn, d, P->fields[sset], cls, d.cpitch, &P->bmaps[sset]) != 0)
                     return bail(cudaErrorInvalidValue, "tensor map encoding");
-            CA(bulk_configure(d.nclasses), "bulk kernel shared memory");
+            // the largest layout (256 classes), so that any plan or batch may launch
+            CA(bulk_configure(256), "bulk kernel shared memory");
         }
     }
     P->step_bytes = bytes;
@@ -646,6 +677,10 @@ int fdtd_plan_create(const fdtd_desc *desc, int device, fdtd_plan **out)
     *out = P;
     return FDTD_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int fdtd_plan_destroy(fdtd_plan *P)
 {
@@ -1092,6 +1127,379 @@ int fdtd_step_bytes(const fdtd_plan *P, double *bytes)
 {
     if (!P || !bytes) return fail(FDTD_E_INVALID, "NULL argument");
     *bytes = P->step_bytes;
+    return FDTD_OK;
+}
+
+}  // extern "C"
+
+// ============================================================== batches
+//
+// Many independent plans (instances of uneven size and material) stepped in
+// lockstep: each kernel of a step is ONE launch over all instances, with the
+// per-instance parameters in device tables (per ping-pong parity) and every
+// work item naming its instance.  The bulk kernel runs persistently: a grid
+// of resident CTAs walks the concatenated item list.  The instance plans keep
+// their own state and remain the handles for fields, probes and far fields.
+
+struct fdtd_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<fdtd_plan *> plans;
+    DevBuf mem;
+    int ncls = 0, sms = 148;
+    int cur = 0;
+    // instances are grouped by kernel variant -- 0: no ADE, 1: Drude, 2: with
+    // critical-point poles -- so that each runs the variant it runs alone and
+    // gives the same bits; a step launches each kernel once per group in use
+    std::vector<int> group;
+    DevPlan *d_plans[2] = {nullptr, nullptr};
+    BulkMaps *d_maps[2] = {nullptr, nullptr};
+    DevAux *d_aux[2] = {nullptr, nullptr};
+    DevNfff *d_nfff[2] = {nullptr, nullptr};
+    BulkItem *d_items[3] = {nullptr, nullptr, nullptr};
+    size_t items_cap[3] = {0, 0, 0};
+    int nitems[3] = {0, 0, 0}, bulk_grid[3] = {0, 0, 0}, chunk_len = 0;
+    bool persistent = true;
+    SlabBox *d_boxes[3] = {nullptr, nullptr, nullptr};
+    int nboxes[3] = {0, 0, 0};
+    long long nslab_blocks[3] = {0, 0, 0};
+    int max_tsf = 0, max_nfff = 0;
+    int *d_err = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_steps = 0;
+};
+
+namespace {
+
+void batch_free(fdtd_batch *B)
+{
+    if (!B) return;
+    cudaSetDevice(B->device);
+    if (B->stream) cudaStreamSynchronize(B->stream);
+    for (int s = 0; s < 2; s++)
+        if (B->graph[s]) cudaGraphExecDestroy(B->graph[s]);
+    for (auto *p : B->plans) fdtd_plan_destroy(p);
+    B->mem.free_all();
+    if (B->stream) cudaStreamDestroy(B->stream);
+    delete B;
+}
+
+// bulk work list of every instance with `len` planes per item (0 = each
+// plan's own choice); grid: resident CTAs of the persistent launch
+cudaError_t batch_set_items(fdtd_batch *B, int len, bool persistent)
+{
+    for (int g = 0; g < 3; g++) {
+        std::vector<BulkItem> all;
+        for (size_t q = 0; q < B->plans.size(); q++) {
+            fdtd_plan *P = B->plans[q];
+            if (!P->bulk_on || B->group[q] != g) continue;
+            const int lo[3] = {P->region[0], P->region[2], P->region[4]}, hi[3] = {P->region[1], P->region[3], P->region[5]};
+            const auto it = bulk_items(lo, hi, len > 0 ? len : P->bulk_len, (int)q);
+            all.insert(all.end(), it.begin(), it.end());
+        }
+        if (all.size() > B->items_cap[g]) {
+            BulkItem *d;
+            cudaError_t e = B->mem.alloc(&d, all.size());
+            if (e != cudaSuccess) return e;
+            B->d_items[g] = d;
+            B->items_cap[g] = all.size();
+        }
+        if (!all.empty()) {
+            cudaError_t e = cudaMemcpy(B->d_items[g], all.data(), all.size() * sizeof(BulkItem), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return e;
+        }
+        B->nitems[g] = (int)all.size();
+        B->bulk_grid[g] = persistent ? 2 * B->sms : std::max(1, B->nitems[g]);
+    }
+    B->chunk_len = len;
+    B->persistent = persistent;
+    for (int s = 0; s < 2; s++)
+        if (B->graph[s]) { cudaGraphExecDestroy(B->graph[s]); B->graph[s] = nullptr; }
+    return cudaSuccess;
+}
+
+int batch_launch_step(fdtd_batch *B, cudaStream_t st)
+{
+    const int in = B->cur, n = (int)B->plans.size();
+    launch_aux_step_batch(B->d_aux[in], n, st);
+    if (B->max_tsf) launch_tsf_faces_batch(B->d_plans[in], n, B->max_tsf, st);
+    for (int g = 0; g < 3; g++) {
+        const bool ade = g > 0;
+        const int npoles = g == 2 ? 2 : 0;
+        cudaError_t e = launch_bulk_batch(B->d_plans[in], B->d_maps[in], B->d_items[g], B->nitems[g], B->bulk_grid[g], B->ncls,
+                                          B->d_err, ade, npoles, st);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched bulk launch: ") + cudaGetErrorString(e));
+        e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], ade, npoles, st);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
+    }
+    if (B->max_nfff) launch_nfff_accumulate_batch(B->d_nfff[in], n, B->max_nfff, st);
+    B->cur = 1 - in;
+    return FDTD_OK;
+}
+
+// the instance plans follow the batch: parity, step count, last probes
+int batch_after_steps(fdtd_batch *B, int nsteps)
+{
+    for (auto *P : B->plans) {
+        P->cur = B->cur;
+        P->host_step += nsteps;
+        final_probes(P, B->stream);
+    }
+    CK(cudaGetLastError());
+    return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch **out)
+{
+    if (!out) return fail(FDTD_E_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!descs || nplans < 1) return fail(FDTD_E_INVALID, "no plans");
+    for (int q = 0; q < nplans; q++)
+        if (descs[q].nfff.enabled && descs[q].nfff.series)
+            return fail(FDTD_E_UNSUPPORTED, "the time-domain far-field series is not available in a batch");
+    fdtd_batch *B = new (std::nothrow) fdtd_batch();
+    if (!B) return fail(FDTD_E_NOMEM, "host allocation failed");
+    B->device = device;
+    auto bail = [&](int rc) { batch_free(B); return rc; };
+    if (cudaSetDevice(device) != cudaSuccess) { delete B; return fail(FDTD_E_CUDA, "cudaSetDevice"); }
+    cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess) { delete B; return fail(FDTD_E_CUDA, "stream"); }
+    for (int q = 0; q < nplans; q++) {
+        fdtd_plan *P = nullptr;
+        const int rc = plan_create_impl(&descs[q], device, &P, false);
+        if (rc != FDTD_OK) {
+            const std::string m = fdtd_last_error();
+            batch_free(B);
+            return fail(rc, "batch plan " + std::to_string(q) + ": " + m);
+        }
+        P->stream = B->stream;
+        B->plans.push_back(P);
+        B->group.push_back(!P->hp.has_ade ? 0 : P->hp.maxpoles > 0 ? 2 : 1);
+        B->ncls = std::max(B->ncls, (int)P->hp.classes.size());
+        B->max_tsf = std::max(B->max_tsf, P->tsf_cells);
+        if (P->nfff && P->nfff_nfreq > 0) B->max_nfff = std::max(B->max_nfff, P->nfff_ns);
+    }
+#define BA(x, what) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { fail(FDTD_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e_)); return bail(FDTD_E_CUDA); } } while (0)
+    // per-instance parameter tables of both parities
+    for (int in = 0; in < 2; in++) {
+        std::vector<DevPlan> dp;
+        std::vector<BulkMaps> bm(nplans);
+        std::vector<DevAux> ax;
+        std::vector<DevNfff> nf(nplans);
+        std::memset(bm.data(), 0, sizeof(BulkMaps) * nplans);
+        std::memset(nf.data(), 0, sizeof(DevNfff) * nplans);
+        for (int q = 0; q < nplans; q++) {
+            fdtd_plan *P = B->plans[q];
+            dp.push_back(plan_for(P, in));
+            if (P->bulk_on) bm[q] = P->bmaps[in];
+            DevAux a = P->aux;
+            a.fields = P->d_fieldptrs[in];
+            ax.push_back(a);
+            if (P->nfff && P->nfff_nfreq > 0) {
+                nf[q] = P->nf;
+                nf[q].e = P->d_efieldptrs[1 - in];
+            }
+        }
+        BA(upload(B->mem, &B->d_plans[in], dp.data(), dp.size()), "batch tables");
+        BA(upload(B->mem, &B->d_maps[in], bm.data(), bm.size()), "batch tables");
+        BA(upload(B->mem, &B->d_aux[in], ax.data(), ax.size()), "batch tables");
+        BA(upload(B->mem, &B->d_nfff[in], nf.data(), nf.size()), "batch tables");
+    }
+    // slab boxes of every instance, one thread per cell, per kernel variant
+    for (int g = 0; g < 3; g++) {
+        std::vector<SlabBox> boxes;
+        for (int q = 0; q < nplans; q++) {
+            if (B->group[q] != g) continue;
+            for (SlabBox b : B->plans[q]->h_boxes) {
+                b.first_block = B->nslab_blocks[g];
+                b.inst = q;
+                boxes.push_back(b);
+                B->nslab_blocks[g] += ((long long)(b.i1 - b.i0) * (b.j1 - b.j0) * (b.k1 - b.k0) + 255) / 256;
+            }
+        }
+        if (B->nslab_blocks[g] > 0x7fffffffLL) { fail(FDTD_E_UNSUPPORTED, "too many slab cells for one launch"); return bail(FDTD_E_UNSUPPORTED); }
+        BA(upload(B->mem, &B->d_boxes[g], boxes.data(), boxes.size()), "batch slab boxes");
+        B->nboxes[g] = (int)boxes.size();
+    }
+    BA(B->mem.alloc(&B->d_err, 1), "error word");
+    BA(batch_set_items(B, 0, true), "batch work list");
+    BA(cudaDeviceSynchronize(), "batch set-up");
+#undef BA
+    *out = B;
+    return FDTD_OK;
+}
+
+int fdtd_batch_destroy(fdtd_batch *B)
+{
+    batch_free(B);
+    return FDTD_OK;
+}
+
+int fdtd_batch_size(const fdtd_batch *B, int *nplans)
+{
+    if (!B || !nplans) return fail(FDTD_E_INVALID, "NULL argument");
+    *nplans = (int)B->plans.size();
+    return FDTD_OK;
+}
+
+int fdtd_batch_plan(fdtd_batch *B, int index, fdtd_plan **plan)
+{
+    if (!B || !plan || index < 0 || index >= (int)B->plans.size()) return fail(FDTD_E_INVALID, "bad argument");
+    *plan = B->plans[index];
+    return FDTD_OK;
+}
+
+int fdtd_batch_step(fdtd_batch *B, int nsteps)
+{
+    if (!B || nsteps < 0) return fail(FDTD_E_INVALID, "bad argument");
+    CK(cudaSetDevice(B->device));
+    for (int s = 0; s < nsteps; s++) {
+        const int rc = batch_launch_step(B, B->stream);
+        if (rc != FDTD_OK) return rc;
+    }
+    return batch_after_steps(B, nsteps);
+}
+
+int fdtd_batch_step_graph(fdtd_batch *B, int nsteps, int chunk)
+{
+    if (!B || nsteps < 0) return fail(FDTD_E_INVALID, "bad argument");
+    CK(cudaSetDevice(B->device));
+    if (chunk < 2) chunk = 2;
+    chunk &= ~1;   // an even number of steps returns the ping-pong parity
+    if (B->graph_steps != chunk) {
+        for (int s = 0; s < 2; s++)
+            if (B->graph[s]) { cudaGraphExecDestroy(B->graph[s]); B->graph[s] = nullptr; }
+        B->graph_steps = chunk;
+    }
+    int done = 0;
+    while (nsteps - done >= chunk) {
+        const int par = B->cur;
+        if (!B->graph[par]) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+            for (int s = 0; s < chunk; s++) {
+                const int rc = batch_launch_step(B, B->stream);
+                if (rc != FDTD_OK) { cudaStreamEndCapture(B->stream, &g); B->cur = par; return rc; }
+            }
+            CK(cudaStreamEndCapture(B->stream, &g));
+            cudaGraphExec_t ge;
+            const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            B->graph[par] = ge;
+            B->cur = par;   // capture advanced cur by chunk (even): unchanged
+        }
+        CK(cudaGraphLaunch(B->graph[par], B->stream));
+        done += chunk;
+    }
+    for (int s = done; s < nsteps; s++) {
+        const int rc = batch_launch_step(B, B->stream);
+        if (rc != FDTD_OK) return rc;
+    }
+    return batch_after_steps(B, nsteps);
+}
+
+int fdtd_batch_sync(fdtd_batch *B)
+{
+    if (!B) return fail(FDTD_E_INVALID, "batch is NULL");
+    CK(cudaSetDevice(B->device));
+    CK(cudaStreamSynchronize(B->stream));
+    int err = 0;
+    CK(cudaMemcpy(&err, B->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail(FDTD_E_TIMEOUT, "a bounded wait of the batched bulk kernel expired");
+    for (auto *P : B->plans) {
+        const int rc = fdtd_sync(P);
+        if (rc != FDTD_OK) return rc;
+    }
+    return FDTD_OK;
+}
+
+int fdtd_batch_tune(fdtd_batch *B, int trial_steps, double *report, int report_len, int *ncand)
+{
+    if (!B || trial_steps < 1) return fail(FDTD_E_INVALID, "bad argument");
+    CK(cudaSetDevice(B->device));
+    CK(cudaStreamSynchronize(B->stream));
+    // keep the state: every plan's stepping state into one device backup
+    size_t total = 0;
+    for (auto *P : B->plans)
+        for (auto &it : P->snap) total += it.bytes;
+    char *backup = nullptr;
+    CK(cudaMalloc(&backup, std::max<size_t>(total, 16)));
+    auto copy_state = [&](bool save) -> cudaError_t {
+        char *q = backup;
+        for (auto *P : B->plans)
+            for (auto &it : P->snap) {
+                cudaError_t e = save ? cudaMemcpyAsync(q, it.ptr, it.bytes, cudaMemcpyDeviceToDevice, B->stream)
+                                     : cudaMemcpyAsync(it.ptr, q, it.bytes, cudaMemcpyDeviceToDevice, B->stream);
+                if (e != cudaSuccess) return e;
+                q += it.bytes;
+            }
+        return cudaSuccess;
+    };
+    const int cur0 = B->cur;
+    std::vector<int> steps0;
+    for (auto *P : B->plans) steps0.push_back(P->host_step);
+    cudaError_t e = copy_state(true);
+    // candidates: planes per item x (persistent grid | one CTA per item)
+    const int lens[] = {8, 16, 32, 64, 1 << 20};
+    int best_len = 0;
+    bool best_pers = true;
+    double best = 1e300;
+    int n = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    for (int li = 0; li < 5 && e == cudaSuccess; li++)
+        for (int pi = 0; pi < 2 && e == cudaSuccess; pi++) {
+            const bool pers = (pi == 0);
+            e = batch_set_items(B, lens[li], pers);
+            if (e != cudaSuccess) break;
+            int rc = batch_launch_step(B, B->stream);   // warm-up
+            if (rc == FDTD_OK) e = cudaEventRecord(e0, B->stream);
+            for (int s = 0; s < trial_steps && rc == FDTD_OK && e == cudaSuccess; s++) rc = batch_launch_step(B, B->stream);
+            if (rc != FDTD_OK) { e = cudaErrorLaunchFailure; break; }
+            if (e == cudaSuccess) e = cudaEventRecord(e1, B->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) break;
+            if (report && 3 * n + 2 < report_len) {
+                report[3 * n] = lens[li] == (1 << 20) ? 0 : lens[li];
+                report[3 * n + 1] = pers ? 1 : 0;
+                report[3 * n + 2] = ms / trial_steps;
+            }
+            n++;
+            if (ms < best) { best = ms; best_len = lens[li]; best_pers = pers; }
+        }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    // restore the state and keep the fastest work list
+    B->cur = cur0;
+    cudaError_t e2 = copy_state(false);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+    cudaFree(backup);
+    for (size_t q = 0; q < B->plans.size(); q++) {
+        B->plans[q]->cur = cur0;
+        B->plans[q]->host_step = steps0[q];
+    }
+    if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batch tuning: ") + cudaGetErrorString(e));
+    if (ncand) *ncand = n;
+    CK(batch_set_items(B, best_len, best_pers));
+    return FDTD_OK;
+}
+
+int fdtd_batch_config(const fdtd_batch *B, int *planes_per_item, int *persistent, int *grid, int *items)
+{
+    if (!B) return fail(FDTD_E_INVALID, "batch is NULL");
+    if (planes_per_item) *planes_per_item = B->chunk_len == (1 << 20) ? 0 : B->chunk_len;
+    if (persistent) *persistent = B->persistent ? 1 : 0;
+    if (grid) *grid = std::max(B->bulk_grid[0], std::max(B->bulk_grid[1], B->bulk_grid[2]));
+    if (items) *items = B->nitems[0] + B->nitems[1] + B->nitems[2];
     return FDTD_OK;
 }
 

@@ -86,19 +86,53 @@ __device__ __forceinline__ unsigned char *cbox(unsigned char *st) { return st + 
 
 // ------------------------------------------------------------- kernel
 
-template <bool ADE, int NPOLES>
-__global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ BulkMaps M,
-                                                      const BulkItem *items, int *err)
+// Shared-memory layout: the TMA ring, the class table (ncls_layout entries),
+// the row exchange of H between warps, one mbarrier per stage and the ADE table.
+struct BulkSmem {
+    unsigned char *stages;
+    float4 *scls;
+    float *hrow;        // [8][2][32]
+    uint64_t *bars;
+    DevAde *sade;
+};
+
+__device__ __forceinline__ BulkSmem bulk_smem(unsigned char *smem, int ncls_layout)
 {
-    extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *stages = smem;
-    float4 *scls = reinterpret_cast<float4 *>(smem + S * STAGE);
-    float *hrow = reinterpret_cast<float *>(smem + S * STAGE + P.nclasses * 64);        // [8][2][32]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S * STAGE + P.nclasses * 64 + 8 * 2 * 32 * 4);
-    DevAde *sade = reinterpret_cast<DevAde *>(smem + S * STAGE + P.nclasses * 64 + 8 * 2 * 32 * 4 + S * 8);
+    BulkSmem m;
+    m.stages = smem;
+    m.scls = reinterpret_cast<float4 *>(smem + S * STAGE);
+    m.hrow = reinterpret_cast<float *>(smem + S * STAGE + ncls_layout * 64);
+    m.bars = reinterpret_cast<uint64_t *>(smem + S * STAGE + ncls_layout * 64 + 8 * 2 * 32 * 4);
+    m.sade = reinterpret_cast<DevAde *>(smem + S * STAGE + ncls_layout * 64 + 8 * 2 * 32 * 4 + S * 8);
+    return m;
+}
+
+// class and ADE tables of one plan into shared memory (all threads)
+template <bool ADE>
+__device__ __forceinline__ void bulk_load_tables(const DevPlan &P, const BulkSmem &m)
+{
+    for (int q = threadIdx.x; q < P.nclasses * 4; q += NTH) m.scls[q] = reinterpret_cast<const float4 *>(P.classes)[q];
+    if (ADE)
+        for (int q = threadIdx.x; q < P.nade * (int)(sizeof(DevAde) / 4); q += NTH)
+            reinterpret_cast<float *>(m.sade)[q] = reinterpret_cast<const float *>(P.ade)[q];
+}
+
+// One work item: the i-march over planes [ib, ie) of one (j,k) tile.  The
+// ring's stage of plane p is (gplane + p - p0) % S with phase parity
+// ((gplane + p - p0) / S) & 1, gplane counting the planes this CTA has
+// streamed in earlier items, so that a persistent CTA keeps its mbarriers.
+// Returns false when a bounded wait gave up (after draining its copies).
+template <bool ADE, int NPOLES>
+__device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, const BulkItem &it, const BulkSmem &m,
+                                          uint32_t &gplane, int *err)
+{
+    unsigned char *stages = m.stages;
+    const float4 *scls = m.scls;
+    float *hrow = m.hrow;
+    uint64_t *bars = m.bars;
+    const DevAde *sade = m.sade;
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const BulkItem it = items[blockIdx.x];
     const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
     const int xr = P.xr, yr = P.yr, zr = P.zr;
     const int64_t si = P.si, sj = P.sj;
@@ -106,27 +140,22 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
     const int off = (k0 - 1) - ka, off8 = (k0 - 1) - ka8;
     const int p0 = (ib > 0) ? ib - 1 : ib;                    // first plane (prologue H when ib > 0)
     const int plast = min(ie, xr - 1);                        // last plane whose data is needed
+    const uint32_t g0 = gplane;
 
-    for (int q = tid; q < P.nclasses * 4; q += NTH) scls[q] = reinterpret_cast<const float4 *>(P.classes)[q];
-    if (ADE)
-        for (int q = tid; q < P.nade * (int)(sizeof(DevAde) / 4); q += NTH)
-            reinterpret_cast<float *>(sade)[q] = reinterpret_cast<const float *>(P.ade)[q];
-    if (tid == 0) {
-        for (int s = 0; s < S; s++) bar_init(&bars[s], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-
-    auto issue = [&](int p) {   // thread 0: all boxes of plane p into stage (p - p0) % S
-        const int s = (p - p0) % S;
+    auto issue = [&](int p) {   // thread 0: all boxes of plane p into its stage
+        const int s = (int)((g0 + (uint32_t)(p - p0)) % S);
         unsigned char *st = stages + s * STAGE;
         bar_expect_tx(&bars[s], STAGE_TX);
         for (int c = 0; c < 3; c++) tma_load3(ebox(st, c), &M.e[c], ka, j0 - 1, p, &bars[s]);
         for (int c = 0; c < 3; c++) tma_load3(hbox(st, c), &M.h[c], ka, j0 - 1, p, &bars[s]);
         tma_load3(cbox(st), &M.cls, ka8, j0 - 1, p, &bars[s]);
     };
-    if (tid == 0)
+    if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         for (int p = p0; p <= plast && p < p0 + S; p++) issue(p);
+    }
+    gplane = g0 + (uint32_t)(plast - p0 + 1);     // every plane p0..plast is streamed once
+    int issued = min(plast, p0 + S - 1);          // last plane issued (uniform over the CTA)
 
     // this thread's cells: rows rr = 4w + r (row 0 = j0-1), column lane (k = k0-1+lane)
     const int k = k0 - 1 + lane;
@@ -148,11 +177,12 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
     }
     bool failed = false;
     for (int i = p0; i <= plast && i < ie; i++) {
-        const int s = (i - p0) % S;
-        const uint32_t par = (uint32_t)(((i - p0) / S) & 1);
+        const uint32_t gi = g0 + (uint32_t)(i - p0);
+        const int s = (int)(gi % S);
+        const uint32_t par = (gi / S) & 1u;
         const bool have_next = (i + 1 <= plast);
-        const int s1 = (i + 1 - p0) % S;
-        const uint32_t par1 = (uint32_t)(((i + 1 - p0) / S) & 1);
+        const int s1 = (int)((gi + 1) % S);
+        const uint32_t par1 = ((gi + 1) / S) & 1u;
         bool ok = bar_wait(&bars[s], par);
         if (have_next) ok = ok && bar_wait(&bars[s1], par1);
         if (__syncthreads_or(!ok)) { failed = true; break; }
@@ -279,18 +309,71 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
         }
         for (int r = 0; r < 4; r++) { him[r][0] = h[r][1]; him[r][1] = h[r][2]; }
         __syncthreads();   // stage s is free
-        if (tid == 0 && i + S <= plast) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(i + S);
+        if (i + S <= plast) {
+            if (tid == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue(i + S);
+            }
+            issued = i + S;
         }
     }
     if (failed) {
         if (tid == 0) {
             atomicExch(err, 1);
-            for (int s = 0; s < S; s++)     // drain: one more bounded wait per stage
-                bar_wait(&bars[s], 0);
+            // drain: a bounded wait on the last phase issued into every stage
+            for (int p = max(p0, issued - S + 1); p <= issued; p++) {
+                const uint32_t gp = g0 + (uint32_t)(p - p0);
+                bar_wait(&bars[gp % S], (gp / S) & 1u);
+            }
         }
         __syncthreads();
+        return false;
+    }
+    return true;
+}
+
+template <bool ADE, int NPOLES>
+__global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ BulkMaps M,
+                                                      const BulkItem *items, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const BulkSmem m = bulk_smem(smem, P.nclasses);
+    bulk_load_tables<ADE>(P, m);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) bar_init(&m.bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t gplane = 0;
+    const BulkItem it = items[blockIdx.x];
+    bulk_item<ADE, NPOLES>(P, M, it, m, gplane, err);
+}
+
+// Many plans in one persistent launch: CTA b takes items b, b + grid, ...;
+// each item names its plan (it.inst) in the per-plan tables of this step's
+// parity.  Class and ADE tables are reloaded when the plan changes.
+template <bool ADE, int NPOLES>
+__global__ void __launch_bounds__(NTH, 2) bulk_kernel_batch(const DevPlan *plans, const BulkMaps *maps,
+                                                            const BulkItem *items, int nitems, int ncls_layout, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const BulkSmem m = bulk_smem(smem, ncls_layout);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) bar_init(&m.bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    uint32_t gplane = 0;
+    int cur = -1;
+    for (int n = blockIdx.x; n < nitems; n += gridDim.x) {
+        const BulkItem it = items[n];
+        const DevPlan &P = plans[it.inst];
+        if (it.inst != cur) {
+            __syncthreads();            // the previous item's readers of the tables are done
+            bulk_load_tables<ADE>(P, m);
+            cur = it.inst;
+        }
+        __syncthreads();
+        if (!bulk_item<ADE, NPOLES>(P, maps[it.inst], it, m, gplane, err)) return;
     }
 }
 
@@ -300,13 +383,16 @@ size_t bulk_smem_bytes(int nclasses) { return (size_t)S * STAGE + (size_t)nclass
 
 cudaError_t bulk_configure(int nclasses)
 {
-    size_t smem = bulk_smem_bytes(nclasses);
+    const int smem = (int)bulk_smem_bytes(nclasses);
     cudaError_t e;
-    e = cudaFuncSetAttribute(bulk_kernel<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(bulk_kernel<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(bulk_kernel<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if ((e = cudaFuncSetAttribute(bulk_kernel<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(bulk_kernel<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(bulk_kernel<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(bulk_kernel_batch<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(bulk_kernel_batch<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(bulk_kernel_batch<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 cudaError_t launch_bulk(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade,
@@ -320,6 +406,21 @@ cudaError_t launch_bulk(const DevPlan &p, const BulkMaps &m, const BulkItem *ite
         bulk_kernel<true, 0><<<nitems, NTH, smem, st>>>(p, m, items, err);
     else
         bulk_kernel<true, 2><<<nitems, NTH, smem, st>>>(p, m, items, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bulk_batch(const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems, int grid,
+                              int ncls_layout, int *err, bool ade, int npoles, cudaStream_t st)
+{
+    if (nitems <= 0) return cudaSuccess;
+    const size_t smem = bulk_smem_bytes(ncls_layout);
+    grid = min(grid, nitems);
+    if (!ade)
+        bulk_kernel_batch<false, 0><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
+    else if (npoles == 0)
+        bulk_kernel_batch<true, 0><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
+    else
+        bulk_kernel_batch<true, 2><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
     return cudaGetLastError();
 }
 

@@ -15,7 +15,7 @@ struct BulkMaps {
 
 // one CTA: own cells [j0, min(j0+31, jhi)) x [k0, min(k0+31, khi)) of planes [ib, ie)
 struct BulkItem {
-    int j0, k0, ib, ie, jhi, khi, pad0, pad1;
+    int j0, k0, ib, ie, jhi, khi, inst, pad0;   // inst: plan of the item in a batched launch
 };
 
 #define BULK_TILE 31
@@ -24,4 +24,8 @@ size_t bulk_smem_bytes(int nclasses);
 cudaError_t bulk_configure(int nclasses);
 cudaError_t launch_bulk(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade,
                         int npoles, cudaStream_t st);
+// all items of many plans in one persistent launch of `grid` CTAs; plans and
+// maps are device tables of this step's parity, indexed by BulkItem::inst
+cudaError_t launch_bulk_batch(const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems, int grid,
+                              int ncls_layout, int *err, bool ade, int npoles, cudaStream_t st);
 int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, BulkMaps *out);

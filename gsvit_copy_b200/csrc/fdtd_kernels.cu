@@ -344,7 +344,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
 // path; slab_e then forms E^{n+1} from the H^{n+1/2} that slab_h and the bulk
 // kernel wrote.  Both read E^n/H^n from the input set only.
 
-__device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &i, int &j, int &k)
+__device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &i, int &j, int &k, int &inst)
 {
     int b = 0;
     while (b + 1 < nboxes && (long long)blockIdx.x >= boxes[b + 1].first_block) b++;
@@ -356,15 +356,14 @@ __device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &
     t /= nk;
     j = B.j0 + (int)(t % nj);
     i = B.i0 + (int)(t / nj);
+    inst = B.inst;
     return true;
 }
 
 // 3 CTAs per SM: the slab kernels are latency-bound, and 24 resident warps
 // beat the register spill this costs e_special (1.95 -> 1.60 ms per 512^3 step)
-__global__ void __launch_bounds__(256, 3) slab_h_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
+__device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int k)
 {
-    int i, j, k;
-    if (!box_cell(boxes, nboxes, i, j, k)) return;
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
     const float *EX = P.fin[0], *EY = P.fin[1], *EZ = P.fin[2];
     const float ex = __ldg(EX + c), ey = __ldg(EY + c), ez = __ldg(EZ + c);
@@ -380,11 +379,21 @@ __global__ void __launch_bounds__(256, 3) slab_h_kernel(const __grid_constant__ 
     P.fout[5][c] = h[2];
 }
 
-template <bool ADE, int NPOLES>
-__global__ void __launch_bounds__(256, 3) slab_e_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
+__global__ void __launch_bounds__(256, 3) slab_h_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
 {
-    int i, j, k;
-    if (!box_cell(boxes, nboxes, i, j, k)) return;
+    int i, j, k, inst;
+    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell(P, i, j, k);
+}
+
+__global__ void __launch_bounds__(256, 3) slab_h_batch(const DevPlan *plans, const SlabBox *boxes, int nboxes)
+{
+    int i, j, k, inst;
+    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell(plans[inst], i, j, k);
+}
+
+template <bool ADE, int NPOLES>
+__device__ __forceinline__ void slab_e_cell(const DevPlan &P, int i, int j, int k)
+{
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
     const float *HX = P.fout[3], *HY = P.fout[4], *HZ = P.fout[5];   // H^{n+1/2}, written this step
     const float3 eo = make_float3(__ldg(P.fin[0] + c), __ldg(P.fin[1] + c), __ldg(P.fin[2] + c));
@@ -399,6 +408,20 @@ __global__ void __launch_bounds__(256, 3) slab_e_kernel(const __grid_constant__ 
     P.fout[2][c] = en.z;
 }
 
+template <bool ADE, int NPOLES>
+__global__ void __launch_bounds__(256, 3) slab_e_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
+{
+    int i, j, k, inst;
+    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_e_cell<ADE, NPOLES>(P, i, j, k);
+}
+
+template <bool ADE, int NPOLES>
+__global__ void __launch_bounds__(256, 3) slab_e_batch(const DevPlan *plans, const SlabBox *boxes, int nboxes)
+{
+    int i, j, k, inst;
+    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_e_cell<ADE, NPOLES>(plans[inst], i, j, k);
+}
+
 // ------------------------------------------------------------ TSF face tables
 
 // This step's TSF corrections for every face cell (source.c:547-771 and
@@ -406,13 +429,12 @@ __global__ void __launch_bounds__(256, 3) slab_e_kernel(const __grid_constant__ 
 // interpolation of dline.c:89-111 (FP64), projected by gex..ghz, scaled by
 // dt/(dx mu0) for H or (dt/dx)/epsilon(cell) for E, gated by TSF_SKIP, the
 // source-skip map and (k0 face) the PEC test.  Runs after aux_step.
-__global__ void tsf_face_kernel(const __grid_constant__ DevPlan P, int total)
+__device__ __forceinline__ void tsf_face_cell(const DevPlan &P, int t)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
     const int i0 = P.t0[0], j0 = P.t0[1], k0 = P.t0[2], in = P.t1[0], jn = P.t1[1], kn = P.t1[2];
     const int ni = in - i0 + 1, nj = jn - j0 + 1, nk = kn - k0 + 1;
     const int sz[3] = {nj * nk, ni * nk, ni * nj};
+    if (!P.tsf_on || t >= 2 * (sz[0] + sz[1] + sz[2])) return;
     int f = 0, off = t;
     while (f < 6 && off >= sz[f / 2]) { off -= sz[f / 2]; f++; }
     if (f >= 6) return;
@@ -488,12 +510,23 @@ __global__ void tsf_face_kernel(const __grid_constant__ DevPlan P, int total)
     (void)a; (void)b;
 }
 
+__global__ void tsf_face_kernel(const __grid_constant__ DevPlan P, int total)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < total) tsf_face_cell(P, t);
+}
+
+__global__ void tsf_face_batch(const DevPlan *plans)
+{
+    tsf_face_cell(plans[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // ------------------------------------------------------------ 1D aux grid
 
 // 1D TSF grid step of source.c:1469-1473 over 1dpool.c:84-162, in FP64 with
 // the reference's operation order (no contraction); also records the probes
 // of the previous step (output.c:341-352).
-__global__ void aux_step_kernel(const DevAux A)
+__device__ __forceinline__ void aux_step_body(const DevAux &A)
 {
     const int s = *A.step;
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -527,6 +560,10 @@ __global__ void aux_step_kernel(const DevAux A)
     if (tid == 0) *A.step = s + 1;
 }
 
+__global__ void aux_step_kernel(const DevAux A) { aux_step_body(A); }
+
+__global__ void aux_step_batch(const DevAux *A) { aux_step_body(A[blockIdx.x]); }
+
 __global__ void probe_capture_kernel(const DevAux A)
 {
     const int s = *A.step;     // number of completed steps
@@ -541,9 +578,8 @@ __global__ void probe_capture_kernel(const DevAux A)
 
 // Per surface cell s and frequency f:  Ehat += E(step) w,  Dhat += dE/dn(step) w,
 // w = exp(-i omega step dt).  FP64 accumulators.
-__global__ void nfff_accumulate_kernel(const DevNfff N)
+__device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= N.ns) return;
     const int step = *N.step - 1;
     const int64_t c = N.cell[s];
@@ -563,6 +599,13 @@ __global__ void nfff_accumulate_kernel(const DevNfff N)
             A.y -= v[q] * sn;
         }
     }
+}
+
+__global__ void nfff_accumulate_kernel(const DevNfff N) { nfff_accumulate_cell(N, blockIdx.x * blockDim.x + threadIdx.x); }
+
+__global__ void nfff_accumulate_batch(const DevNfff *N)
+{
+    nfff_accumulate_cell(N[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------------ far-field integration
@@ -747,6 +790,35 @@ cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes
     else
         slab_e_kernel<true, 2><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     return cudaGetLastError();
+}
+
+void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st)
+{
+    if (nplans > 0) aux_step_batch<<<nplans, 1024, 0, st>>>(a);
+}
+
+void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStream_t st)
+{
+    if (nplans > 0 && max_cells > 0) tsf_face_batch<<<dim3((max_cells + 255) / 256, nplans), 256, 0, st>>>(p);
+}
+
+cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade,
+                                    int npoles, cudaStream_t st)
+{
+    if (nblocks <= 0) return cudaSuccess;
+    slab_h_batch<<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    if (!ade)
+        slab_e_batch<false, 0><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    else if (npoles == 0)
+        slab_e_batch<true, 0><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    else
+        slab_e_batch<true, 2><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    return cudaGetLastError();
+}
+
+void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st)
+{
+    if (nplans > 0 && max_cells > 0) nfff_accumulate_batch<<<dim3((max_cells + 255) / 256, nplans), 256, 0, st>>>(n);
 }
 
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st)

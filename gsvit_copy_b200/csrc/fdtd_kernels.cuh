@@ -39,9 +39,18 @@ struct DevNfff {
 struct SlabBox {
     int i0, i1, j0, j1, k0, k1;
     long long first_block;
+    int inst, pad;              // plan of the box in a batched launch
 };
 
 void launch_aux_step(const DevAux &a, cudaStream_t st);
+
+// Batched forms: one launch covers many plans whose per-plan parameters are
+// device tables (of this step's parity), indexed by the plan number.
+void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st);
+void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStream_t st);
+cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade,
+                                    int npoles, cudaStream_t st);
+void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st);
 void launch_probe_capture(const DevAux &a, cudaStream_t st);
 void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st);
 cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,

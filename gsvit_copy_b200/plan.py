@@ -376,48 +376,74 @@ def rough_surface_scene(res: int = 512, zres: Optional[int] = None, dx: float = 
                         surface_frac: float = 0.5, theta_deg: float = 150.0, wavelength: float = 600e-9,
                         nfff_angles=(91, 181), nfff_wavelengths=(500e-9, 600e-9, 700e-9),
                         dtmult: float = 0.5, tsf_skipdepth: int = 2, tsf_margin: int = 8,
-                        nfff_margin: int = 4) -> Scene:
-    """Rough Drude-silver surface: res x res x zres cells (default 512^3), dx = 5 nm,
-    16-cell CPML, silver as ADE type 5 (eps_inf 3.7, wp 1.38e16 rad/s,
-    gamma 2.73e13 1/s, no CP poles) below a Gaussian-correlated height map
-    (rms 10 nm, correlation 50 nm, seeded FFT-filtered white noise), vacuum
+                        nfff_margin: int = 4, yres: Optional[int] = None, material: str = "drude") -> Scene:
+    """Rough metal surface: res x yres x zres cells (default 512^3), dx = 5 nm,
+    16-cell CPML, the substrate as ADE type 5 below a Gaussian-correlated height
+    map (rms 10 nm, correlation 50 nm, seeded FFT-filtered white noise), vacuum
     above; p-polarised TSF plane wave at 30 deg incidence from +z (theta = 150
     deg, phi = 0, psi = 0) with a 600 nm Gaussian pulse; NFFF box between CPML
     and TSF box with far points on a 91 x 181 theta-phi grid and running DFTs at
     500/600/700 nm.  DT_MULT is 0.5 (the value GSvit's dispersive self-tests
-    use)."""
+    use).  material "drude": silver (eps_inf 3.7, wp 1.38e16 rad/s, gamma
+    2.73e13 1/s, no CP poles); "lorentz": one Lorentz pole (eps_s 5, eps_inf 2,
+    w0 4e15 rad/s, delta 1e14 1/s) as a critical-point term."""
+    xres = res
+    yres = yres or res
     zres = zres or res
     dt = plan_dt(dx, dx, dx, dtmult)
-    s = Scene(name=f"rough{res}x{zres}", xres=res, yres=res, zres=zres, dx=dx, dt=dt, nsteps=nsteps)
-    silver = ade_material(3.7, 0.0, 1.38e16, 2.73e13, [(0, 0, 0, 0), (0, 0, 0, 0)], dt)
-    s.mats = [vacuum_material(), silver]
-    h = gaussian_height_map(res, res, rms / dx, corr_len / dx, seed)
+    s = Scene(name=f"rough{xres}x{yres}x{zres}", xres=xres, yres=yres, zres=zres, dx=dx, dt=dt, nsteps=nsteps)
+    if material == "drude":
+        metal = ade_material(3.7, 0.0, 1.38e16, 2.73e13, [(0, 0, 0, 0), (0, 0, 0, 0)], dt)
+    elif material == "lorentz":
+        metal = ade_material(2.0, 0.0, 0.0, 0.0, [lorentz_as_cp(5.0, 2.0, 4e15, 1e14), (0, 0, 0, 0)], dt)
+    else:
+        raise ValueError(material)
+    s.mats = [vacuum_material(), metal]
+    h = gaussian_height_map(xres, yres, rms / dx, corr_len / dx, seed)
     z0 = surface_frac * zres
     surf = z0 + h                                     # in cells
     kk = np.arange(zres, dtype=np.float64)[None, None, :] + 0.5
-    s.mat = (kk < surf[:, :, None]).astype(np.int32)  # VTK index map: 1 = silver
+    s.mat = (kk < surf[:, :, None]).astype(np.int32)  # VTK index map: 1 = metal
     s.cpml = cpml_all(cpml_depth, 3, -1, 1.0, 0.0, dx)
     lo = cpml_depth + tsf_margin
-    hi_xy = res - lo
-    hi_z = zres - lo
     th = math.radians(theta_deg)
     nw = nsteps + 1
-    s.tsf = dict(box=((lo, lo, lo), (hi_xy, hi_xy, hi_z)), theta=th, phi=0.0, psi=0.0,
+    s.tsf = dict(box=((lo, lo, lo), (xres - lo, yres - lo, zres - lo)), theta=th, phi=0.0, psi=0.0,
                  skip=[0, 0, 0, 0, 1, 0], skipdepth=tsf_skipdepth,
                  wave=gaussian_pulse(nw, dt, wavelength, 3 * 4e-15, 4e-15))
     if nfff_angles:
         nlo = cpml_depth + nfff_margin
-        box = ((nlo, nlo, nlo), (res - nlo, res - nlo, zres - nlo))
-        radius = 10 * max(res, zres)
+        box = ((nlo, nlo, nlo), (xres - nlo, yres - nlo, zres - nlo))
+        radius = 10 * max(xres, yres, zres)
         pts = spherical_area(nfff_angles[0], nfff_angles[1], radius, 0.0, 0.0, G_PI / 2, 2 * G_PI,
-                             res, res, zres)
+                             xres, yres, zres)
         s.nfff = dict(box=box, points=pts, istart=nfff_istart(pts, dt, dx, shared=True),
                       omega=np.array([2 * G_PI * C0 / w for w in nfff_wavelengths]))
-    s.probes = np.asarray([(res // 2, res // 2, min(zres - cpml_depth - 2, int(z0) + 20)),
-                           (res // 2, res // 2, int(z0) + 2),
-                           (res // 3, res // 2, int(z0) - 2)], dtype=np.int32)
+    s.probes = np.asarray([(xres // 2, yres // 2, min(zres - cpml_depth - 2, int(z0) + 20)),
+                           (xres // 2, yres // 2, int(z0) + 2),
+                           (xres // 3, yres // 2, int(z0) - 2)], dtype=np.int32)
     s.meta.update(height_map=h, surface_z=z0)
     return s
+
+
+def batch_scenes(n: int = 48, nsteps: int = 2000, seed: int = 7, sizes_xy=(64, 96, 128, 192), sizes_z=(64, 96, 128),
+                 nfff_angles=(10, 19)) -> List[Scene]:
+    """Independent rough-surface realisations of uneven size for batched runs:
+    x, y drawn from {64, 96, 128, 192} and z from {64, 96, 128}; rms height
+    5-20 nm, correlation length 30-100 nm, Drude silver or a single-pole
+    Lorentz substrate, incidence 0-60 deg, 8-cell CPML, dx = 5 nm."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        xr, yr = int(rng.choice(sizes_xy)), int(rng.choice(sizes_xy))
+        zr = int(rng.choice(sizes_z))
+        s = rough_surface_scene(res=xr, yres=yr, zres=zr, nsteps=nsteps, cpml_depth=8, seed=int(rng.integers(1 << 30)),
+                                rms=float(rng.uniform(5e-9, 20e-9)), corr_len=float(rng.uniform(30e-9, 100e-9)),
+                                theta_deg=180.0 - float(rng.uniform(0.0, 60.0)), tsf_margin=6,
+                                material="drude" if rng.random() < 0.5 else "lorentz", nfff_angles=nfff_angles)
+        s.name = f"batch{q}_{xr}x{yr}x{zr}"
+        out.append(s)
+    return out
 
 
 def selftest_scene(code: str, res: int, nsteps: int) -> Scene:

@@ -15,21 +15,25 @@ from . import abi
 
 
 class Solver:
-    def __init__(self, scene, device: int = 0):
+    def __init__(self, scene, device: int = 0, _handle=None):
         self.lib = abi.load_library()
         self.scene = scene
+        self.shape = (scene.xres, scene.yres, scene.zres)
+        self.n = scene.ncells
+        self._owner = _handle is None
+        if _handle is not None:     # a plan owned by a Batch
+            self.h = _handle
+            return
         self._desc, self._keep = scene.desc()
         h = C.c_void_p()
         abi.check(self.lib.fdtd_plan_create(C.byref(self._desc), device, C.byref(h)), "fdtd_plan_create")
         self.h = h
-        self.shape = (scene.xres, scene.yres, scene.zres)
-        self.n = scene.ncells
 
     # -- lifetime
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and self._owner:
             self.lib.fdtd_plan_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -145,3 +149,67 @@ class Solver:
     def restore(self, buf: bytearray):
         cbuf = (C.c_char * len(buf)).from_buffer(buf)
         abi.check(self.lib.fdtd_snapshot_restore(self.h, C.cast(cbuf, C.c_void_p), len(buf)), "fdtd_snapshot_restore")
+
+
+class Batch:
+    """Many scenes stepped in lockstep, one launch per kernel for all of them
+    (fdtd_batch_*).  `batch[i]` is a Solver view of instance i for fields,
+    probes, far fields and maps; step through the batch only."""
+
+    def __init__(self, scenes, device: int = 0):
+        self.lib = abi.load_library()
+        self.scenes = list(scenes)
+        descs, self._keep = [], []
+        for sc in self.scenes:
+            d, k = sc.desc()
+            descs.append(d)
+            self._keep.append(k)
+        self._descs = (abi.Desc * len(descs))(*descs)
+        h = C.c_void_p()
+        abi.check(self.lib.fdtd_batch_create(self._descs, len(descs), device, C.byref(h)), "fdtd_batch_create")
+        self.h = h
+        self.views = []
+        for i, sc in enumerate(self.scenes):
+            ph = C.c_void_p()
+            abi.check(self.lib.fdtd_batch_plan(self.h, i, C.byref(ph)), "fdtd_batch_plan")
+            self.views.append(Solver(sc, _handle=ph))
+
+    def __len__(self):
+        return len(self.views)
+
+    def __getitem__(self, i):
+        return self.views[i]
+
+    def close(self):
+        if getattr(self, "h", None):
+            for v in self.views:
+                v.h = None
+            self.lib.fdtd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        abi.check(self.lib.fdtd_batch_step(self.h, n), "fdtd_batch_step")
+
+    def step_graph(self, n: int, chunk: int = 16):
+        abi.check(self.lib.fdtd_batch_step_graph(self.h, n, chunk), "fdtd_batch_step_graph")
+
+    def sync(self):
+        abi.check(self.lib.fdtd_batch_sync(self.h), "fdtd_batch_sync")
+
+    def tune(self, trial_steps: int = 4):
+        """Autotune the work list; returns [(planes per item (0 = whole), persistent, ms/step), ...]."""
+        rep = (C.c_double * 60)()
+        n = C.c_int()
+        abi.check(self.lib.fdtd_batch_tune(self.h, trial_steps, rep, 60, C.byref(n)), "fdtd_batch_tune")
+        return [(int(rep[3 * i]), bool(rep[3 * i + 1]), rep[3 * i + 2]) for i in range(n.value)]
+
+    def config(self) -> dict:
+        v = [C.c_int() for _ in range(4)]
+        abi.check(self.lib.fdtd_batch_config(self.h, *[C.byref(x) for x in v]), "fdtd_batch_config")
+        return dict(zip(["planes_per_item", "persistent", "grid", "items"], [x.value for x in v]))

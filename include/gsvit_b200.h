@@ -290,6 +290,40 @@ int fdtd_get_map(fdtd_plan *plan, int which, int32_t *out, size_t out_len);
 /* Number of distinct coefficient classes the plan derived. */
 int fdtd_get_nclasses(const fdtd_plan *plan, int *nclasses);
 
+/* ---- batches ---------------------------------------------------------------
+ * No counterpart in the reference (GSvit steps one domain per process).  Many
+ * independent plans -- instances of uneven size, material and source -- are
+ * stepped in lockstep: each kernel of a step is one launch over all of them,
+ * with per-instance parameter tables on the device and a persistent bulk
+ * kernel that walks the concatenated work list (one launch per kernel
+ * variant in use: no ADE, Drude, critical-point poles).  Results are
+ * bit-identical to the same plans stepped one by one. */
+typedef struct fdtd_batch fdtd_batch;
+
+/* Create nplans plans from descs[0..nplans) on one device and stream.  The
+ * time-domain far-field series (nfff.series) is not available in a batch. */
+int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch **out);
+int fdtd_batch_destroy(fdtd_batch *batch);
+int fdtd_batch_size(const fdtd_batch *batch, int *nplans);
+/* The plan of instance `index`, for fields, probes, far fields, maps and
+ * snapshots; it is stepped only through the batch. */
+int fdtd_batch_plan(fdtd_batch *batch, int index, fdtd_plan **plan);
+/* Advance every instance by nsteps (eager launches / CUDA graph of `chunk`
+ * steps, as fdtd_step and fdtd_step_graph). */
+int fdtd_batch_step(fdtd_batch *batch, int nsteps);
+int fdtd_batch_step_graph(fdtd_batch *batch, int nsteps, int chunk);
+/* Wait for the batch; reports an expired bounded wait as FDTD_E_TIMEOUT. */
+int fdtd_batch_sync(fdtd_batch *batch);
+/* Autotuner: times trial_steps steps for each candidate work list (planes per
+ * bulk item 8 / 16 / 32 / 64 / whole, persistent grid or one CTA per item),
+ * keeps the fastest and restores every instance's state.  report (if not
+ * NULL) receives up to report_len/3 rows {planes (0 = whole), persistent,
+ * ms per step}; *ncand the number of rows. */
+int fdtd_batch_tune(fdtd_batch *batch, int trial_steps, double *report, int report_len, int *ncand);
+/* The work list in use: planes per item (0 = whole), persistent launch,
+ * grid size and number of items. */
+int fdtd_batch_config(const fdtd_batch *batch, int *planes_per_item, int *persistent, int *grid, int *items);
+
 /* ---- checkpoint (forward snapshots) ---------------------------------------- */
 
 /* Bytes needed for one snapshot of the complete stepping state (fields, CPML
