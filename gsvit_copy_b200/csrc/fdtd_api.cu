@@ -6,6 +6,8 @@
 // every launch (gpu.c:787-801, gpu_kernels.cu:6063-6068); here a step is
 // three stream-ordered launches with no host synchronisation, and
 // fdtd_step_graph replays them from a CUDA graph.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -79,6 +81,8 @@ struct SnapItem {      // one contiguous device range that is part of the steppi
 struct fdtd_plan {
     HostPlan hp;
     int device = 0;
+    int storage = FDTD_STORE_F32;  // element type of the fields and psi slabs
+    size_t esz = 4;                // its size in bytes
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     DevBuf mem;
@@ -147,10 +151,10 @@ int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
     DevPlan d = plan_for(P, in);
     cudaError_t e;
     if (P->bulk_on) {   // first: the slab E update reads H^{n+1/2} the bulk kernel wrote next to the slabs
-        e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, st);
+        e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
     }
-    e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, st);
+    e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
     if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
     return FDTD_OK;
 }
@@ -242,8 +246,6 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     if (!out) return fail(FDTD_E_INVALID, "out is NULL");
     *out = nullptr;
     if (!desc) return fail(FDTD_E_INVALID, "desc is NULL");
-    if (desc->storage != FDTD_STORE_F32)
-        return fail(FDTD_E_UNSUPPORTED, "reduced-precision field storage is not available in this build");
     fdtd_plan *P = new (std::nothrow) fdtd_plan();
     if (!P) return fail(FDTD_E_NOMEM, "host allocation failed");
     std::string err;
@@ -254,6 +256,9 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     }
     HostPlan &hp = P->hp;
     if (pole_arrays && hp.has_ade) hp.maxpoles = 2;
+    P->storage = desc->storage;
+    P->esz = (desc->storage == FDTD_STORE_F32) ? 4 : 2;
+    const size_t esz = P->esz;
     P->device = device;
     cudaError_t ce = cudaSetDevice(device);
     if (ce != cudaSuccess) { delete P; return fail(FDTD_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce)); }
@@ -274,10 +279,27 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     d.sj = hp.zr;
     d.si = (int64_t)hp.yr * hp.zr;
     d.dx = (float)hp.dx;
+    // 16-bit storage scales, chosen so that every stored value of a field of
+    // unit amplitude is of order one: H ~ E / Z0 (Z0 = 377 ohm) is stored
+    // times 2^9; psi_H accumulates dE/dx ~ E / dx and is stored times the
+    // power of two nearest dx; psi_E accumulates dH/dx and is stored times
+    // that and 2^9.  Powers of two make scaling and unscaling exact.
+    d.hs = 1.f; d.ihs = 1.f; d.ps = 1.f; d.ips = 1.f; d.pse = 1.f; d.ipse = 1.f;
+    if (P->storage != FDTD_STORE_F32) {
+        const int e2 = std::max(-100, std::min(100, (int)std::lround(std::log2(hp.dx))));
+        d.hs = 512.f;
+        d.ihs = 1.f / 512.f;
+        d.ps = std::ldexp(1.f, e2);
+        d.ips = std::ldexp(1.f, -e2);
+        d.pse = std::ldexp(1.f, e2 + 9);
+        d.ipse = std::ldexp(1.f, -e2 - 9);
+    }
+    // a field or psi array of `cnt` elements of the storage type, in float units
+    auto store_alloc = [&](float **ptr, size_t cnt) { return P->mem.alloc(ptr, (cnt * esz + 3) / 4); };
     for (int s = 0; s < 2; s++)
         for (int c = 0; c < 6; c++) {
-            CA(P->mem.alloc(&P->fields[s][c], n), "field allocation");
-            P->snap.push_back({P->fields[s][c], n * sizeof(float)});
+            CA(store_alloc(&P->fields[s][c], n), "field allocation");
+            P->snap.push_back({P->fields[s][c], n * esz});
         }
     uint8_t *cls;
     {
@@ -293,7 +315,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     CA(upload(P->mem, &classes, hp.classes.data(), hp.classes.size()), "class table");
     d.classes = classes;
     d.nclasses = (int)hp.classes.size();
-    double bytes = 49.0 * (double)n;   // 6 field reads + 6 writes + class byte
+    double bytes = (12.0 * esz + 1.0) * (double)n;   // 6 field reads + 6 writes + class byte
     if (hp.has_ade) {
         DevAde *ade;
         CA(upload(P->mem, &ade, hp.ades.data(), hp.ades.size()), "ADE table");
@@ -308,13 +330,13 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
                 P->snap.push_back({d.pc[a][q], n * 4}); P->snap.push_back({d.qc[a][q], n * 4});
             }
         }
-        size_t nd = 0;   // dispersive components: Q read + written, E^{n-1} read (12 B), + 16 B per pole (p, q)
+        size_t nd = 0;   // dispersive components: Q read + written (8 B), E^{n-1} read, + 16 B per pole (p, q)
         for (size_t c = 0; c < n; c++) {
             const DevClass &k = hp.classes[hp.cls[c]];
             if (k.flags & CF_ADE_BRANCH)
                 nd += ((k.flags & CF_ADE_X) ? 1 : 0) + ((k.flags & CF_ADE_Y) ? 1 : 0) + ((k.flags & CF_ADE_Z) ? 1 : 0);
         }
-        bytes += (double)nd * (12.0 + 16.0 * hp.maxpoles);
+        bytes += (double)nd * (8.0 + esz + 16.0 * hp.maxpoles);
     }
     // CPML
     for (int f = 0; f < 6; f++) {
@@ -330,14 +352,14 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         d.be[f] = be; d.ce[f] = ce; d.bh[f] = bh; d.ch[f] = ch;
         size_t cnt = (f < 2) ? (size_t)dep * hp.yr * hp.zr : (f < 4) ? (size_t)hp.xr * dep * hp.zr : (size_t)hp.xr * hp.yr * dep;
         for (int q = 0; q < 2; q++) {
-            CA(P->mem.alloc(&d.psie[f][q], cnt), "cpml psi");
-            P->snap.push_back({d.psie[f][q], cnt * 4});
+            CA(store_alloc(&d.psie[f][q], cnt), "cpml psi");
+            P->snap.push_back({d.psie[f][q], cnt * esz});
             for (int s = 0; s < 2; s++) {
-                CA(P->mem.alloc(&P->psih[s][f][q], cnt), "cpml psi");
-                P->snap.push_back({P->psih[s][f][q], cnt * 4});
+                CA(store_alloc(&P->psih[s][f][q], cnt), "cpml psi");
+                P->snap.push_back({P->psih[s][f][q], cnt * esz});
             }
         }
-        bytes += (double)cnt * 4 * 2 * 4;   // 4 psi arrays read + written
+        bytes += (double)cnt * esz * 2 * 4;   // 4 psi arrays read + written
     }
     for (int ax = 0; ax < 3; ax++) {
         float *a, *b;
@@ -351,6 +373,9 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     CA(P->mem.alloc(&P->d_step, 1), "step counter");
     P->snap.push_back({P->d_step, sizeof(int)});
     P->aux.step = P->d_step;
+    d.stepc = P->d_step;
+    P->aux.storage = P->storage;
+    P->aux.ihs = d.ihs;
     d.tsf_on = hp.tsf;
     if (hp.tsf) {
         const fdtd_tsf &t = desc->tsf;
@@ -533,6 +558,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             P->nf.acc = acc;
             P->nf.omega_dt = dodt;
             P->nf.step = P->d_step;
+            P->nf.storage = P->storage;
             P->nf.inv2dx = 1.0 / (2.0 * hp.dx);
             P->ff.npoints = f.npoints;
             P->ff.nfreq = f.nfreq;
@@ -572,10 +598,11 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             P->ns.istart = dist;
             P->ns.series = ser;
             P->ns.step = P->d_step;
+            P->ns.storage = P->storage;
             P->ns.dx = hp.dx;
             P->ns.dt = hp.dt;
         }
-        if (f.nfreq > 0) bytes += (double)cell.size() * (9 * 4 + (double)f.nfreq * 6 * 16 * 2);
+        if (f.nfreq > 0) bytes += (double)cell.size() * (9.0 * esz + (double)f.nfreq * 6 * 16 * 2);
     }
     // work decomposition: the bulk box (outside every CPML slab, one extra
     // plane on the low sides so that its halo row/column/plane is slab-free)
@@ -592,7 +619,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             hi[ax] = hp.cp[2 * ax + 1].enabled ? res[ax] - hp.cp[2 * ax + 1].depth : res[ax];
         }
         const char *nob = getenv("GSVIT_B200_NO_BULK");
-        P->bulk_on = (Z % 4 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
+        P->bulk_on = ((size_t)Z * esz % 16 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
         std::vector<SlabBox> boxes;
         std::vector<BulkItem> blk;
         long long nblk = 0;
@@ -633,10 +660,10 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
                     for (int j = j0; j < j1; j++)
                         for (int k = k0; k < k1; k++) {
                             const DevClass &c = hp.classes[hp.cls[((size_t)i * Y + j) * Z + k]];
-                            b += 49.0;
+                            b += 12.0 * esz + 1.0;
                             if (c.flags & CF_ADE_BRANCH)
                                 b += (((c.flags & CF_ADE_X) ? 1 : 0) + ((c.flags & CF_ADE_Y) ? 1 : 0) + ((c.flags & CF_ADE_Z) ? 1 : 0)) *
-                                     (12.0 + 16.0 * hp.maxpoles);
+                                     (8.0 + esz + 16.0 * hp.maxpoles);
                         }
                 return b;
             };
@@ -646,7 +673,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             for (int f = 0; f < 6; f++)
                 if (hp.cp[f].enabled) {
                     const int dep = hp.cp[f].depth;
-                    psi += ((f < 2) ? (double)dep * Y * Z : (f < 4) ? (double)X * dep * Z : (double)X * Y * dep) * 4 * 8.0;
+                    psi += ((f < 2) ? (double)dep * Y * Z : (f < 4) ? (double)X * dep * Z : (double)X * Y * dep) * 4 * 2.0 * esz;
                 }
             P->slab_bytes = total + psi;
             P->bulk_bytes = P->bulk_on ? cell_bytes(lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]) : 0;
@@ -665,16 +692,80 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             CA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q), "driver entry point");
             if (!fn || q != cudaDriverEntryPointSuccess) return bail(cudaErrorNotSupported, "cuTensorMapEncodeTiled");
             for (int sset = 0; sset < 2; sset++)
-                if (bulk_make_maps(fn, d, P->fields[sset], cls, d.cpitch, &P->bmaps[sset]) != 0)
+                if (bulk_make_maps(fn, d, P->fields[sset], cls, d.cpitch, P->storage, &P->bmaps[sset]) != 0)
                     return bail(cudaErrorInvalidValue, "tensor map encoding");
             // the largest layout (256 classes), so that any plan or batch may launch
-            CA(bulk_configure(256), "bulk kernel shared memory");
+            CA(bulk_configure(), "bulk kernel shared memory");
         }
     }
     P->step_bytes = bytes;
     CA(cudaDeviceSynchronize(), "plan set-up");
 #undef CA
     *out = P;
+    return FDTD_OK;
+}
+
+// FP32 <-> storage element conversion on the host (H components carry hs)
+void pack_storage(int storage, float scale, const float *src, size_t n, uint16_t *dst)
+{
+    for (size_t q = 0; q < n; q++) {
+        const float v = src[q] * scale;
+        if (storage == FDTD_STORE_F16) {
+            __half h = __float2half_rn(v);
+            std::memcpy(&dst[q], &h, 2);
+        } else {
+            __nv_bfloat16 h = __float2bfloat16_rn(v);
+            std::memcpy(&dst[q], &h, 2);
+        }
+    }
+}
+
+void unpack_storage(int storage, float scale, const uint16_t *src, size_t n, float *dst)
+{
+    for (size_t q = 0; q < n; q++) {
+        if (storage == FDTD_STORE_F16) {
+            __half h;
+            std::memcpy(&h, &src[q], 2);
+            dst[q] = __half2float(h) * scale;
+        } else {
+            __nv_bfloat16 h;
+            std::memcpy(&h, &src[q], 2);
+            dst[q] = __bfloat162float(h) * scale;
+        }
+    }
+}
+
+// component c of the current set from FP32 host values; `sync` makes the
+// copy complete before returning (FP32 storage copies asynchronously
+// otherwise, 16-bit storage always completes, its staging buffer is local)
+int upload_comp(fdtd_plan *P, int c, const float *src, bool sync)
+{
+    const size_t n = P->hp.n;
+    if (P->storage == FDTD_STORE_F32) {
+        CK(cudaMemcpyAsync(P->fields[P->cur][c], src, n * 4, cudaMemcpyHostToDevice, P->stream));
+        if (sync) CK(cudaStreamSynchronize(P->stream));
+        return FDTD_OK;
+    }
+    std::vector<uint16_t> tmp(n);
+    pack_storage(P->storage, c >= 3 ? P->dp.hs : 1.f, src, n, tmp.data());
+    CK(cudaMemcpyAsync(P->fields[P->cur][c], tmp.data(), n * 2, cudaMemcpyHostToDevice, P->stream));
+    CK(cudaStreamSynchronize(P->stream));
+    return FDTD_OK;
+}
+
+// component c of the current set as FP32 host values (FP32 storage: an
+// asynchronous copy the caller synchronises)
+int download_comp(fdtd_plan *P, int c, float *dst)
+{
+    const size_t n = P->hp.n;
+    if (P->storage == FDTD_STORE_F32) {
+        CK(cudaMemcpyAsync(dst, P->fields[P->cur][c], n * 4, cudaMemcpyDeviceToHost, P->stream));
+        return FDTD_OK;
+    }
+    std::vector<uint16_t> tmp(n);
+    CK(cudaMemcpyAsync(tmp.data(), P->fields[P->cur][c], n * 2, cudaMemcpyDeviceToHost, P->stream));
+    CK(cudaStreamSynchronize(P->stream));
+    unpack_storage(P->storage, c >= 3 ? P->dp.ihs : 1.f, tmp.data(), n, dst);
     return FDTD_OK;
 }
 
@@ -722,8 +813,8 @@ int fdtd_set_fields(fdtd_plan *P, int mask, const double *const comps[6])
         if (!(mask & (1 << c))) continue;
         if (!comps[c]) return fail(FDTD_E_INVALID, "selected component pointer is NULL");
         for (size_t q = 0; q < P->hp.n; q++) tmp[q] = (float)comps[c][q];
-        CK(cudaMemcpyAsync(P->fields[P->cur][c], tmp.data(), P->hp.n * 4, cudaMemcpyHostToDevice, P->stream));
-        CK(cudaStreamSynchronize(P->stream));
+        int rc = upload_comp(P, c, tmp.data(), true);
+        if (rc != FDTD_OK) return rc;
     }
     return FDTD_OK;
 }
@@ -735,7 +826,8 @@ int fdtd_set_fields_f32(fdtd_plan *P, int mask, const float *const comps[6])
     for (int c = 0; c < 6; c++) {
         if (!(mask & (1 << c))) continue;
         if (!comps[c]) return fail(FDTD_E_INVALID, "selected component pointer is NULL");
-        CK(cudaMemcpyAsync(P->fields[P->cur][c], comps[c], P->hp.n * 4, cudaMemcpyHostToDevice, P->stream));
+        int rc = upload_comp(P, c, comps[c], false);
+        if (rc != FDTD_OK) return rc;
     }
     return FDTD_OK;
 }
@@ -747,7 +839,8 @@ int fdtd_get_fields_f32(fdtd_plan *P, int mask, float *const comps[6])
     for (int c = 0; c < 6; c++) {
         if (!(mask & (1 << c))) continue;
         if (!comps[c]) return fail(FDTD_E_INVALID, "selected component pointer is NULL");
-        CK(cudaMemcpyAsync(comps[c], P->fields[P->cur][c], P->hp.n * 4, cudaMemcpyDeviceToHost, P->stream));
+        int rc = download_comp(P, c, comps[c]);
+        if (rc != FDTD_OK) return rc;
     }
     CK(cudaStreamSynchronize(P->stream));
     return FDTD_OK;
@@ -761,7 +854,8 @@ int fdtd_get_fields(fdtd_plan *P, int mask, double *const comps[6])
     for (int c = 0; c < 6; c++) {
         if (!(mask & (1 << c))) continue;
         if (!comps[c]) return fail(FDTD_E_INVALID, "selected component pointer is NULL");
-        CK(cudaMemcpyAsync(tmp.data(), P->fields[P->cur][c], P->hp.n * 4, cudaMemcpyDeviceToHost, P->stream));
+        int rc = download_comp(P, c, tmp.data());
+        if (rc != FDTD_OK) return rc;
         CK(cudaStreamSynchronize(P->stream));
         for (size_t q = 0; q < P->hp.n; q++) comps[c][q] = (double)tmp[q];
     }
@@ -966,11 +1060,11 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
         CK(cudaEventRecord(E[1], st));
         DevPlan d = plan_for(P, in);
         if (P->bulk_on) {
-            cudaError_t e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, st);
+            cudaError_t e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
             if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
         }
         CK(cudaEventRecord(E[2], st));
-        cudaError_t e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, st);
+        cudaError_t e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
         CK(cudaEventRecord(E[3], st));
         launch_nfff(P, in, st);
@@ -1148,6 +1242,7 @@ struct fdtd_batch {
     DevBuf mem;
     int ncls = 0, sms = 148;
     int cur = 0;
+    int storage = FDTD_STORE_F32;   // one field storage type for every instance
     // instances are grouped by kernel variant -- 0: no ADE, 1: Drude, 2: with
     // critical-point poles -- so that each runs the variant it runs alone and
     // gives the same bits; a step launches each kernel once per group in use
@@ -1227,9 +1322,10 @@ int batch_launch_step(fdtd_batch *B, cudaStream_t st)
         const bool ade = g > 0;
         const int npoles = g == 2 ? 2 : 0;
         cudaError_t e = launch_bulk_batch(B->d_plans[in], B->d_maps[in], B->d_items[g], B->nitems[g], B->bulk_grid[g], B->ncls,
-                                          B->d_err, ade, npoles, st);
+                                          B->d_err, ade, npoles, B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched bulk launch: ") + cudaGetErrorString(e));
-        e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], ade, npoles, st);
+        e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], ade, npoles, B->storage,
+                                    st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
     }
     if (B->max_nfff) launch_nfff_accumulate_batch(B->d_nfff[in], n, B->max_nfff, st);
@@ -1261,9 +1357,13 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
     for (int q = 0; q < nplans; q++)
         if (descs[q].nfff.enabled && descs[q].nfff.series)
             return fail(FDTD_E_UNSUPPORTED, "the time-domain far-field series is not available in a batch");
+    for (int q = 1; q < nplans; q++)
+        if (descs[q].storage != descs[0].storage)
+            return fail(FDTD_E_UNSUPPORTED, "the instances of a batch must share one field storage type");
     fdtd_batch *B = new (std::nothrow) fdtd_batch();
     if (!B) return fail(FDTD_E_NOMEM, "host allocation failed");
     B->device = device;
+    B->storage = descs[0].storage;
     auto bail = [&](int rc) { batch_free(B); return rc; };
     if (cudaSetDevice(device) != cudaSuccess) { delete B; return fail(FDTD_E_CUDA, "cudaSetDevice"); }
     cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, device);

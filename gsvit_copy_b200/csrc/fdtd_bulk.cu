@@ -19,22 +19,32 @@
 #include <cuda_runtime.h>
 
 #include "fdtd_bulk.cuh"
+#include "../../include/gsvit_b200.h"
 #include "fdtd_device.cuh"
 
 namespace {
 
-constexpr int BROWS_E = 33, BROWS_H = 32, BW = 36, BWC = 48;
+// Box geometry per storage type T: E boxes BW x 33 and H boxes BW x 32
+// elements (k innermost) from the aligned column ka <= k0 - 1, the class byte
+// box 48 x 32 from ka8.  TMA needs the box start x and the inner box extent in
+// multiples of 16 bytes: 4 floats / 8 16-bit elements.
+constexpr int BROWS_E = 33, BROWS_H = 32, BWC = 48;
 constexpr int S = 3;
-constexpr int EBOX = BROWS_E * BW * 4;                     // 4752 B
-constexpr int EBOX_PAD = (EBOX + 127) / 128 * 128;         // 4864 B
-constexpr int HBOX = BROWS_H * BW * 4;                     // 4608 B
 constexpr int CBOX = BROWS_H * BWC;                        // 1536 B
-constexpr int STAGE = 3 * EBOX_PAD + 3 * HBOX + CBOX;      // 29952 B
-constexpr uint32_t STAGE_TX = 3 * EBOX + 3 * HBOX + CBOX;  // bytes the TMA delivers per stage
+template <class T>
+struct Geo {
+    static constexpr int XAL = 16 / (int)sizeof(T);                        // x alignment (elements)
+    static constexpr int BW = sizeof(T) == 4 ? 36 : 40;                     // box width (elements)
+    static constexpr int EBOX = BROWS_E * BW * (int)sizeof(T);              // 4752 / 2640 B
+    static constexpr int EBOX_PAD = (EBOX + 127) / 128 * 128;               // 4864 / 2688 B
+    static constexpr int HBOX = BROWS_H * BW * (int)sizeof(T);              // 4608 / 2560 B
+    static constexpr int STAGE = 3 * EBOX_PAD + 3 * HBOX + CBOX;           // 29952 / 17280 B
+    static constexpr uint32_t TX = 3 * EBOX + 3 * HBOX + CBOX;             // bytes the TMA delivers per stage
+    static_assert(EBOX_PAD % 128 == 0 && HBOX % 128 == 0 && CBOX % 128 == 0, "TMA boxes must stay 128-B aligned");
+};
 constexpr int NTH = 256;
 constexpr long long WAIT_LIMIT = 1ll << 22;
 
-static_assert(EBOX_PAD % 128 == 0 && HBOX % 128 == 0 && CBOX % 128 == 0, "TMA boxes must stay 128-B aligned");
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -77,12 +87,15 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int
         : "memory");
 }
 
-__device__ __forceinline__ float *ebox(unsigned char *st, int c) { return reinterpret_cast<float *>(st + c * EBOX_PAD); }
-__device__ __forceinline__ float *hbox(unsigned char *st, int c)
+template <class T>
+__device__ __forceinline__ T *ebox(unsigned char *st, int c) { return reinterpret_cast<T *>(st + c * Geo<T>::EBOX_PAD); }
+template <class T>
+__device__ __forceinline__ T *hbox(unsigned char *st, int c)
 {
-    return reinterpret_cast<float *>(st + 3 * EBOX_PAD + c * HBOX);
+    return reinterpret_cast<T *>(st + 3 * Geo<T>::EBOX_PAD + c * Geo<T>::HBOX);
 }
-__device__ __forceinline__ unsigned char *cbox(unsigned char *st) { return st + 3 * EBOX_PAD + 3 * HBOX; }
+template <class T>
+__device__ __forceinline__ unsigned char *cbox(unsigned char *st) { return st + 3 * Geo<T>::EBOX_PAD + 3 * Geo<T>::HBOX; }
 
 // ------------------------------------------------------------- kernel
 
@@ -96,14 +109,16 @@ struct BulkSmem {
     DevAde *sade;
 };
 
+template <class T>
 __device__ __forceinline__ BulkSmem bulk_smem(unsigned char *smem, int ncls_layout)
 {
+    constexpr int SS = S * Geo<T>::STAGE;
     BulkSmem m;
     m.stages = smem;
-    m.scls = reinterpret_cast<float4 *>(smem + S * STAGE);
-    m.hrow = reinterpret_cast<float *>(smem + S * STAGE + ncls_layout * 64);
-    m.bars = reinterpret_cast<uint64_t *>(smem + S * STAGE + ncls_layout * 64 + 8 * 2 * 32 * 4);
-    m.sade = reinterpret_cast<DevAde *>(smem + S * STAGE + ncls_layout * 64 + 8 * 2 * 32 * 4 + S * 8);
+    m.scls = reinterpret_cast<float4 *>(smem + SS);
+    m.hrow = reinterpret_cast<float *>(smem + SS + ncls_layout * 64);
+    m.bars = reinterpret_cast<uint64_t *>(smem + SS + ncls_layout * 64 + 8 * 2 * 32 * 4);
+    m.sade = reinterpret_cast<DevAde *>(smem + SS + ncls_layout * 64 + 8 * 2 * 32 * 4 + S * 8);
     return m;
 }
 
@@ -122,7 +137,7 @@ __device__ __forceinline__ void bulk_load_tables(const DevPlan &P, const BulkSme
 // ((gplane + p - p0) / S) & 1, gplane counting the planes this CTA has
 // streamed in earlier items, so that a persistent CTA keeps its mbarriers.
 // Returns false when a bounded wait gave up (after draining its copies).
-template <bool ADE, int NPOLES>
+template <bool ADE, int NPOLES, class T>
 __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, const BulkItem &it, const BulkSmem &m,
                                           uint32_t &gplane, int *err)
 {
@@ -136,19 +151,21 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
     const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
     const int xr = P.xr, yr = P.yr, zr = P.zr;
     const int64_t si = P.si, sj = P.sj;
-    const int ka = (k0 - 1) & ~3, ka8 = (k0 - 1) & ~15;      // box origins (16-byte aligned x)
+    constexpr int BW = Geo<T>::BW, STAGE = Geo<T>::STAGE;
+    const int ka = (k0 - 1) & ~(Geo<T>::XAL - 1), ka8 = (k0 - 1) & ~15;   // box origins (16-byte aligned x)
     const int off = (k0 - 1) - ka, off8 = (k0 - 1) - ka8;
     const int p0 = (ib > 0) ? ib - 1 : ib;                    // first plane (prologue H when ib > 0)
     const int plast = min(ie, xr - 1);                        // last plane whose data is needed
     const uint32_t g0 = gplane;
+    const uint32_t stp = sr_step<T>(P);           // step number of the BF16 rounding dither
 
     auto issue = [&](int p) {   // thread 0: all boxes of plane p into its stage
         const int s = (int)((g0 + (uint32_t)(p - p0)) % S);
         unsigned char *st = stages + s * STAGE;
-        bar_expect_tx(&bars[s], STAGE_TX);
-        for (int c = 0; c < 3; c++) tma_load3(ebox(st, c), &M.e[c], ka, j0 - 1, p, &bars[s]);
-        for (int c = 0; c < 3; c++) tma_load3(hbox(st, c), &M.h[c], ka, j0 - 1, p, &bars[s]);
-        tma_load3(cbox(st), &M.cls, ka8, j0 - 1, p, &bars[s]);
+        bar_expect_tx(&bars[s], Geo<T>::TX);
+        for (int c = 0; c < 3; c++) tma_load3(ebox<T>(st, c), &M.e[c], ka, j0 - 1, p, &bars[s]);
+        for (int c = 0; c < 3; c++) tma_load3(hbox<T>(st, c), &M.h[c], ka, j0 - 1, p, &bars[s]);
+        tma_load3(cbox<T>(st), &M.cls, ka8, j0 - 1, p, &bars[s]);
     };
     if (tid == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -187,10 +204,12 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
         if (have_next) ok = ok && bar_wait(&bars[s1], par1);
         if (__syncthreads_or(!ok)) { failed = true; break; }
         unsigned char *st = stages + s * STAGE, *st1 = stages + s1 * STAGE;
-        const float *EX = ebox(st, 0), *EY = ebox(st, 1), *EZ = ebox(st, 2);
-        const float *HX = hbox(st, 0), *HY = hbox(st, 1), *HZ = hbox(st, 2);
-        const unsigned char *CL = cbox(st);
-        const float *EY1 = ebox(st1, 1), *EZ1 = ebox(st1, 2);
+        const T *EX = ebox<T>(st, 0), *EY = ebox<T>(st, 1), *EZ = ebox<T>(st, 2);
+        const T *HX = hbox<T>(st, 0), *HY = hbox<T>(st, 1), *HZ = hbox<T>(st, 2);
+        const unsigned char *CL = cbox<T>(st);
+        const T *EY1 = ebox<T>(st1, 1), *EZ1 = ebox<T>(st1, 2);
+        auto cv = [](T v) { return Stor<T>::cvt(v); };
+        const float ihs = Stor<T>::scaled ? P.ihs : 1.f;
         const bool prologue = (i < ib);
         const bool il = (i == xr - 1);
         // Drude state of this plane's own cells (Q and E^{n-1}), requested before
@@ -206,7 +225,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                 for (int a = 0; a < 3; a++) {
                     const bool need = (fl & CF_ADE_BRANCH) && (fl & cm[a]);
                     aq[r][a] = need ? P.q[a][c] : 0.f;
-                    aep[r][a] = need ? P.fout[a][c] : 0.f;
+                    aep[r][a] = need ? ldE<T>(P.fout[a], c) : 0.f;
                 }
             }
         }
@@ -214,14 +233,15 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
         for (int r = 0; r < 4; r++) {
             const int rr = 4 * w + r, j = jr[r];
             const int b = rr * BW + ce;
-            const float ex = EX[b], ey = EY[b], ez = EZ[b];
+            const float ex = cv(EX[b]), ey = cv(EY[b]), ez = cv(EZ[b]);
             e[r][0] = ex; e[r][1] = ey; e[r][2] = ez;
-            const float exj = EX[b + BW], ezj = EZ[b + BW];
-            const float exk = EX[b + 1], eyk = EY[b + 1];
-            const float eyi = have_next ? EY1[b] : 0.f, ezi = have_next ? EZ1[b] : 0.f;
+            const float exj = cv(EX[b + BW]), ezj = cv(EZ[b + BW]);
+            const float exk = cv(EX[b + 1]), eyk = cv(EY[b + 1]);
+            const float eyi = have_next ? cv(EY1[b]) : 0.f, ezi = have_next ? cv(EZ1[b]) : 0.f;
             const int cl = CL[rr * BWC + ce8];
             const float4 hc = scls[cl * 4 + 2];
-            float hx = HX[b], hy = HY[b], hz = HZ[b];
+            float hx = cv(HX[b]), hy = cv(HY[b]), hz = cv(HZ[b]);
+            if (Stor<T>::scaled) { hx *= ihs; hy *= ihs; hz *= ihs; }
             const bool jl = (j == yr - 1), kl = (k == zr - 1);
             if (!(jl || kl)) hx = hc.x * hx + hc.y * ((eyk - ey) - (ezj - ez));
             if (!(il || kl)) hy = hc.x * hy + hc.y * ((ezi - ez) - (exk - ex));
@@ -230,9 +250,9 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
             h[r][0] = hx; h[r][1] = hy; h[r][2] = hz;
             if (!prologue && own[r]) {
                 const int64_t c = (int64_t)i * si + (int64_t)j * sj + k;
-                P.fout[3][c] = hx;
-                P.fout[4][c] = hy;
-                P.fout[5][c] = hz;
+                stH<T>(P, P.fout[3], c, hx, stp, 3);
+                stH<T>(P, P.fout[4], c, hy, stp, 4);
+                stH<T>(P, P.fout[5], c, hz, stp, 5);
             }
         }
         if (!prologue) {
@@ -272,7 +292,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                         if (!(fl & cm[a])) continue;
                         const float eo = e[r][a];
                         // difference-form state (DevAde); E^{n-1} is the output set before this step writes it
-                        const float qd = (NPOLES == 0) ? aq[r][a] : P.q[a][c], ep = (NPOLES == 0) ? aep[r][a] : P.fout[a][c];
+                        const float qd = (NPOLES == 0) ? aq[r][a] : P.q[a][c], ep = (NPOLES == 0) ? aep[r][a] : ldE<T>(P.fout[a], c);
                         float pc[2] = {0.f, 0.f}, qc[2] = {0.f, 0.f};
                         for (int n = 0; n < NPOLES; n++) { pc[n] = P.pc[a][n][c]; qc[n] = P.qc[a][n][c]; }
                         float v = eo;
@@ -302,9 +322,9 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                 if (fl & CF_PEC_Y) ny = 0.f;
                 if (fl & CF_PEC_Z) nz = 0.f;
                 if (tsf) tsf_add_e(P, i, j, k, nx, ny, nz);
-                P.fout[0][c] = nx;
-                P.fout[1][c] = ny;
-                P.fout[2][c] = nz;
+                stE<T>(P.fout[0], c, nx, stp, 0);
+                stE<T>(P.fout[1], c, ny, stp, 1);
+                stE<T>(P.fout[2], c, nz, stp, 2);
             }
         }
         for (int r = 0; r < 4; r++) { him[r][0] = h[r][1]; him[r][1] = h[r][2]; }
@@ -332,12 +352,12 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
     return true;
 }
 
-template <bool ADE, int NPOLES>
+template <bool ADE, int NPOLES, class T>
 __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ BulkMaps M,
                                                       const BulkItem *items, int *err)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    const BulkSmem m = bulk_smem(smem, P.nclasses);
+    const BulkSmem m = bulk_smem<T>(smem, P.nclasses);
     bulk_load_tables<ADE>(P, m);
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; s++) bar_init(&m.bars[s], 1);
@@ -346,18 +366,18 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel(const __grid_constant__ De
     __syncthreads();
     uint32_t gplane = 0;
     const BulkItem it = items[blockIdx.x];
-    bulk_item<ADE, NPOLES>(P, M, it, m, gplane, err);
+    bulk_item<ADE, NPOLES, T>(P, M, it, m, gplane, err);
 }
 
 // Many plans in one persistent launch: CTA b takes items b, b + grid, ...;
 // each item names its plan (it.inst) in the per-plan tables of this step's
 // parity.  Class and ADE tables are reloaded when the plan changes.
-template <bool ADE, int NPOLES>
+template <bool ADE, int NPOLES, class T>
 __global__ void __launch_bounds__(NTH, 2) bulk_kernel_batch(const DevPlan *plans, const BulkMaps *maps,
                                                             const BulkItem *items, int nitems, int ncls_layout, int *err)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    const BulkSmem m = bulk_smem(smem, ncls_layout);
+    const BulkSmem m = bulk_smem<T>(smem, ncls_layout);
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; s++) bar_init(&m.bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -373,74 +393,114 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel_batch(const DevPlan *plans
             cur = it.inst;
         }
         __syncthreads();
-        if (!bulk_item<ADE, NPOLES>(P, maps[it.inst], it, m, gplane, err)) return;
+        if (!bulk_item<ADE, NPOLES, T>(P, maps[it.inst], it, m, gplane, err)) return;
     }
 }
 
 }  // namespace
 
-size_t bulk_smem_bytes(int nclasses) { return (size_t)S * STAGE + (size_t)nclasses * 64 + 8 * 2 * 32 * 4 + S * 8 + FDTD_MAX_ADE * sizeof(DevAde); }
-
-cudaError_t bulk_configure(int nclasses)
+size_t bulk_smem_bytes(int nclasses, int storage)
 {
-    const int smem = (int)bulk_smem_bytes(nclasses);
+    const size_t stage = storage == FDTD_STORE_F32 ? (size_t)Geo<float>::STAGE : (size_t)Geo<__half>::STAGE;
+    return S * stage + (size_t)nclasses * 64 + 8 * 2 * 32 * 4 + S * 8 + FDTD_MAX_ADE * sizeof(DevAde);
+}
+
+template <class T>
+cudaError_t configure_t()
+{
+    const int smem = (int)bulk_smem_bytes(256, sizeof(T) == 4 ? FDTD_STORE_F32 : FDTD_STORE_F16);
+    const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(bulk_kernel<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(bulk_kernel<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(bulk_kernel<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(bulk_kernel_batch<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-        return e;
-    if ((e = cudaFuncSetAttribute(bulk_kernel_batch<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-        return e;
-    return cudaFuncSetAttribute(bulk_kernel_batch<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if ((e = cudaFuncSetAttribute(bulk_kernel<false, 0, T>, A, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(bulk_kernel<true, 0, T>, A, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(bulk_kernel<true, 2, T>, A, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(bulk_kernel_batch<false, 0, T>, A, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(bulk_kernel_batch<true, 0, T>, A, smem)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(bulk_kernel_batch<true, 2, T>, A, smem);
+}
+
+// every variant accepts the largest layout (256 classes), so that any plan or
+// batch may launch it
+cudaError_t bulk_configure()
+{
+    cudaError_t e;
+    if ((e = configure_t<float>()) != cudaSuccess) return e;
+    if ((e = configure_t<__half>()) != cudaSuccess) return e;
+    return configure_t<__nv_bfloat16>();
+}
+
+template <class T>
+void launch_bulk_t(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade, int npoles,
+                   size_t smem, cudaStream_t st)
+{
+    if (!ade)
+        bulk_kernel<false, 0, T><<<nitems, NTH, smem, st>>>(p, m, items, err);
+    else if (npoles == 0)
+        bulk_kernel<true, 0, T><<<nitems, NTH, smem, st>>>(p, m, items, err);
+    else
+        bulk_kernel<true, 2, T><<<nitems, NTH, smem, st>>>(p, m, items, err);
 }
 
 cudaError_t launch_bulk(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade,
-                        int npoles, cudaStream_t st)
+                        int npoles, int storage, cudaStream_t st)
 {
     if (nitems <= 0) return cudaSuccess;
-    size_t smem = bulk_smem_bytes(p.nclasses);
-    if (!ade)
-        bulk_kernel<false, 0><<<nitems, NTH, smem, st>>>(p, m, items, err);
-    else if (npoles == 0)
-        bulk_kernel<true, 0><<<nitems, NTH, smem, st>>>(p, m, items, err);
-    else
-        bulk_kernel<true, 2><<<nitems, NTH, smem, st>>>(p, m, items, err);
+    const size_t smem = bulk_smem_bytes(p.nclasses, storage);
+    if (storage == FDTD_STORE_F16) launch_bulk_t<__half>(p, m, items, nitems, err, ade, npoles, smem, st);
+    else if (storage == FDTD_STORE_BF16) launch_bulk_t<__nv_bfloat16>(p, m, items, nitems, err, ade, npoles, smem, st);
+    else launch_bulk_t<float>(p, m, items, nitems, err, ade, npoles, smem, st);
     return cudaGetLastError();
 }
 
+template <class T>
+void launch_bulk_batch_t(const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems, int grid,
+                         int ncls_layout, int *err, bool ade, int npoles, size_t smem, cudaStream_t st)
+{
+    if (!ade)
+        bulk_kernel_batch<false, 0, T><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
+    else if (npoles == 0)
+        bulk_kernel_batch<true, 0, T><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
+    else
+        bulk_kernel_batch<true, 2, T><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
+}
+
 cudaError_t launch_bulk_batch(const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems, int grid,
-                              int ncls_layout, int *err, bool ade, int npoles, cudaStream_t st)
+                              int ncls_layout, int *err, bool ade, int npoles, int storage, cudaStream_t st)
 {
     if (nitems <= 0) return cudaSuccess;
-    const size_t smem = bulk_smem_bytes(ncls_layout);
+    const size_t smem = bulk_smem_bytes(ncls_layout, storage);
     grid = min(grid, nitems);
-    if (!ade)
-        bulk_kernel_batch<false, 0><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
-    else if (npoles == 0)
-        bulk_kernel_batch<true, 0><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
+    if (storage == FDTD_STORE_F16)
+        launch_bulk_batch_t<__half>(plans, maps, items, nitems, grid, ncls_layout, err, ade, npoles, smem, st);
+    else if (storage == FDTD_STORE_BF16)
+        launch_bulk_batch_t<__nv_bfloat16>(plans, maps, items, nitems, grid, ncls_layout, err, ade, npoles, smem, st);
     else
-        bulk_kernel_batch<true, 2><<<grid, NTH, smem, st>>>(plans, maps, items, nitems, ncls_layout, err);
+        launch_bulk_batch_t<float>(plans, maps, items, nitems, grid, ncls_layout, err, ade, npoles, smem, st);
     return cudaGetLastError();
 }
 
 // Tensor maps of one field set: 3D (k, j, i) float boxes of 36 x 33 (E) and
 // 36 x 32 (H); class bytes 48 x 32 over a row pitch padded to 16 bytes.
-int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, BulkMaps *out)
+int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, int storage, BulkMaps *out)
 {
     auto enc = reinterpret_cast<CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
                                              CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
                                              CUtensorMapFloatOOBfill)>(encode_fn);
     const cuuint64_t dims[3] = {(cuuint64_t)p.zr, (cuuint64_t)p.yr, (cuuint64_t)p.xr};
-    const cuuint64_t strides[2] = {(cuuint64_t)p.zr * 4, (cuuint64_t)p.zr * 4 * (cuuint64_t)p.yr};
+    const cuuint64_t es = storage == FDTD_STORE_F32 ? 4 : 2;
+    const CUtensorMapDataType dtype = storage == FDTD_STORE_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                      : storage == FDTD_STORE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const cuuint32_t BW = storage == FDTD_STORE_F32 ? Geo<float>::BW : Geo<__half>::BW;
+    const cuuint64_t strides[2] = {(cuuint64_t)p.zr * es, (cuuint64_t)p.zr * es * (cuuint64_t)p.yr};
     const cuuint32_t estr[3] = {1, 1, 1};
     const cuuint32_t boxe[3] = {BW, BROWS_E, 1}, boxh[3] = {BW, BROWS_H, 1}, boxc[3] = {BWC, BROWS_H, 1};
     for (int c = 0; c < 3; c++) {
-        if (enc(&out->e[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, f[c], dims, strides, boxe, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        if (enc(&out->e[c], dtype, 3, f[c], dims, strides, boxe, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return -1;
-        if (enc(&out->h[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, f[3 + c], dims, strides, boxh, estr,
+        if (enc(&out->h[c], dtype, 3, f[3 + c], dims, strides, boxh, estr,
                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return -1;

@@ -20,12 +20,13 @@ struct BulkItem {
 
 #define BULK_TILE 31
 
-size_t bulk_smem_bytes(int nclasses);
-cudaError_t bulk_configure(int nclasses);
+size_t bulk_smem_bytes(int nclasses, int storage);
+cudaError_t bulk_configure();
 cudaError_t launch_bulk(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade,
-                        int npoles, cudaStream_t st);
+                        int npoles, int storage, cudaStream_t st);
 // all items of many plans in one persistent launch of `grid` CTAs; plans and
 // maps are device tables of this step's parity, indexed by BulkItem::inst
 cudaError_t launch_bulk_batch(const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems, int grid,
-                              int ncls_layout, int *err, bool ade, int npoles, cudaStream_t st);
-int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, BulkMaps *out);
+                              int ncls_layout, int *err, bool ade, int npoles, int storage, cudaStream_t st);
+int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, int storage,
+                   BulkMaps *out);

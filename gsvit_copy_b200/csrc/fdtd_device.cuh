@@ -3,7 +3,154 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "fdtd_internal.h"
+
+// ---- field storage: FP32, FP16 or BF16 elements behind the float pointers
+// of DevPlan; arithmetic is FP32 throughout.  Stor<T>::scaled tells whether
+// H and psi carry the power-of-two scales of DevPlan (16-bit storage only).
+template <class T>
+struct Stor;
+
+// murmur3's 32-bit finaliser: a bijection with full avalanche, used as the
+// random source of stochastic rounding (deterministic given cell, step and array)
+__device__ __forceinline__ uint32_t sr_mix(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x85ebca6bu;
+    x ^= x >> 13;
+    x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x;
+}
+
+// per-step, per-array seed of the rounding dither (array: 0-5 the field
+// components, 6-17 psi_E, 18-29 psi_H)
+__device__ __forceinline__ uint32_t sr_seed(uint32_t step, uint32_t array)
+{
+    return sr_mix(step * 0x9e3779b9u ^ (array + 1u) * 0x27d4eb2fu);
+}
+
+template <>
+struct Stor<float> {
+    static constexpr bool scaled = false;
+    static constexpr bool stochastic = false;
+    __device__ static float ld(const float *p, int64_t i) { return p[i]; }
+    __device__ static float ldg(const float *p, int64_t i) { return __ldg(p + i); }
+    __device__ static void st(float *p, int64_t i, float v) { p[i] = v; }
+    __device__ static float cvt(float v) { return v; }
+};
+template <>
+struct Stor<__half> {
+    static constexpr bool scaled = true;
+    static constexpr bool stochastic = false;
+    __device__ static float ld(const float *p, int64_t i) { return __half2float(reinterpret_cast<const __half *>(p)[i]); }
+    __device__ static float ldg(const float *p, int64_t i) { return __half2float(__ldg(reinterpret_cast<const __half *>(p) + i)); }
+    __device__ static void st(float *p, int64_t i, float v) { reinterpret_cast<__half *>(p)[i] = __float2half_rn(v); }
+    __device__ static float cvt(__half v) { return __half2float(v); }
+};
+template <>
+struct Stor<__nv_bfloat16> {
+    // BF16 keeps 8 significant bits: round to nearest would drop every
+    // per-step increment below half an ulp (a wave resolved by hundreds of
+    // steps per period stalls), so stores round stochastically -- the 16
+    // dropped bits are compared against a uniform random number, which makes
+    // the stored value an unbiased estimate of the FP32 result.
+    static constexpr bool scaled = true;
+    static constexpr bool stochastic = true;
+    __device__ static float ld(const float *p, int64_t i)
+    {
+        return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(p)[i]);
+    }
+    __device__ static float ldg(const float *p, int64_t i)
+    {
+        return __bfloat162float(__ldg(reinterpret_cast<const __nv_bfloat16 *>(p) + i));
+    }
+    __device__ static void st(float *p, int64_t i, float v) { reinterpret_cast<__nv_bfloat16 *>(p)[i] = __float2bfloat16_rn(v); }
+    __device__ static void st_sr(float *p, int64_t i, float v, uint32_t seed)
+    {
+        uint32_t u = __float_as_uint(v);
+        if ((u & 0x7f800000u) != 0x7f800000u) u += sr_mix((uint32_t)i ^ seed) & 0xffffu;   // finite values only
+        reinterpret_cast<uint16_t *>(p)[i] = (uint16_t)(u >> 16);
+    }
+    __device__ static float cvt(__nv_bfloat16 v) { return __bfloat162float(v); }
+};
+
+// one element of a field stored as FDTD_STORE_* `storage` (small kernels
+// that read a few values per thread branch on it at run time)
+__device__ __forceinline__ float ld_any(const float *p, int64_t i, int storage)
+{
+    if (storage == 1) return Stor<__half>::ld(p, i);
+    if (storage == 2) return Stor<__nv_bfloat16>::ld(p, i);
+    return p[i];
+}
+
+// E (unscaled), H (times hs), psi_H (times ps) and psi_E (times pse) element
+// access.  Stores take the step number `stp` (sr_step) and the array index of
+// sr_seed, which only stochastic rounding uses.
+template <class T>
+__device__ __forceinline__ uint32_t sr_step(const DevPlan &P)
+{
+    if constexpr (Stor<T>::stochastic) return (uint32_t)__ldg(P.stepc);
+    else return 0u;
+}
+template <class T>
+__device__ __forceinline__ void st_any(float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+{
+    if constexpr (Stor<T>::stochastic) Stor<T>::st_sr(p, i, v, sr_seed(stp, array));
+    else Stor<T>::st(p, i, v);
+}
+template <class T>
+__device__ __forceinline__ float ldE(const float *p, int64_t i) { return Stor<T>::ld(p, i); }
+template <class T>
+__device__ __forceinline__ float ldgE(const float *p, int64_t i) { return Stor<T>::ldg(p, i); }
+template <class T>
+__device__ __forceinline__ void stE(float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+{
+    st_any<T>(p, i, v, stp, array);
+}
+template <class T>
+__device__ __forceinline__ float ldH(const DevPlan &P, const float *p, int64_t i)
+{
+    return Stor<T>::scaled ? Stor<T>::ld(p, i) * P.ihs : Stor<T>::ld(p, i);
+}
+template <class T>
+__device__ __forceinline__ float ldgH(const DevPlan &P, const float *p, int64_t i)
+{
+    return Stor<T>::scaled ? Stor<T>::ldg(p, i) * P.ihs : Stor<T>::ldg(p, i);
+}
+template <class T>
+__device__ __forceinline__ void stH(const DevPlan &P, float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+{
+    st_any<T>(p, i, Stor<T>::scaled ? v * P.hs : v, stp, array);
+}
+template <class T>
+__device__ __forceinline__ float ldPsi(const DevPlan &P, const float *p, int64_t i)
+{
+    return Stor<T>::scaled ? Stor<T>::ld(p, i) * P.ips : Stor<T>::ld(p, i);
+}
+template <class T>
+__device__ __forceinline__ float ldgPsi(const DevPlan &P, const float *p, int64_t i)
+{
+    return Stor<T>::scaled ? Stor<T>::ldg(p, i) * P.ips : Stor<T>::ldg(p, i);
+}
+template <class T>
+__device__ __forceinline__ void stPsi(const DevPlan &P, float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+{
+    st_any<T>(p, i, Stor<T>::scaled ? v * P.ps : v, stp, array);
+}
+template <class T>
+__device__ __forceinline__ float ldPsiE(const DevPlan &P, const float *p, int64_t i)
+{
+    return Stor<T>::scaled ? Stor<T>::ld(p, i) * P.ipse : Stor<T>::ld(p, i);
+}
+template <class T>
+__device__ __forceinline__ void stPsiE(const DevPlan &P, float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+{
+    st_any<T>(p, i, Stor<T>::scaled ? v * P.pse : v, stp, array);
+}
 
 __device__ __forceinline__ int cls_at(const DevPlan &P, int i, int j, int k)
 {

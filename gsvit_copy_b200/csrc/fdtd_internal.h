@@ -71,6 +71,12 @@ struct DevPlan {
     int xr, yr, zr;
     int64_t si, sj;                 // strides of i and j (k stride is 1)
     float dx;                       // cell size (cubic cells)
+    // 16-bit field storage (FDTD_STORE_F16 / _BF16): H is stored times hs,
+    // psi_H times ps and psi_E times pse (powers of two, so the scaling is
+    // exact); FP32 storage uses none of them.  The field and psi pointers
+    // below then point to 16-bit elements.
+    float hs, ihs, ps, ips, pse, ipse;
+    const int *stepc;               // device step counter (seeds the BF16 stochastic rounding)
     // fields: [0..2] = E x,y,z, [3..5] = H x,y,z
     const float *fin[6];
     float *fout[6];

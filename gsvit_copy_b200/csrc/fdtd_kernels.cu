@@ -19,6 +19,7 @@
 // byte through HBM (49 B); halo reads are served by L1/L2.
 #include <cuda_runtime.h>
 
+#include "../../include/gsvit_b200.h"
 #include "fdtd_device.cuh"
 #include "fdtd_kernels.cuh"
 
@@ -35,9 +36,11 @@ enum { X0 = 0, XN = 1, Y0 = 2, YN = 3, Z0 = 4, ZN = 5 };
 // xn yn zn), TSF H corrections (source.c:1476-1672) and the outer H planes
 // zeroed by boundary_hstep (boundary.c:418-420, 455-457, 490-492), applied to
 // H after ystep_h.  `owner` cells write their psi_H.
+template <class T>
 __device__ __noinline__ float3 h_special(const DevPlan &P, int i, int j, int k, bool owner, float db, float dey_i,
                                          float dez_i, float dex_j, float dez_j, float dex_k, float dey_k, float3 hin)
 {
+    const uint32_t stp = sr_step<T>(P);
     float hx = hin.x, hy = hin.y, hz = hin.z;
     const int xr = P.xr, yr = P.yr, zr = P.zr;
     const bool il = (i == xr - 1), jl = (j == yr - 1), kl = (k == zr - 1);
@@ -48,29 +51,29 @@ __device__ __noinline__ float3 h_special(const DevPlan &P, int i, int j, int k, 
     if (P.cp_on[X0] && i < P.cp_d[X0] - 1 && jin && kin) {
         const int64_t q = ((int64_t)i * yr + j) * zr + k;
         const float bh = __ldg(P.bh[X0] + i), ch = __ldg(P.ch[X0] + i);
-        float pzx = bh * __ldg(P.psih_in[X0][1] + q) + ch * dey_i * idx_;
-        float pyx = bh * __ldg(P.psih_in[X0][0] + q) + ch * dez_i * idx_;
+        float pzx = bh * ldgPsi<T>(P, P.psih_in[X0][1], q) + ch * dey_i * idx_;
+        float pyx = bh * ldgPsi<T>(P, P.psih_in[X0][0], q) + ch * dez_i * idx_;
         hy += dbdx * pyx;
         hz -= dbdx * pzx;
-        if (owner) { P.psih_out[X0][1][q] = pzx; P.psih_out[X0][0][q] = pyx; }
+        if (owner) { stPsi<T>(P, P.psih_out[X0][1], q, pzx, stp, 18 + 2 * X0 + 1); stPsi<T>(P, P.psih_out[X0][0], q, pyx, stp, 18 + 2 * X0 + 0); }
     }
     if (P.cp_on[Y0] && j < P.cp_d[Y0] - 1 && iin && kin) {
         const int64_t q = ((int64_t)i * P.cp_d[Y0] + j) * zr + k;
         const float bh = __ldg(P.bh[Y0] + j), ch = __ldg(P.ch[Y0] + j);
-        float pxy = bh * __ldg(P.psih_in[Y0][0] + q) + ch * dez_j * idx_;
-        float pzy = bh * __ldg(P.psih_in[Y0][1] + q) + ch * dex_j * idx_;
+        float pxy = bh * ldgPsi<T>(P, P.psih_in[Y0][0], q) + ch * dez_j * idx_;
+        float pzy = bh * ldgPsi<T>(P, P.psih_in[Y0][1], q) + ch * dex_j * idx_;
         hx -= dbdx * pxy;
         hz += dbdx * pzy;
-        if (owner) { P.psih_out[Y0][0][q] = pxy; P.psih_out[Y0][1][q] = pzy; }
+        if (owner) { stPsi<T>(P, P.psih_out[Y0][0], q, pxy, stp, 18 + 2 * Y0 + 0); stPsi<T>(P, P.psih_out[Y0][1], q, pzy, stp, 18 + 2 * Y0 + 1); }
     }
     if (P.cp_on[Z0] && k < P.cp_d[Z0] - 1 && iin && jin) {
         const int64_t q = ((int64_t)i * yr + j) * P.cp_d[Z0] + k;
         const float bh = __ldg(P.bh[Z0] + k), ch = __ldg(P.ch[Z0] + k);
-        float pyz = bh * __ldg(P.psih_in[Z0][1] + q) + ch * dex_k * idx_;
-        float pxz = bh * __ldg(P.psih_in[Z0][0] + q) + ch * dey_k * idx_;
+        float pyz = bh * ldgPsi<T>(P, P.psih_in[Z0][1], q) + ch * dex_k * idx_;
+        float pxz = bh * ldgPsi<T>(P, P.psih_in[Z0][0], q) + ch * dey_k * idx_;
         hy -= dbdx * pyz;
         hx += dbdx * pxz;
-        if (owner) { P.psih_out[Z0][1][q] = pyz; P.psih_out[Z0][0][q] = pxz; }
+        if (owner) { stPsi<T>(P, P.psih_out[Z0][1], q, pyz, stp, 18 + 2 * Z0 + 1); stPsi<T>(P, P.psih_out[Z0][0], q, pxz, stp, 18 + 2 * Z0 + 0); }
     }
     if (P.cp_on[XN]) {
         const int d = P.cp_d[XN];
@@ -78,11 +81,11 @@ __device__ __noinline__ float3 h_special(const DevPlan &P, int i, int j, int k, 
             const int ir = i - (xr - d);
             const int64_t q = ((int64_t)ir * yr + j) * zr + k;
             const float bh = __ldg(P.bh[XN] + ir), ch = __ldg(P.ch[XN] + ir);
-            float pzx = bh * __ldg(P.psih_in[XN][1] + q) + ch * dey_i * idx_;
-            float pyx = bh * __ldg(P.psih_in[XN][0] + q) + ch * dez_i * idx_;
+            float pzx = bh * ldgPsi<T>(P, P.psih_in[XN][1], q) + ch * dey_i * idx_;
+            float pyx = bh * ldgPsi<T>(P, P.psih_in[XN][0], q) + ch * dez_i * idx_;
             hy += dbdx * pyx;
             hz -= dbdx * pzx;
-            if (owner) { P.psih_out[XN][1][q] = pzx; P.psih_out[XN][0][q] = pyx; }
+            if (owner) { stPsi<T>(P, P.psih_out[XN][1], q, pzx, stp, 18 + 2 * XN + 1); stPsi<T>(P, P.psih_out[XN][0], q, pyx, stp, 18 + 2 * XN + 0); }
         }
     }
     if (P.cp_on[YN]) {
@@ -91,11 +94,11 @@ __device__ __noinline__ float3 h_special(const DevPlan &P, int i, int j, int k, 
             const int jr = j - (yr - d);
             const int64_t q = ((int64_t)i * d + jr) * zr + k;
             const float bh = __ldg(P.bh[YN] + jr), ch = __ldg(P.ch[YN] + jr);
-            float pxy = bh * __ldg(P.psih_in[YN][0] + q) + ch * dez_j * idx_;
-            float pzy = bh * __ldg(P.psih_in[YN][1] + q) + ch * dex_j * idx_;
+            float pxy = bh * ldgPsi<T>(P, P.psih_in[YN][0], q) + ch * dez_j * idx_;
+            float pzy = bh * ldgPsi<T>(P, P.psih_in[YN][1], q) + ch * dex_j * idx_;
             hx -= dbdx * pxy;
             hz += dbdx * pzy;
-            if (owner) { P.psih_out[YN][0][q] = pxy; P.psih_out[YN][1][q] = pzy; }
+            if (owner) { stPsi<T>(P, P.psih_out[YN][0], q, pxy, stp, 18 + 2 * YN + 0); stPsi<T>(P, P.psih_out[YN][1], q, pzy, stp, 18 + 2 * YN + 1); }
         }
     }
     if (P.cp_on[ZN]) {
@@ -104,11 +107,11 @@ __device__ __noinline__ float3 h_special(const DevPlan &P, int i, int j, int k, 
             const int kr = k - (zr - d);
             const int64_t q = ((int64_t)i * yr + j) * d + kr;
             const float bh = __ldg(P.bh[ZN] + kr), ch = __ldg(P.ch[ZN] + kr);
-            float pyz = bh * __ldg(P.psih_in[ZN][1] + q) + ch * dex_k * idx_;
-            float pxz = bh * __ldg(P.psih_in[ZN][0] + q) + ch * dey_k * idx_;
+            float pyz = bh * ldgPsi<T>(P, P.psih_in[ZN][1], q) + ch * dex_k * idx_;
+            float pxz = bh * ldgPsi<T>(P, P.psih_in[ZN][0], q) + ch * dey_k * idx_;
             hy -= dbdx * pyz;
             hx += dbdx * pxz;
-            if (owner) { P.psih_out[ZN][1][q] = pyz; P.psih_out[ZN][0][q] = pxz; }
+            if (owner) { stPsi<T>(P, P.psih_out[ZN][1], q, pyz, stp, 18 + 2 * ZN + 1); stPsi<T>(P, P.psih_out[ZN][0], q, pxz, stp, 18 + 2 * ZN + 0); }
         }
     }
     if ((P.cp_on[XN] && il && jin && kin) || (P.cp_on[YN] && jl && iin && kin) || (P.cp_on[ZN] && kl && iin && jin))
@@ -118,6 +121,7 @@ __device__ __noinline__ float3 h_special(const DevPlan &P, int i, int j, int k, 
 
 // H^{n+1/2}(i) at one cell from E^n and the six E differences (ystep_h,
 // yee.c:246-256, then h_special where the cell lies in a slab or on a face).
+template <class T>
 __device__ __forceinline__ void h_update(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k,
                                          bool special, bool owner, float dey_i, float dez_i, float dex_j, float dez_j,
                                          float dex_k, float dey_k, float h[3])
@@ -130,7 +134,7 @@ __device__ __forceinline__ void h_update(const DevPlan &P, const float4 *scls, i
     if (!(il || kl)) h[1] = hc.x * h[1] + hc.y * (dez_i * ikx - dex_k * ikz);
     if (!(il || jl)) h[2] = hc.x * h[2] + hc.y * (dex_j * iky - dey_i * ikx);
     if (special) {
-        const float3 o = h_special(P, i, j, k, owner, hc.y, dey_i, dez_i, dex_j, dez_j, dex_k, dey_k,
+        const float3 o = h_special<T>(P, i, j, k, owner, hc.y, dey_i, dez_i, dex_j, dez_j, dex_k, dey_k,
                                    make_float3(h[0], h[1], h[2]));
         h[0] = o.x; h[1] = o.y; h[2] = o.z;
     }
@@ -140,11 +144,12 @@ __device__ __forceinline__ void h_update(const DevPlan &P, const float4 *scls, i
 // (yee.c:914-1108), ordinary update (yee.c:1113-1128), PEC rule
 // (yee.c:1138-1237), boundary_estep zero planes, psi_E and corrections
 // (boundary.c:691-884) and TSF E (source.c:547-771).
-template <bool ADE, int NPOLES>
+template <bool ADE, int NPOLES, class T>
 __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k,
                                          float3 eo3, float3 h3, float hx_jm, float hz_jm, float hx_km, float hy_km,
                                          float hy_im, float hz_im)
 {
+    const uint32_t stp = sr_step<T>(P);
     const float eo[3] = {eo3.x, eo3.y, eo3.z};
     const float h[3] = {h3.x, h3.y, h3.z};
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
@@ -174,12 +179,12 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
     const bool zero = (P.cp_on[X0] && i == 0) || (P.cp_on[Y0] && j == 0) || (P.cp_on[Z0] && k == 0);
     int64_t qx0 = 0, qxn = 0, qy0 = 0, qyn = 0, qz0 = 0, qzn = 0;
     if (!zero) {
-        if (inx0) { qx0 = ((int64_t)i * yr + j) * zr + k; px0[0] = P.psie[X0][0][qx0]; px0[1] = P.psie[X0][1][qx0]; }
-        if (inxn) { qxn = ((int64_t)(i - (xr - P.cp_d[XN])) * yr + j) * zr + k; pxn[0] = P.psie[XN][0][qxn]; pxn[1] = P.psie[XN][1][qxn]; }
-        if (iny0) { qy0 = ((int64_t)i * P.cp_d[Y0] + j) * zr + k; py0[0] = P.psie[Y0][0][qy0]; py0[1] = P.psie[Y0][1][qy0]; }
-        if (inyn) { qyn = ((int64_t)i * P.cp_d[YN] + (j - (yr - P.cp_d[YN]))) * zr + k; pyn[0] = P.psie[YN][0][qyn]; pyn[1] = P.psie[YN][1][qyn]; }
-        if (inz0) { qz0 = ((int64_t)i * yr + j) * P.cp_d[Z0] + k; pz0[0] = P.psie[Z0][0][qz0]; pz0[1] = P.psie[Z0][1][qz0]; }
-        if (inzn) { qzn = ((int64_t)i * yr + j) * P.cp_d[ZN] + (k - (zr - P.cp_d[ZN])); pzn[0] = P.psie[ZN][0][qzn]; pzn[1] = P.psie[ZN][1][qzn]; }
+        if (inx0) { qx0 = ((int64_t)i * yr + j) * zr + k; px0[0] = ldPsiE<T>(P, P.psie[X0][0], qx0); px0[1] = ldPsiE<T>(P, P.psie[X0][1], qx0); }
+        if (inxn) { qxn = ((int64_t)(i - (xr - P.cp_d[XN])) * yr + j) * zr + k; pxn[0] = ldPsiE<T>(P, P.psie[XN][0], qxn); pxn[1] = ldPsiE<T>(P, P.psie[XN][1], qxn); }
+        if (iny0) { qy0 = ((int64_t)i * P.cp_d[Y0] + j) * zr + k; py0[0] = ldPsiE<T>(P, P.psie[Y0][0], qy0); py0[1] = ldPsiE<T>(P, P.psie[Y0][1], qy0); }
+        if (inyn) { qyn = ((int64_t)i * P.cp_d[YN] + (j - (yr - P.cp_d[YN]))) * zr + k; pyn[0] = ldPsiE<T>(P, P.psie[YN][0], qyn); pyn[1] = ldPsiE<T>(P, P.psie[YN][1], qyn); }
+        if (inz0) { qz0 = ((int64_t)i * yr + j) * P.cp_d[Z0] + k; pz0[0] = ldPsiE<T>(P, P.psie[Z0][0], qz0); pz0[1] = ldPsiE<T>(P, P.psie[Z0][1], qz0); }
+        if (inzn) { qzn = ((int64_t)i * yr + j) * P.cp_d[ZN] + (k - (zr - P.cp_d[ZN])); pzn[0] = ldPsiE<T>(P, P.psie[ZN][0], qzn); pzn[1] = ldPsiE<T>(P, P.psie[ZN][1], qzn); }
     }
     if (ADE && (fl & CF_ADE_BRANCH)) {
         const DevAde &A = P.ade[ade_set];
@@ -188,7 +193,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
         float qd[3] = {0, 0, 0}, ep[3] = {0, 0, 0}, pc[3][2], qc[3][2];
         for (int a = 0; a < 3; a++) {
             if (!comp[a]) continue;
-            qd[a] = P.q[a][c]; ep[a] = P.fout[a][c];
+            qd[a] = P.q[a][c]; ep[a] = ldE<T>(P.fout[a], c);
             for (int n = 0; n < NPOLES; n++) { pc[a][n] = P.pc[a][n][c]; qc[a][n] = P.qc[a][n][c]; }
         }
         const float curl[3] = {curlx, curly, curlz};
@@ -276,7 +281,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
             if (j > 0 && k > 0) {
                 if (ty) ny -= dx * cb[1] * px0[0];
                 if (tz) nz += dx * cb[2] * px0[1];
-                P.psie[X0][0][qx0] = px0[0]; P.psie[X0][1][qx0] = px0[1];
+                stPsiE<T>(P, P.psie[X0][0], qx0, px0[0], stp, 6 + 2 * X0 + 0); stPsiE<T>(P, P.psie[X0][1], qx0, px0[1], stp, 6 + 2 * X0 + 1);
             }
         }
         if (iny0) {
@@ -286,7 +291,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
             if (i > 0 && k > 0) {
                 if (tx) nx += dx * cb[0] * py0[0];
                 if (tz) nz -= dx * cb[2] * py0[1];
-                P.psie[Y0][0][qy0] = py0[0]; P.psie[Y0][1][qy0] = py0[1];
+                stPsiE<T>(P, P.psie[Y0][0], qy0, py0[0], stp, 6 + 2 * Y0 + 0); stPsiE<T>(P, P.psie[Y0][1], qy0, py0[1], stp, 6 + 2 * Y0 + 1);
             }
         }
         if (inz0) {
@@ -296,7 +301,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
             if (i > 0 && j > 0) {
                 if (ty) ny += dx * cb[1] * pz0[1];
                 if (tz) nx -= dx * cb[0] * pz0[0];     // gated by ztbc in the reference (boundary.c:758-759)
-                P.psie[Z0][0][qz0] = pz0[0]; P.psie[Z0][1][qz0] = pz0[1];
+                stPsiE<T>(P, P.psie[Z0][0], qz0, pz0[0], stp, 6 + 2 * Z0 + 0); stPsiE<T>(P, P.psie[Z0][1], qz0, pz0[1], stp, 6 + 2 * Z0 + 1);
             }
         }
         if (inxn) {
@@ -307,7 +312,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
             if (j > 0 && k > 0) {
                 if (ty) ny -= dx * cb[1] * pxn[0];
                 if (tz) nz += dx * cb[2] * pxn[1];
-                P.psie[XN][0][qxn] = pxn[0]; P.psie[XN][1][qxn] = pxn[1];
+                stPsiE<T>(P, P.psie[XN][0], qxn, pxn[0], stp, 6 + 2 * XN + 0); stPsiE<T>(P, P.psie[XN][1], qxn, pxn[1], stp, 6 + 2 * XN + 1);
             }
         }
         if (inyn) {
@@ -318,7 +323,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
             if (i > 0 && k > 0) {
                 if (tx) nx += dx * cb[0] * pyn[0];
                 if (tz) nz -= dx * cb[2] * pyn[1];
-                P.psie[YN][0][qyn] = pyn[0]; P.psie[YN][1][qyn] = pyn[1];
+                stPsiE<T>(P, P.psie[YN][0], qyn, pyn[0], stp, 6 + 2 * YN + 0); stPsiE<T>(P, P.psie[YN][1], qyn, pyn[1], stp, 6 + 2 * YN + 1);
             }
         }
         if (inzn) {
@@ -329,7 +334,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
             if (i > 0 && j > 0) {
                 if (ty) ny += dx * cb[1] * pzn[1];
                 if (tx) nx -= dx * cb[0] * pzn[0];
-                P.psie[ZN][0][qzn] = pzn[0]; P.psie[ZN][1][qzn] = pzn[1];
+                stPsiE<T>(P, P.psie[ZN][0], qzn, pzn[0], stp, 6 + 2 * ZN + 0); stPsiE<T>(P, P.psie[ZN][1], qzn, pzn[1], stp, 6 + 2 * ZN + 1);
             }
         }
     }
@@ -362,64 +367,70 @@ __device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &
 
 // 3 CTAs per SM: the slab kernels are latency-bound, and 24 resident warps
 // beat the register spill this costs e_special (1.95 -> 1.60 ms per 512^3 step)
+template <class T>
 __device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int k)
 {
+    const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
     const float *EX = P.fin[0], *EY = P.fin[1], *EZ = P.fin[2];
-    const float ex = __ldg(EX + c), ey = __ldg(EY + c), ez = __ldg(EZ + c);
+    const float ex = ldgE<T>(EX, c), ey = ldgE<T>(EY, c), ez = ldgE<T>(EZ, c);
     const bool il = (i == P.xr - 1), jl = (j == P.yr - 1), kl = (k == P.zr - 1);
-    const float eyk = kl ? 0.f : __ldg(EY + c + 1), exk = kl ? 0.f : __ldg(EX + c + 1);
-    const float ezj = jl ? 0.f : __ldg(EZ + c + P.sj), exj = jl ? 0.f : __ldg(EX + c + P.sj);
-    const float ezi = il ? 0.f : __ldg(EZ + c + P.si), eyi = il ? 0.f : __ldg(EY + c + P.si);
-    float h[3] = {__ldg(P.fin[3] + c), __ldg(P.fin[4] + c), __ldg(P.fin[5] + c)};
+    const float eyk = kl ? 0.f : ldgE<T>(EY, c + 1), exk = kl ? 0.f : ldgE<T>(EX, c + 1);
+    const float ezj = jl ? 0.f : ldgE<T>(EZ, c + P.sj), exj = jl ? 0.f : ldgE<T>(EX, c + P.sj);
+    const float ezi = il ? 0.f : ldgE<T>(EZ, c + P.si), eyi = il ? 0.f : ldgE<T>(EY, c + P.si);
+    float h[3] = {ldgH<T>(P, P.fin[3], c), ldgH<T>(P, P.fin[4], c), ldgH<T>(P, P.fin[5], c)};
     const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
-    h_update(P, cl, cls_at(P, i, j, k), i, j, k, true, true, eyi - ey, ezi - ez, exj - ex, ezj - ez, exk - ex, eyk - ey, h);
-    P.fout[3][c] = h[0];
-    P.fout[4][c] = h[1];
-    P.fout[5][c] = h[2];
+    h_update<T>(P, cl, cls_at(P, i, j, k), i, j, k, true, true, eyi - ey, ezi - ez, exj - ex, ezj - ez, exk - ex, eyk - ey, h);
+    stH<T>(P, P.fout[3], c, h[0], stp, 3);
+    stH<T>(P, P.fout[4], c, h[1], stp, 4);
+    stH<T>(P, P.fout[5], c, h[2], stp, 5);
 }
 
+template <class T>
 __global__ void __launch_bounds__(256, 3) slab_h_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell(P, i, j, k);
+    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell<T>(P, i, j, k);
 }
 
+template <class T>
 __global__ void __launch_bounds__(256, 3) slab_h_batch(const DevPlan *plans, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell(plans[inst], i, j, k);
+    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell<T>(plans[inst], i, j, k);
 }
 
-template <bool ADE, int NPOLES>
+template <bool ADE, int NPOLES, class T>
 __device__ __forceinline__ void slab_e_cell(const DevPlan &P, int i, int j, int k)
 {
+    const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
     const float *HX = P.fout[3], *HY = P.fout[4], *HZ = P.fout[5];   // H^{n+1/2}, written this step
-    const float3 eo = make_float3(__ldg(P.fin[0] + c), __ldg(P.fin[1] + c), __ldg(P.fin[2] + c));
-    const float3 h = make_float3(HX[c], HY[c], HZ[c]);
-    const float hx_jm = j > 0 ? HX[c - P.sj] : 0.f, hz_jm = j > 0 ? HZ[c - P.sj] : 0.f;
-    const float hx_km = k > 0 ? HX[c - 1] : 0.f, hy_km = k > 0 ? HY[c - 1] : 0.f;
-    const float hy_im = i > 0 ? HY[c - P.si] : 0.f, hz_im = i > 0 ? HZ[c - P.si] : 0.f;
+    const float3 eo = make_float3(ldgE<T>(P.fin[0], c), ldgE<T>(P.fin[1], c), ldgE<T>(P.fin[2], c));
+    const float3 h = make_float3(ldH<T>(P, HX, c), ldH<T>(P, HY, c), ldH<T>(P, HZ, c));
+    const float hx_jm = j > 0 ? ldH<T>(P, HX, c - P.sj) : 0.f, hz_jm = j > 0 ? ldH<T>(P, HZ, c - P.sj) : 0.f;
+    const float hx_km = k > 0 ? ldH<T>(P, HX, c - 1) : 0.f, hy_km = k > 0 ? ldH<T>(P, HY, c - 1) : 0.f;
+    const float hy_im = i > 0 ? ldH<T>(P, HY, c - P.si) : 0.f, hz_im = i > 0 ? ldH<T>(P, HZ, c - P.si) : 0.f;
     const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
-    const float3 en = e_special<ADE, NPOLES>(P, cl, cls_at(P, i, j, k), i, j, k, eo, h, hx_jm, hz_jm, hx_km, hy_km, hy_im, hz_im);
-    P.fout[0][c] = en.x;
-    P.fout[1][c] = en.y;
-    P.fout[2][c] = en.z;
+    const float3 en =
+        e_special<ADE, NPOLES, T>(P, cl, cls_at(P, i, j, k), i, j, k, eo, h, hx_jm, hz_jm, hx_km, hy_km, hy_im, hz_im);
+    stE<T>(P.fout[0], c, en.x, stp, 0);
+    stE<T>(P.fout[1], c, en.y, stp, 1);
+    stE<T>(P.fout[2], c, en.z, stp, 2);
 }
 
-template <bool ADE, int NPOLES>
+template <bool ADE, int NPOLES, class T>
 __global__ void __launch_bounds__(256, 3) slab_e_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_e_cell<ADE, NPOLES>(P, i, j, k);
+    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_e_cell<ADE, NPOLES, T>(P, i, j, k);
 }
 
-template <bool ADE, int NPOLES>
+template <bool ADE, int NPOLES, class T>
 __global__ void __launch_bounds__(256, 3) slab_e_batch(const DevPlan *plans, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_e_cell<ADE, NPOLES>(plans[inst], i, j, k);
+    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_e_cell<ADE, NPOLES, T>(plans[inst], i, j, k);
 }
 
 // ------------------------------------------------------------ TSF face tables
@@ -533,7 +544,7 @@ __device__ __forceinline__ void aux_step_body(const DevAux &A)
     if (s > 0 && s - 1 < A.nsteps_planned) {
         for (int q = tid; q < A.nprobes * 6; q += nt) {
             int p = q / 6, comp = q % 6;
-            A.probe_out[((size_t)p * A.nsteps_planned + (s - 1)) * 6 + comp] = (double)A.fields[comp][A.probe_cells[p]];
+            A.probe_out[((size_t)p * A.nsteps_planned + (s - 1)) * 6 + comp] = (double)(ld_any(A.fields[comp], A.probe_cells[p], A.storage) * (comp >= 3 && A.storage ? A.ihs : 1.f));
         }
     }
     if (A.res > 0) {
@@ -570,7 +581,7 @@ __global__ void probe_capture_kernel(const DevAux A)
     if (s < 1 || s - 1 >= A.nsteps_planned) return;
     for (int q = threadIdx.x; q < A.nprobes * 6; q += blockDim.x) {
         int p = q / 6, comp = q % 6;
-        A.probe_out[((size_t)p * A.nsteps_planned + (s - 1)) * 6 + comp] = (double)A.fields[comp][A.probe_cells[p]];
+        A.probe_out[((size_t)p * A.nsteps_planned + (s - 1)) * 6 + comp] = (double)(ld_any(A.fields[comp], A.probe_cells[p], A.storage) * (comp >= 3 && A.storage ? A.ihs : 1.f));
     }
 }
 
@@ -587,8 +598,8 @@ __device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
     double v[6];
     for (int a = 0; a < 3; a++) {
         const float *E = N.e[a];
-        v[a] = (double)E[c];
-        v[3 + a] = ((double)E[c + st] - (double)E[c - st]) * N.inv2dx;
+        v[a] = (double)ld_any(E, c, N.storage);
+        v[3 + a] = ((double)ld_any(E, c + st, N.storage) - (double)ld_any(E, c - st, N.storage)) * N.inv2dx;
     }
     for (int f = 0; f < N.nfreq; f++) {
         double sn, cs;
@@ -733,8 +744,8 @@ __global__ void nfff_series_kernel(const DevNfffSeries S)
     double ev[3], dv[3];
     for (int a = 0; a < 3; a++) {
         const float *E = S.e[a];
-        ev[a] = (double)E[cc];
-        dv[a] = (double)E[cc + st] - (double)E[cc - st];
+        ev[a] = (double)ld_any(E, cc, S.storage);
+        dv[a] = (double)ld_any(E, cc + st, S.storage) - (double)ld_any(E, cc - st, S.storage);
     }
     const double size = __dmul_rn(dx, dx);
     const double pos = (fc & 1) ? 1.0 : -1.0;
@@ -778,18 +789,27 @@ void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st)
     if (total > 0) tsf_face_kernel<<<(total + 255) / 256, 256, 0, st>>>(p, total);
 }
 
+template <class T>
+cudaError_t slab_steps_t(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
+                         cudaStream_t st)
+{
+    slab_h_kernel<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    if (!ade)
+        slab_e_kernel<false, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    else if (npoles == 0)
+        slab_e_kernel<true, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    else
+        slab_e_kernel<true, 2, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
-                              cudaStream_t st)
+                              int storage, cudaStream_t st)
 {
     if (nblocks <= 0) return cudaSuccess;
-    slab_h_kernel<<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    if (!ade)
-        slab_e_kernel<false, 0><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    else if (npoles == 0)
-        slab_e_kernel<true, 0><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    else
-        slab_e_kernel<true, 2><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    return cudaGetLastError();
+    if (storage == FDTD_STORE_F16) return slab_steps_t<__half>(p, boxes, nboxes, nblocks, ade, npoles, st);
+    if (storage == FDTD_STORE_BF16) return slab_steps_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, ade, npoles, st);
+    return slab_steps_t<float>(p, boxes, nboxes, nblocks, ade, npoles, st);
 }
 
 void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st)
@@ -802,18 +822,27 @@ void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStr
     if (nplans > 0 && max_cells > 0) tsf_face_batch<<<dim3((max_cells + 255) / 256, nplans), 256, 0, st>>>(p);
 }
 
+template <class T>
+cudaError_t slab_steps_batch_t(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
+                               cudaStream_t st)
+{
+    slab_h_batch<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    if (!ade)
+        slab_e_batch<false, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    else if (npoles == 0)
+        slab_e_batch<true, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    else
+        slab_e_batch<true, 2, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade,
-                                    int npoles, cudaStream_t st)
+                                    int npoles, int storage, cudaStream_t st)
 {
     if (nblocks <= 0) return cudaSuccess;
-    slab_h_batch<<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    if (!ade)
-        slab_e_batch<false, 0><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    else if (npoles == 0)
-        slab_e_batch<true, 0><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    else
-        slab_e_batch<true, 2><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    return cudaGetLastError();
+    if (storage == FDTD_STORE_F16) return slab_steps_batch_t<__half>(p, boxes, nboxes, nblocks, ade, npoles, st);
+    if (storage == FDTD_STORE_BF16) return slab_steps_batch_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, ade, npoles, st);
+    return slab_steps_batch_t<float>(p, boxes, nboxes, nblocks, ade, npoles, st);
 }
 
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st)

@@ -21,6 +21,8 @@ struct DevAux {                 // 1D auxiliary grid of the TSF source (1dpool.c
     const float *const *fields; // 6 pointers to the field set that holds the previous step
     double *probe_out;          // [p][nsteps][6]
     int nsteps_planned;
+    int storage;                // FDTD_STORE_* of the fields
+    float ihs;                  // 1 / H storage scale
 };
 
 struct DevNfff {
@@ -33,6 +35,7 @@ struct DevNfff {
     const double *omega_dt;     // nfreq
     const int *step;            // device step counter (already advanced)
     double inv2dx;
+    int storage;                // FDTD_STORE_* of the fields
 };
 
 // a box of cells handled one thread per cell; blocks [first_block, next box's first_block)
@@ -49,12 +52,12 @@ void launch_aux_step(const DevAux &a, cudaStream_t st);
 void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st);
 void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStream_t st);
 cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade,
-                                    int npoles, cudaStream_t st);
+                                    int npoles, int storage, cudaStream_t st);
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st);
 void launch_probe_capture(const DevAux &a, cudaStream_t st);
 void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st);
 cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
-                              cudaStream_t st);
+                              int storage, cudaStream_t st);
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st);
 
 struct DevFarfield {
@@ -88,6 +91,7 @@ struct DevNfffSeries {
     double *series;             // [(p*3 + c)*ndata + m]
     const int *step;            // device step counter (already advanced)
     double dx, dt;
+    int storage;                // FDTD_STORE_* of the fields
 };
 void launch_nfff_series(const DevNfffSeries &s, cudaStream_t st);
 

@@ -68,7 +68,15 @@ extern "C" {
 #define FDTD_FACE_Z0 4
 #define FDTD_FACE_ZN 5
 
-/* field storage precision of the device copy (arithmetic is always FP32) */
+/* field storage precision of the device copy (arithmetic is always FP32).
+ * F16 / BF16 hold the six field components and the CPML psi slabs as 16-bit
+ * numbers (H times 2^9, psi_H times the power of two nearest dx, psi_E times
+ * that and 2^9); the Drude/critical-point state and the far-field
+ * accumulators stay FP32/FP64.  BF16 stores round stochastically (a
+ * deterministic hash of cell, array and step), F16 stores to nearest.  The
+ * bulk kernel needs z rows of a multiple of 16 bytes (zres a multiple of 8
+ * at 16 bits).  No counterpart in the reference, which stores FP32 on the GPU
+ * (gpu.c:805-1172). */
 #define FDTD_STORE_F32   0
 #define FDTD_STORE_F16   1
 #define FDTD_STORE_BF16  2

@@ -89,7 +89,7 @@ def _create(desc):
     (lambda s, d: setattr(d, "xres", 2), -1, "at least 3"),
     (lambda s, d: setattr(d, "dt", -1.0), -1, "positive"),
     (lambda s, d: setattr(d, "dy", d.dx * 2), -2, "non-cubic"),
-    (lambda s, d: setattr(d, "storage", 7), -2, "storage"),
+    (lambda s, d: setattr(d, "storage", 7), -1, "storage"),
     (lambda s, d: setattr(d.tsf, "theta", 4.0), -1, "theta"),
     (lambda s, d: setattr(d.cpml[0], "depth", 1), -1, "CPML depth"),
 ])
