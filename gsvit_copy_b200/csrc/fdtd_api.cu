@@ -206,15 +206,15 @@ std::vector<BulkItem> bulk_items(const int lo[3], const int hi[3], int len, int 
 {
     std::vector<BulkItem> blk;
     for (int ib = lo[0]; ib < hi[0]; ib += len)
-        for (int j0 = lo[1]; j0 < hi[1]; j0 += BULK_TILE)
-            for (int k0 = lo[2]; k0 < hi[2]; k0 += BULK_TILE)
+        for (int j0 = lo[1]; j0 < hi[1]; j0 += BULK_TJ)
+            for (int k0 = lo[2]; k0 < hi[2]; k0 += BULK_TK)
                 blk.push_back({j0, k0, ib, std::min(hi[0], ib + len), hi[1], hi[2], inst, 0});
     return blk;
 }
 
 int bulk_tiles(const int lo[3], const int hi[3])
 {
-    return ((hi[1] - lo[1] + BULK_TILE - 1) / BULK_TILE) * ((hi[2] - lo[2] + BULK_TILE - 1) / BULK_TILE);
+    return ((hi[1] - lo[1] + BULK_TJ - 1) / BULK_TJ) * ((hi[2] - lo[2] + BULK_TK - 1) / BULK_TK);
 }
 
 int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool pole_arrays);
@@ -605,9 +605,10 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         if (f.nfreq > 0) bytes += (double)cell.size() * (9.0 * esz + (double)f.nfreq * 6 * 16 * 2);
     }
     // work decomposition: the bulk box (outside every CPML slab, one extra
-    // plane on the low sides so that its halo row/column/plane is slab-free)
-    // goes to the TMA kernel when the k rows are 16-byte multiples; the rest
-    // (slabs, zeroed planes) to the general kernel
+    // plane on the low sides so that its halo row/column/plane is slab-free,
+    // off the grid's edge planes, k bounds multiples of 4) goes to the TMA
+    // kernel when the k rows are 16-byte multiples; the rest (slabs, edge
+    // planes) to the general kernel
     {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -615,9 +616,11 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         int lo[3], hi[3];
         const int res[3] = {X, Y, Z};
         for (int ax = 0; ax < 3; ax++) {
-            lo[ax] = hp.cp[2 * ax].enabled ? hp.cp[2 * ax].depth + 1 : 0;
-            hi[ax] = hp.cp[2 * ax + 1].enabled ? res[ax] - hp.cp[2 * ax + 1].depth : res[ax];
+            lo[ax] = std::max(1, hp.cp[2 * ax].enabled ? hp.cp[2 * ax].depth + 1 : 0);
+            hi[ax] = std::min(res[ax] - 1, hp.cp[2 * ax + 1].enabled ? res[ax] - hp.cp[2 * ax + 1].depth : res[ax]);
         }
+        lo[2] = std::max(4, (lo[2] + 3) / 4 * 4);   // the k halo group k0-4..k0-1 stays in the grid
+        hi[2] = hi[2] / 4 * 4;
         const char *nob = getenv("GSVIT_B200_NO_BULK");
         P->bulk_on = ((size_t)Z * esz % 16 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
         std::vector<SlabBox> boxes;

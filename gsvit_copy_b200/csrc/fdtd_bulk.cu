@@ -1,20 +1,25 @@
 // fdtd_bulk.cu -- TMA-staged fused step for the bulk of the grid.
 //
-// The bulk region is every cell outside the CPML slabs (their H/E updates,
-// psi recursions and zeroed planes are done by the general kernel).  Inside
-// it a step is: ystep_h (yee.c:146-265) + TSF H (source.c:1464-1672), then
-// ystep_e with the ADE branch and the PEC rule (yee.c:530-1247) + TSF E
-// (source.c:547-771).  kappa is 1 everywhere here.
+// The bulk region is every cell outside the CPML slabs and off the grid's
+// edge planes (their H/E updates, psi recursions and zeroed planes are done by
+// the general kernel).  Inside it a step is: ystep_h (yee.c:146-265) + TSF H
+// (source.c:1464-1672), then ystep_e with the ADE branch and the PEC rule
+// (yee.c:530-1247) + TSF E (source.c:547-771).  kappa is 1 everywhere here and
+// no edge test of the reference applies.
 //
-// A CTA owns 31 x 31 (j,k) cells of every plane of its i-chunk.  Its 8 warps
-// compute H on the 32 x 32 cells [j0-1, j0+31) x [k0-1, k0+31) -- the own
-// cells plus the row and column the E update needs from its neighbours --
-// with warp w on rows 4w..4w+3 and lane = column, then E on the own cells.
-// Thread 0 streams the planes through a 3-stage shared-memory ring with
-// cp.async.bulk.tensor (TMA) two planes ahead: E(p) box 36 x 33, H(p) box
-// 36 x 32 (floats, k innermost) and the class byte box 48 x 32, completion
-// on one mbarrier per stage.  Every wait is bounded; a CTA that gives up sets
-// the error word and returns after draining its copies.
+// A CTA owns 15 x 60 (j,k) cells of every plane of its i-chunk.  Thread
+// (r, g), r = tid / 16, g = tid % 16, holds the four consecutive k cells
+// k0 - 4 + 4g .. k0 - 1 + 4g of row j0 - 1 + r: the 16 x 64 cells on which H
+// is computed are the own cells plus the row and the k group the E update
+// needs from its neighbours.  Fields move as 4-vectors (16-byte shared and
+// global accesses; 8 bytes at 16-bit storage).  The H row above comes through
+// a double-buffered exchange, so that one barrier per plane suffices; the k
+// neighbour through a shuffle; the plane below stays in registers, and so
+// does E(i+1), which becomes the next plane's own E.  Thread 0 streams the
+// planes through a 3-stage shared-memory ring with cp.async.bulk.tensor (TMA)
+// two planes ahead: E(p) box 17 rows, H(p) box 16 rows, class bytes 16 rows,
+// completion on one mbarrier per stage.  Every wait is bounded; a CTA that
+// gives up sets the error word and returns after draining its copies.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -24,27 +29,34 @@
 
 namespace {
 
-// Box geometry per storage type T: E boxes BW x 33 and H boxes BW x 32
-// elements (k innermost) from the aligned column ka <= k0 - 1, the class byte
-// box 48 x 32 from ka8.  TMA needs the box start x and the inner box extent in
-// multiples of 16 bytes: 4 floats / 8 16-bit elements.
-constexpr int BROWS_E = 33, BROWS_H = 32, BWC = 48;
-constexpr int S = 3;
-constexpr int CBOX = BROWS_H * BWC;                        // 1536 B
-template <class T>
-struct Geo {
-    static constexpr int XAL = 16 / (int)sizeof(T);                        // x alignment (elements)
-    static constexpr int BW = sizeof(T) == 4 ? 36 : 40;                     // box width (elements)
-    static constexpr int EBOX = BROWS_E * BW * (int)sizeof(T);              // 4752 / 2640 B
-    static constexpr int EBOX_PAD = (EBOX + 127) / 128 * 128;               // 4864 / 2688 B
-    static constexpr int HBOX = BROWS_H * BW * (int)sizeof(T);              // 4608 / 2560 B
-    static constexpr int STAGE = 3 * EBOX_PAD + 3 * HBOX + CBOX;           // 29952 / 17280 B
-    static constexpr uint32_t TX = 3 * EBOX + 3 * HBOX + CBOX;             // bytes the TMA delivers per stage
-    static_assert(EBOX_PAD % 128 == 0 && HBOX % 128 == 0 && CBOX % 128 == 0, "TMA boxes must stay 128-B aligned");
-};
 constexpr int NTH = 256;
+constexpr int TROWS = 16;                 // thread rows: j0-1 .. j0+14
+constexpr int TGRP = 16;                  // 4-cell groups per row: k0-4 .. k0+59
+static_assert(TROWS * TGRP == NTH, "one thread per 4-cell group");
+static_assert(BULK_TJ == TROWS - 1 && BULK_TK == 4 * TGRP - 4, "tile of the host work list");
+constexpr int ROWS_E = TROWS + 1, ROWS_H = TROWS, BWC = 80;
+constexpr int S = 3;
+constexpr int CBOX = ROWS_H * BWC;        // 1280 B
 constexpr long long WAIT_LIMIT = 1ll << 22;
 
+// Box geometry per storage type T (elements, k innermost).  Boxes start at
+// the column ka = (k0 - 4) rounded down to 16 bytes; the E box reaches the
+// k + 1 neighbour of the last group (one group further), the class box is
+// 80 bytes from (k0 - 4) rounded down to 16.
+template <class T>
+struct Geo {
+    static constexpr int XAL = 16 / (int)sizeof(T);                    // x alignment (elements)
+    static constexpr int BWE = sizeof(T) == 4 ? 68 : 72;
+    static constexpr int BWH = sizeof(T) == 4 ? 64 : 72;
+    static constexpr int EBOX = ROWS_E * BWE * (int)sizeof(T);          // 4624 / 2448 B
+    static constexpr int EBOX_PAD = (EBOX + 127) / 128 * 128;           // 4736 / 2560 B
+    static constexpr int HBOX = ROWS_H * BWH * (int)sizeof(T);          // 4096 / 2304 B
+    static constexpr int HBOX_PAD = (HBOX + 127) / 128 * 128;
+    static constexpr int STAGE = 3 * EBOX_PAD + 3 * HBOX_PAD + CBOX;    // 27776 / 15872 B
+    static constexpr uint32_t TX = 3 * EBOX + 3 * HBOX + CBOX;          // bytes the TMA delivers per stage
+    static_assert(EBOX_PAD % 128 == 0 && HBOX_PAD % 128 == 0 && CBOX % 128 == 0, "TMA boxes must stay 128-B aligned");
+    static_assert((BWE * sizeof(T)) % 16 == 0 && (BWH * sizeof(T)) % 16 == 0, "TMA inner extent");
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -92,22 +104,111 @@ __device__ __forceinline__ T *ebox(unsigned char *st, int c) { return reinterpre
 template <class T>
 __device__ __forceinline__ T *hbox(unsigned char *st, int c)
 {
-    return reinterpret_cast<T *>(st + 3 * Geo<T>::EBOX_PAD + c * Geo<T>::HBOX);
+    return reinterpret_cast<T *>(st + 3 * Geo<T>::EBOX_PAD + c * Geo<T>::HBOX_PAD);
 }
 template <class T>
-__device__ __forceinline__ unsigned char *cbox(unsigned char *st) { return st + 3 * Geo<T>::EBOX_PAD + 3 * Geo<T>::HBOX; }
+__device__ __forceinline__ unsigned char *cbox(unsigned char *st) { return st + 3 * Geo<T>::EBOX_PAD + 3 * Geo<T>::HBOX_PAD; }
+
+// ---- 4-vectors of the storage type
+
+// four consecutive elements from shared memory (16- or 8-byte aligned)
+template <class T>
+__device__ __forceinline__ float4 lds4(const T *p);
+template <>
+__device__ __forceinline__ float4 lds4<float>(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+template <>
+__device__ __forceinline__ float4 lds4<__half>(const __half *p)
+{
+    const uint2 u = *reinterpret_cast<const uint2 *>(p);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&u.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+template <>
+__device__ __forceinline__ float4 lds4<__nv_bfloat16>(const __nv_bfloat16 *p)
+{
+    const uint2 u = *reinterpret_cast<const uint2 *>(p);
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.x));
+    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
+// four consecutive elements of a global field array (element index c, c % 4 == 0)
+template <class T>
+__device__ __forceinline__ float4 ldg4(const float *base, int64_t c)
+{
+    if constexpr (sizeof(T) == 4) return *reinterpret_cast<const float4 *>(base + c);
+    else return lds4<T>(reinterpret_cast<const T *>(base) + c);
+}
+
+// round one FP32 value to the 16-bit storage type (bits), as Stor<T>::st does
+template <class T>
+__device__ __forceinline__ uint32_t bits16(float v, int64_t i, uint32_t seed)
+{
+    if constexpr (Stor<T>::stochastic) {
+        uint32_t u = __float_as_uint(v);
+        if ((u & 0x7f800000u) != 0x7f800000u) u += sr_mix((uint32_t)i ^ seed) & 0xffffu;
+        return u >> 16;
+    } else {
+        const __half h = __float2half_rn(v);
+        return (uint32_t)*reinterpret_cast<const unsigned short *>(&h);
+    }
+}
+
+// store four values (times `scale` at 16-bit storage) at element c, c % 4 == 0
+template <class T>
+__device__ __forceinline__ void stg4(float *base, int64_t c, float4 v, float scale, uint32_t stp, uint32_t array)
+{
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4 *>(base + c) = v;
+    } else {
+        const uint32_t seed = Stor<T>::stochastic ? sr_seed(stp, array) : 0u;
+        const uint32_t a = bits16<T>(v.x * scale, c, seed), b = bits16<T>(v.y * scale, c + 1, seed);
+        const uint32_t d = bits16<T>(v.z * scale, c + 2, seed), e = bits16<T>(v.w * scale, c + 3, seed);
+        *reinterpret_cast<uint2 *>(reinterpret_cast<T *>(base) + c) = make_uint2(a | (b << 16), d | (e << 16));
+    }
+}
+
+// the same as arrays of four floats
+template <class T>
+__device__ __forceinline__ void lds4a(float (&d)[4], const T *p)
+{
+    const float4 v = lds4<T>(p);
+    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+}
+template <class T>
+__device__ __forceinline__ void ldg4a(float (&d)[4], const float *base, int64_t c)
+{
+    const float4 v = ldg4<T>(base, c);
+    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+}
+template <class T>
+__device__ __forceinline__ void stg4a(float *base, int64_t c, const float (&v)[4], float scale, uint32_t stp, uint32_t array)
+{
+    stg4<T>(base, c, make_float4(v[0], v[1], v[2], v[3]), scale, stp, array);
+}
+// FP32 state arrays (ADE)
+__device__ __forceinline__ void ldq4a(float (&d)[4], const float *p)
+{
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+}
+__device__ __forceinline__ void stq4a(float *p, const float (&v)[4]) { *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]); }
 
 // ------------------------------------------------------------- kernel
 
 // Shared-memory layout: the TMA ring, the class table (ncls_layout entries),
-// the row exchange of H between warps, one mbarrier per stage and the ADE table.
+// the H row exchange [2 parities][hx, hz][16 rows][16 groups], one mbarrier
+// per stage and the ADE table.
 struct BulkSmem {
     unsigned char *stages;
     float4 *scls;
-    float *hrow;        // [8][2][32]
+    float4 *xch;
     uint64_t *bars;
     DevAde *sade;
 };
+
+constexpr int XCH_BYTES = 2 * 2 * TROWS * TGRP * 16;   // 16 KB
 
 template <class T>
 __device__ __forceinline__ BulkSmem bulk_smem(unsigned char *smem, int ncls_layout)
@@ -116,9 +217,9 @@ __device__ __forceinline__ BulkSmem bulk_smem(unsigned char *smem, int ncls_layo
     BulkSmem m;
     m.stages = smem;
     m.scls = reinterpret_cast<float4 *>(smem + SS);
-    m.hrow = reinterpret_cast<float *>(smem + SS + ncls_layout * 64);
-    m.bars = reinterpret_cast<uint64_t *>(smem + SS + ncls_layout * 64 + 8 * 2 * 32 * 4);
-    m.sade = reinterpret_cast<DevAde *>(smem + SS + ncls_layout * 64 + 8 * 2 * 32 * 4 + S * 8);
+    m.xch = reinterpret_cast<float4 *>(smem + SS + ncls_layout * 64);
+    m.bars = reinterpret_cast<uint64_t *>(smem + SS + ncls_layout * 64 + XCH_BYTES);
+    m.sade = reinterpret_cast<DevAde *>(smem + SS + ncls_layout * 64 + XCH_BYTES + S * 8);
     return m;
 }
 
@@ -143,21 +244,20 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
 {
     unsigned char *stages = m.stages;
     const float4 *scls = m.scls;
-    float *hrow = m.hrow;
+    float4 *xch = m.xch;
     uint64_t *bars = m.bars;
     const DevAde *sade = m.sade;
 
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int tid = threadIdx.x, tr = tid >> 4, tg = tid & 15;
     const int j0 = it.j0, k0 = it.k0, ib = it.ib, ie = it.ie;
-    const int xr = P.xr, yr = P.yr, zr = P.zr;
     const int64_t si = P.si, sj = P.sj;
-    constexpr int BW = Geo<T>::BW, STAGE = Geo<T>::STAGE;
-    const int ka = (k0 - 1) & ~(Geo<T>::XAL - 1), ka8 = (k0 - 1) & ~15;   // box origins (16-byte aligned x)
-    const int off = (k0 - 1) - ka, off8 = (k0 - 1) - ka8;
-    const int p0 = (ib > 0) ? ib - 1 : ib;                    // first plane (prologue H when ib > 0)
-    const int plast = min(ie, xr - 1);                        // last plane whose data is needed
+    constexpr int BWE = Geo<T>::BWE, BWH = Geo<T>::BWH, STAGE = Geo<T>::STAGE;
+    const int ka = (k0 - 4) & ~(Geo<T>::XAL - 1), ka8 = (k0 - 4) & ~15;   // box origins (16-byte aligned x)
+    const int off = (k0 - 4) - ka, off8 = (k0 - 4) - ka8;
+    const int p0 = ib - 1;                  // prologue plane: H of plane ib - 1 (ib >= 1 in the bulk)
+    const int plast = ie;                   // E(ie) feeds H of plane ie - 1 (ie <= xres - 1)
     const uint32_t g0 = gplane;
-    const uint32_t stp = sr_step<T>(P);           // step number of the BF16 rounding dither
+    const uint32_t stp = sr_step<T>(P);     // step number of the BF16 rounding dither
 
     auto issue = [&](int p) {   // thread 0: all boxes of plane p into its stage
         const int s = (int)((g0 + (uint32_t)(p - p0)) % S);
@@ -174,167 +274,255 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
     gplane = g0 + (uint32_t)(plast - p0 + 1);     // every plane p0..plast is streamed once
     int issued = min(plast, p0 + S - 1);          // last plane issued (uniform over the CTA)
 
-    // this thread's cells: rows rr = 4w + r (row 0 = j0-1), column lane (k = k0-1+lane)
-    const int k = k0 - 1 + lane;
-    const int ce = off + lane, ce8 = off8 + lane;
-    const bool kown = lane >= 1 && k < it.khi;
-    int jr[4];
-    bool own[4];
-    for (int r = 0; r < 4; r++) {
-        jr[r] = j0 - 1 + 4 * w + r;
-        own[r] = kown && (4 * w + r) >= 1 && jr[r] < it.jhi;
+    // this thread's cells: row j = j0 - 1 + tr, k = kq .. kq + 3
+    const int j = j0 - 1 + tr, kq = k0 - 4 + 4 * tg;
+    const bool own = tr >= 1 && tg >= 1 && j < it.jhi && kq < it.khi;   // groups are whole (khi - k0 % 4 == 0)
+    const int eb = tr * BWE + off + 4 * tg, hb = tr * BWH + off + 4 * tg, cb = tr * BWC + off8 + 4 * tg;
+    // TSF: does this thread's group touch a face of the TSF box?  Per plane
+    // below: faces i = i0-1, i0, in over the box's (j,k) extent; lateral faces
+    // j = j0-1, j0, jn and k = k0-1, k0, kn inside [i0, in].  The per-cell tests
+    // are those of tsf_add_h/e.
+    bool tifc = false, tlat = false;
+    const int ti0 = P.t0[0], tin = P.t1[0];
+    if (P.tsf_on) {
+        const int tj0 = P.t0[1], tjn = P.t1[1], tk0 = P.t0[2], tkn = P.t1[2], kh = kq + 3;
+        const bool jin = j >= tj0 - 1 && j <= tjn, kin = kh >= tk0 - 1 && kq <= tkn;
+        const bool jf = j == tj0 - 1 || j == tj0 || j == tjn;
+        const bool kf = (kq <= tk0 && kh >= tk0 - 1) || (kq <= tkn && kh >= tkn);
+        tifc = jin && kin;
+        tlat = (jin && kf) || (kin && jf);
     }
-    // TSF face membership by axis (source.c box faces)
-    const bool tsf = P.tsf_on != 0;
 
-    float e[4][3], h[4][3], him[4][2];
-    for (int r = 0; r < 4; r++) {
-        him[r][0] = him[r][1] = 0.f;
-        for (int a = 0; a < 3; a++) { e[r][a] = 0.f; h[r][a] = 0.f; }
-    }
+    // per-thread state of the march: E^n of plane i (own group), E(i+1) (read
+    // for H, carried as the next plane's E), H^{n+1/2} of planes i and i-1
+    float ex[4], ey[4], ez[4], eyi[4], ezi[4], hx[4], hy[4], hz[4], hyim[4], hzim[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) hyim[c] = hzim[c] = 0.f;
     bool failed = false;
-    for (int i = p0; i <= plast && i < ie; i++) {
+    for (int i = p0; i < ie; i++) {
         const uint32_t gi = g0 + (uint32_t)(i - p0);
-        const int s = (int)(gi % S);
-        const uint32_t par = (gi / S) & 1u;
-        const bool have_next = (i + 1 <= plast);
-        const int s1 = (int)((gi + 1) % S);
-        const uint32_t par1 = ((gi + 1) / S) & 1u;
-        bool ok = bar_wait(&bars[s], par);
-        if (have_next) ok = ok && bar_wait(&bars[s1], par1);
-        if (__syncthreads_or(!ok)) { failed = true; break; }
+        const int s = (int)(gi % S), s1 = (int)((gi + 1) % S);
+        bool ok = bar_wait(&bars[s], (gi / S) & 1u);
+        ok = ok && bar_wait(&bars[s1], ((gi + 1) / S) & 1u);
         unsigned char *st = stages + s * STAGE, *st1 = stages + s1 * STAGE;
-        const T *EX = ebox<T>(st, 0), *EY = ebox<T>(st, 1), *EZ = ebox<T>(st, 2);
-        const T *HX = hbox<T>(st, 0), *HY = hbox<T>(st, 1), *HZ = hbox<T>(st, 2);
-        const unsigned char *CL = cbox<T>(st);
-        const T *EY1 = ebox<T>(st1, 1), *EZ1 = ebox<T>(st1, 2);
-        auto cv = [](T v) { return Stor<T>::cvt(v); };
-        const float ihs = Stor<T>::scaled ? P.ihs : 1.f;
         const bool prologue = (i < ib);
-        const bool il = (i == xr - 1);
-        // Drude state of this plane's own cells (Q and E^{n-1}), requested before
-        // the H phase so that the loads overlap it
-        float aq[4][3], aep[4][3];
-        if (ADE && NPOLES == 0) {
+        const bool act = !prologue && own && ok;     // this thread updates and stores its group
+        const uint32_t cw = *reinterpret_cast<const uint32_t *>(cbox<T>(st) + cb);
+        const int cl0 = cw & 0xff;
+        const bool uni = cw == (uint32_t)cl0 * 0x01010101u;   // one class for the four cells
+        const bool tsf_plane = (tifc && (i == ti0 - 1 || i == ti0 || i == tin)) || (tlat && i >= ti0 && i <= tin);
+        const int64_t c0i = (int64_t)i * si + (int64_t)j * sj + kq;   // global index of this group's first cell
+        // dispersive state of this group, requested before the H phase so that
+        // the loads overlap it (Drude: Q and E^{n-1}; the pole state follows in
+        // the E phase)
+        float aq[3][4], aep[3][4];
+        uint32_t adem = 0;   // components with at least one dispersive cell in the group
+        if (ADE) {
+            if (act) {
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const unsigned fl = (!prologue && own[r]) ? __float_as_uint(scls[CL[(4 * w + r) * BWC + ce8] * 4].w) : 0u;
-                const int64_t c = (int64_t)i * si + (int64_t)jr[r] * sj + k;
-                const unsigned cm[3] = {CF_ADE_X, CF_ADE_Y, CF_ADE_Z};
+                for (int c = 0; c < 4; c++) {
+                    const int cl = (cw >> (8 * c)) & 0xff;
+                    const uint32_t fl = __float_as_uint(scls[cl * 4].w);
+                    if (fl & CF_ADE_BRANCH) adem |= fl & (CF_ADE_X | CF_ADE_Y | CF_ADE_Z);
+                    if (uni) break;
+                }
+            }
 #pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    const bool need = (fl & CF_ADE_BRANCH) && (fl & cm[a]);
-                    aq[r][a] = need ? P.q[a][c] : 0.f;
-                    aep[r][a] = need ? ldE<T>(P.fout[a], c) : 0.f;
+            for (int a = 0; a < 3; a++) {
+                if (adem & (1u << a)) {
+                    ldq4a(aq[a], P.q[a] + c0i);
+                    ldg4a<T>(aep[a], P.fout[a], c0i);
                 }
             }
         }
-        // ---- H phase: 4 cells per thread
-        for (int r = 0; r < 4; r++) {
-            const int rr = 4 * w + r, j = jr[r];
-            const int b = rr * BW + ce;
-            const float ex = cv(EX[b]), ey = cv(EY[b]), ez = cv(EZ[b]);
-            e[r][0] = ex; e[r][1] = ey; e[r][2] = ez;
-            const float exj = cv(EX[b + BW]), ezj = cv(EZ[b + BW]);
-            const float exk = cv(EX[b + 1]), eyk = cv(EY[b + 1]);
-            const float eyi = have_next ? cv(EY1[b]) : 0.f, ezi = have_next ? cv(EZ1[b]) : 0.f;
-            const int cl = CL[rr * BWC + ce8];
-            const float4 hc = scls[cl * 4 + 2];
-            float hx = cv(HX[b]), hy = cv(HY[b]), hz = cv(HZ[b]);
-            if (Stor<T>::scaled) { hx *= ihs; hy *= ihs; hz *= ihs; }
-            const bool jl = (j == yr - 1), kl = (k == zr - 1);
-            if (!(jl || kl)) hx = hc.x * hx + hc.y * ((eyk - ey) - (ezj - ez));
-            if (!(il || kl)) hy = hc.x * hy + hc.y * ((ezi - ez) - (exk - ex));
-            if (!(il || jl)) hz = hc.x * hz + hc.y * ((exj - ex) - (eyi - ey));
-            if (tsf) tsf_add_h(P, i, j, k, hx, hy, hz);
-            h[r][0] = hx; h[r][1] = hy; h[r][2] = hz;
-            if (!prologue && own[r]) {
-                const int64_t c = (int64_t)i * si + (int64_t)j * sj + k;
-                stH<T>(P, P.fout[3], c, hx, stp, 3);
-                stH<T>(P, P.fout[4], c, hy, stp, 4);
-                stH<T>(P, P.fout[5], c, hz, stp, 5);
+        // ---- H phase: four cells per thread
+        {
+            const T *EX = ebox<T>(st, 0), *EY = ebox<T>(st, 1), *EZ = ebox<T>(st, 2);
+            if (i == p0) { lds4a<T>(ey, EY + eb); lds4a<T>(ez, EZ + eb); }   // later planes: carried E(i+1)
+            lds4a<T>(ex, EX + eb);
+            float exj[4], ezj[4];
+            lds4a<T>(exj, EX + eb + BWE);
+            lds4a<T>(ezj, EZ + eb + BWE);
+            const float exk4 = lds4<T>(EX + eb + 4).x, eyk4 = lds4<T>(EY + eb + 4).x;
+            lds4a<T>(eyi, ebox<T>(st1, 1) + eb);
+            lds4a<T>(ezi, ebox<T>(st1, 2) + eb);
+            lds4a<T>(hx, hbox<T>(st, 0) + hb);
+            lds4a<T>(hy, hbox<T>(st, 1) + hb);
+            lds4a<T>(hz, hbox<T>(st, 2) + hb);
+            float da[4], db[4];
+            {
+                const float4 hc = scls[cl0 * 4 + 2];
+#pragma unroll
+                for (int c = 0; c < 4; c++) { da[c] = hc.x; db[c] = hc.y; }
             }
-        }
-        if (!prologue) {
-            hrow[(w * 2 + 0) * 32 + lane] = h[3][2];
-            hrow[(w * 2 + 1) * 32 + lane] = h[3][0];
-        }
-        __syncthreads();
-        // ---- E phase on own cells
-        if (!prologue) {
-            float hyk[4], hxk[4];
-            for (int r = 0; r < 4; r++) {
-                hyk[r] = __shfl_up_sync(0xffffffffu, h[r][1], 1);
-                hxk[r] = __shfl_up_sync(0xffffffffu, h[r][0], 1);
-            }
-            for (int r = 0; r < 4; r++) {
-                if (!own[r]) continue;
-                const int rr = 4 * w + r, j = jr[r];
-                const float hzj = r ? h[r - 1][2] : hrow[((w - 1) * 2 + 0) * 32 + lane];
-                const float hxj = r ? h[r - 1][0] : hrow[((w - 1) * 2 + 1) * 32 + lane];
-                const int cl = CL[rr * BWC + ce8];
-                const float4 c0 = scls[cl * 4 + 0], c1 = scls[cl * 4 + 1];
-                const unsigned fl = __float_as_uint(c0.w);
-                const float curlx = (h[r][2] - hzj) - (h[r][1] - hyk[r]);
-                const float curly = (h[r][0] - hxk[r]) - (h[r][2] - him[r][1]);
-                const float curlz = (h[r][1] - him[r][0]) - (h[r][0] - hxj);
-                const bool gx = (j > 0 && k > 0), gy = (i > 0 && k > 0), gz = (i > 0 && j > 0);
-                float nx = e[r][0], ny = e[r][1], nz = e[r][2];
-                const int64_t c = (int64_t)i * si + (int64_t)j * sj + k;
-                if (ADE && (fl & CF_ADE_BRANCH)) {
-                    // ADE branch (yee.c:914-1108) without CPML: only the owned components
-                    const DevAde &A = sade[__float_as_int(scls[cl * 4 + 2].z)];
-                    const float curl[3] = {curlx, curly, curlz};
-                    const bool gd[3] = {gx, gy, gz};
-                    const unsigned cm[3] = {CF_ADE_X, CF_ADE_Y, CF_ADE_Z};
-                    float ne[3] = {nx, ny, nz};
-                    for (int a = 0; a < 3; a++) {
-                        if (!(fl & cm[a])) continue;
-                        const float eo = e[r][a];
-                        // difference-form state (DevAde); E^{n-1} is the output set before this step writes it
-                        const float qd = (NPOLES == 0) ? aq[r][a] : P.q[a][c], ep = (NPOLES == 0) ? aep[r][a] : ldE<T>(P.fout[a], c);
-                        float pc[2] = {0.f, 0.f}, qc[2] = {0.f, 0.f};
-                        for (int n = 0; n < NPOLES; n++) { pc[n] = P.pc[a][n][c]; qc[n] = P.qc[a][n][c]; }
-                        float v = eo;
-                        if (gd[a]) {
-                            v = A.c0dx * curl[a] + A.qe * qd;
-                            for (int n = 0; n < NPOLES; n++) v += A.qpe[n] * qc[n] + A.pe[n] * pc[n];
-                            v += A.c2 * ep + A.c3 * eo;
-                        }
-                        ne[a] = v;
-                        P.q[a][c] = A.ma0 * qd + A.a2 * (ep + 2.f * eo + v);
-                        for (int n = 0; n < NPOLES; n++) {
-                            const float qn = A.rp[n] * pc[n] + A.rq[n] * qc[n] + A.bp2[n] * ep + A.bp3[n] * eo + A.bp4[n] * v;
-                            P.qc[a][n][c] = qn;
-                            P.pc[a][n][c] = pc[n] + qn;
-                        }
-                    }
-                    if (gx && !(fl & CF_ADE_X)) ne[0] = c0.x * nx + c1.x * curlx;
-                    if (gy && !(fl & CF_ADE_Y)) ne[1] = c0.y * ny + c1.y * curly;
-                    if (gz && !(fl & CF_ADE_Z)) ne[2] = c0.z * nz + c1.z * curlz;
-                    nx = ne[0]; ny = ne[1]; nz = ne[2];
-                } else {
-                    if (gx) nx = c0.x * nx + c1.x * curlx;
-                    if (gy) ny = c0.y * ny + c1.y * curly;
-                    if (gz) nz = c0.z * nz + c1.z * curlz;
+            if (!uni) {
+#pragma unroll
+                for (int c = 1; c < 4; c++) {
+                    const float4 hc = scls[((cw >> (8 * c)) & 0xff) * 4 + 2];
+                    da[c] = hc.x; db[c] = hc.y;
                 }
-                if (fl & CF_PEC_X) nx = 0.f;
-                if (fl & CF_PEC_Y) ny = 0.f;
-                if (fl & CF_PEC_Z) nz = 0.f;
-                if (tsf) tsf_add_e(P, i, j, k, nx, ny, nz);
-                stE<T>(P.fout[0], c, nx, stp, 0);
-                stE<T>(P.fout[1], c, ny, stp, 1);
-                stE<T>(P.fout[2], c, nz, stp, 2);
             }
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                if (Stor<T>::scaled) { hx[c] *= P.ihs; hy[c] *= P.ihs; hz[c] *= P.ihs; }
+                const float eyk = c < 3 ? ey[c + 1] : eyk4, exk = c < 3 ? ex[c + 1] : exk4;
+                hx[c] = da[c] * hx[c] + db[c] * ((eyk - ey[c]) - (ezj[c] - ez[c]));
+                hy[c] = da[c] * hy[c] + db[c] * ((ezi[c] - ez[c]) - (exk - ex[c]));
+                hz[c] = da[c] * hz[c] + db[c] * ((exj[c] - ex[c]) - (eyi[c] - ey[c]));
+            }
+            if (tsf_plane) {
+#pragma unroll
+                for (int c = 0; c < 4; c++) tsf_add_h(P, i, j, kq + c, hx[c], hy[c], hz[c]);
+            }
+            if (act) {
+                const float q = Stor<T>::scaled ? P.hs : 1.f;
+                stg4a<T>(P.fout[3], c0i, hx, q, stp, 3);
+                stg4a<T>(P.fout[4], c0i, hy, q, stp, 4);
+                stg4a<T>(P.fout[5], c0i, hz, q, stp, 5);
+            }
+            const int xb = ((int)(i & 1) * 2 * TROWS + tr) * TGRP + tg;
+            xch[xb] = make_float4(hx[0], hx[1], hx[2], hx[3]);
+            xch[xb + TROWS * TGRP] = make_float4(hz[0], hz[1], hz[2], hz[3]);
         }
-        for (int r = 0; r < 4; r++) { him[r][0] = h[r][1]; him[r][1] = h[r][2]; }
-        __syncthreads();   // stage s is free
+        if (__syncthreads_or(!ok)) { failed = true; break; }
+        // stage s is free: every thread has read plane i (here and as plane i+1 before)
         if (i + S <= plast) {
             if (tid == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 issue(i + S);
             }
             issued = i + S;
+        }
+        // ---- E phase on own cells
+        const float hyk0 = __shfl_up_sync(0xffffffffu, hy[3], 1), hxk0 = __shfl_up_sync(0xffffffffu, hx[3], 1);
+        if (act) {
+            const int xb = ((int)(i & 1) * 2 * TROWS + tr - 1) * TGRP + tg;
+            const float4 hxj4 = xch[xb], hzj4 = xch[xb + TROWS * TGRP];
+            const float hxj[4] = {hxj4.x, hxj4.y, hxj4.z, hxj4.w}, hzj[4] = {hzj4.x, hzj4.y, hzj4.z, hzj4.w};
+            float cu[3][4];   // curl H of the four cells
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const float hxk = c ? hx[c - 1] : hxk0, hyk = c ? hy[c - 1] : hyk0;
+                cu[0][c] = (hz[c] - hzj[c]) - (hy[c] - hyk);
+                cu[1][c] = (hx[c] - hxk) - (hz[c] - hzim[c]);
+                cu[2][c] = (hy[c] - hyim[c]) - (hx[c] - hxj[c]);
+            }
+            const float *eo[3] = {ex, ey, ez};
+            float ne[3][4];
+            float pq[3][2][4], qq[3][2][4];   // critical-point state p, q (NPOLES > 0)
+            if (ADE && NPOLES > 0) {
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int n = 0; n < NPOLES; n++)
+                        if (adem & (1u << a)) {
+                            ldq4a(pq[a][n], P.pc[a][n] + c0i);
+                            ldq4a(qq[a][n], P.qc[a][n] + c0i);
+                        }
+            }
+            const unsigned cm[3] = {CF_ADE_X, CF_ADE_Y, CF_ADE_Z};
+            if (uni) {
+                // one class: coefficients and branches once for the group
+                const float4 c0 = scls[cl0 * 4 + 0], c1 = scls[cl0 * 4 + 1];
+                const unsigned fl = __float_as_uint(c0.w);
+                const float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z};
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) ne[a][c] = ca[a] * eo[a][c] + cb[a] * cu[a][c];
+                if (ADE && (fl & CF_ADE_BRANCH)) {
+                    // ADE branch (yee.c:914-1108) without CPML: only the owned components
+                    const DevAde &A = sade[__float_as_int(scls[cl0 * 4 + 2].z)];
+                    const float c0dx = A.c0dx, qe = A.qe, c2 = A.c2, c3 = A.c3, ma0 = A.ma0, a2 = A.a2;
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        if (!(fl & cm[a])) continue;
+#pragma unroll
+                        for (int c = 0; c < 4; c++) {
+                            // difference-form state (DevAde); E^{n-1} is the output set before this step writes it
+                            const float qd = aq[a][c], ep = aep[a][c], e0 = eo[a][c];
+                            float v = c0dx * cu[a][c] + qe * qd;
+#pragma unroll
+                            for (int n = 0; n < NPOLES; n++) v += A.qpe[n] * qq[a][n][c] + A.pe[n] * pq[a][n][c];
+                            v += c2 * ep + c3 * e0;
+                            ne[a][c] = v;
+                            aq[a][c] = ma0 * qd + a2 * (ep + 2.f * e0 + v);
+#pragma unroll
+                            for (int n = 0; n < NPOLES; n++) {
+                                const float pc = pq[a][n][c], qc = qq[a][n][c];
+                                const float qn = A.rp[n] * pc + A.rq[n] * qc + A.bp2[n] * ep + A.bp3[n] * e0 + A.bp4[n] * v;
+                                qq[a][n][c] = qn;
+                                pq[a][n][c] = pc + qn;
+                            }
+                        }
+                    }
+                }
+                const unsigned pm[3] = {CF_PEC_X, CF_PEC_Y, CF_PEC_Z};
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+                    if (fl & pm[a])
+#pragma unroll
+                        for (int c = 0; c < 4; c++) ne[a][c] = 0.f;
+            } else {
+                // material boundary inside the group: cell by cell
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int cl = (cw >> (8 * c)) & 0xff;
+                    const float4 c0 = scls[cl * 4 + 0], c1 = scls[cl * 4 + 1];
+                    const unsigned fl = __float_as_uint(c0.w);
+                    const float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z};
+#pragma unroll
+                    for (int a = 0; a < 3; a++) ne[a][c] = ca[a] * eo[a][c] + cb[a] * cu[a][c];
+                    if (ADE && (fl & CF_ADE_BRANCH)) {
+                        const DevAde &A = sade[__float_as_int(scls[cl * 4 + 2].z)];
+#pragma unroll
+                        for (int a = 0; a < 3; a++) {
+                            if (!(fl & cm[a])) continue;
+                            const float qd = aq[a][c], ep = aep[a][c], e0 = eo[a][c];
+                            float v = A.c0dx * cu[a][c] + A.qe * qd;
+#pragma unroll
+                            for (int n = 0; n < NPOLES; n++) v += A.qpe[n] * qq[a][n][c] + A.pe[n] * pq[a][n][c];
+                            v += A.c2 * ep + A.c3 * e0;
+                            ne[a][c] = v;
+                            aq[a][c] = A.ma0 * qd + A.a2 * (ep + 2.f * e0 + v);
+#pragma unroll
+                            for (int n = 0; n < NPOLES; n++) {
+                                const float pc = pq[a][n][c], qc = qq[a][n][c];
+                                const float qn = A.rp[n] * pc + A.rq[n] * qc + A.bp2[n] * ep + A.bp3[n] * e0 + A.bp4[n] * v;
+                                qq[a][n][c] = qn;
+                                pq[a][n][c] = pc + qn;
+                            }
+                        }
+                    }
+                    if (fl & CF_PEC_X) ne[0][c] = 0.f;
+                    if (fl & CF_PEC_Y) ne[1][c] = 0.f;
+                    if (fl & CF_PEC_Z) ne[2][c] = 0.f;
+                }
+            }
+            if (tsf_plane) {
+#pragma unroll
+                for (int c = 0; c < 4; c++) tsf_add_e(P, i, j, kq + c, ne[0][c], ne[1][c], ne[2][c]);
+            }
+            stg4a<T>(P.fout[0], c0i, ne[0], 1.f, stp, 0);
+            stg4a<T>(P.fout[1], c0i, ne[1], 1.f, stp, 1);
+            stg4a<T>(P.fout[2], c0i, ne[2], 1.f, stp, 2);
+            if (ADE) {
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    if (!(adem & (1u << a))) continue;
+                    stq4a(P.q[a] + c0i, aq[a]);
+#pragma unroll
+                    for (int n = 0; n < NPOLES; n++) {
+                        stq4a(P.qc[a][n] + c0i, qq[a][n]);
+                        stq4a(P.pc[a][n] + c0i, pq[a][n]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            hyim[c] = hy[c]; hzim[c] = hz[c];
+            ey[c] = eyi[c]; ez[c] = ezi[c];
         }
     }
     if (failed) {
@@ -349,6 +537,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
         __syncthreads();
         return false;
     }
+    __syncthreads();   // the exchange buffer and the stages are free for the next item
     return true;
 }
 
@@ -402,7 +591,7 @@ __global__ void __launch_bounds__(NTH, 2) bulk_kernel_batch(const DevPlan *plans
 size_t bulk_smem_bytes(int nclasses, int storage)
 {
     const size_t stage = storage == FDTD_STORE_F32 ? (size_t)Geo<float>::STAGE : (size_t)Geo<__half>::STAGE;
-    return S * stage + (size_t)nclasses * 64 + 8 * 2 * 32 * 4 + S * 8 + FDTD_MAX_ADE * sizeof(DevAde);
+    return S * stage + (size_t)nclasses * 64 + XCH_BYTES + S * 8 + FDTD_MAX_ADE * sizeof(DevAde);
 }
 
 template <class T>
@@ -479,23 +668,25 @@ cudaError_t launch_bulk_batch(const DevPlan *plans, const BulkMaps *maps, const 
     return cudaGetLastError();
 }
 
-// Tensor maps of one field set: 3D (k, j, i) float boxes of 36 x 33 (E) and
-// 36 x 32 (H); class bytes 48 x 32 over a row pitch padded to 16 bytes.
-int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, int storage, BulkMaps *out)
+// Tensor maps of one field set: 3D (k, j, i) boxes of BWE x 17 (E) and
+// BWH x 16 (H) elements; class bytes 80 x 16 over a row pitch padded to 16 bytes.
+int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, int storage,
+                   BulkMaps *out)
 {
     auto enc = reinterpret_cast<CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
                                              CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
                                              CUtensorMapFloatOOBfill)>(encode_fn);
     const cuuint64_t dims[3] = {(cuuint64_t)p.zr, (cuuint64_t)p.yr, (cuuint64_t)p.xr};
-    const cuuint64_t es = storage == FDTD_STORE_F32 ? 4 : 2;
+    const bool f32 = storage == FDTD_STORE_F32;
+    const cuuint64_t es = f32 ? 4 : 2;
     const CUtensorMapDataType dtype = storage == FDTD_STORE_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                       : storage == FDTD_STORE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    const cuuint32_t BW = storage == FDTD_STORE_F32 ? Geo<float>::BW : Geo<__half>::BW;
+    const cuuint32_t bwe = f32 ? Geo<float>::BWE : Geo<__half>::BWE, bwh = f32 ? Geo<float>::BWH : Geo<__half>::BWH;
     const cuuint64_t strides[2] = {(cuuint64_t)p.zr * es, (cuuint64_t)p.zr * es * (cuuint64_t)p.yr};
     const cuuint32_t estr[3] = {1, 1, 1};
-    const cuuint32_t boxe[3] = {BW, BROWS_E, 1}, boxh[3] = {BW, BROWS_H, 1}, boxc[3] = {BWC, BROWS_H, 1};
+    const cuuint32_t boxe[3] = {bwe, ROWS_E, 1}, boxh[3] = {bwh, ROWS_H, 1}, boxc[3] = {BWC, ROWS_H, 1};
     for (int c = 0; c < 3; c++) {
         if (enc(&out->e[c], dtype, 3, f[c], dims, strides, boxe, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)

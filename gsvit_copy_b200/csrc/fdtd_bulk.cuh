@@ -13,12 +13,15 @@ struct BulkMaps {
     CUtensorMap cls;
 };
 
-// one CTA: own cells [j0, min(j0+31, jhi)) x [k0, min(k0+31, khi)) of planes [ib, ie)
+// one CTA: own cells [j0, min(j0+15, jhi)) x [k0, min(k0+60, khi)) of planes [ib, ie)
 struct BulkItem {
     int j0, k0, ib, ie, jhi, khi, inst, pad0;   // inst: plan of the item in a batched launch
 };
 
-#define BULK_TILE 31
+// own rows and columns of a tile; the bulk box has 1 <= lo, hi <= res - 1 on
+// every axis and its k bounds (hence k0 and khi) are multiples of 4
+#define BULK_TJ 15
+#define BULK_TK 60
 
 size_t bulk_smem_bytes(int nclasses, int storage);
 cudaError_t bulk_configure();
