@@ -109,92 +109,6 @@ __device__ __forceinline__ T *hbox(unsigned char *st, int c)
 template <class T>
 __device__ __forceinline__ unsigned char *cbox(unsigned char *st) { return st + 3 * Geo<T>::EBOX_PAD + 3 * Geo<T>::HBOX_PAD; }
 
-// ---- 4-vectors of the storage type
-
-// four consecutive elements from shared memory (16- or 8-byte aligned)
-template <class T>
-__device__ __forceinline__ float4 lds4(const T *p);
-template <>
-__device__ __forceinline__ float4 lds4<float>(const float *p) { return *reinterpret_cast<const float4 *>(p); }
-template <>
-__device__ __forceinline__ float4 lds4<__half>(const __half *p)
-{
-    const uint2 u = *reinterpret_cast<const uint2 *>(p);
-    const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&u.x));
-    const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&u.y));
-    return make_float4(a.x, a.y, b.x, b.y);
-}
-template <>
-__device__ __forceinline__ float4 lds4<__nv_bfloat16>(const __nv_bfloat16 *p)
-{
-    const uint2 u = *reinterpret_cast<const uint2 *>(p);
-    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.x));
-    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.y));
-    return make_float4(a.x, a.y, b.x, b.y);
-}
-
-// four consecutive elements of a global field array (element index c, c % 4 == 0)
-template <class T>
-__device__ __forceinline__ float4 ldg4(const float *base, int64_t c)
-{
-    if constexpr (sizeof(T) == 4) return *reinterpret_cast<const float4 *>(base + c);
-    else return lds4<T>(reinterpret_cast<const T *>(base) + c);
-}
-
-// round one FP32 value to the 16-bit storage type (bits), as Stor<T>::st does
-template <class T>
-__device__ __forceinline__ uint32_t bits16(float v, int64_t i, uint32_t seed)
-{
-    if constexpr (Stor<T>::stochastic) {
-        uint32_t u = __float_as_uint(v);
-        if ((u & 0x7f800000u) != 0x7f800000u) u += sr_mix((uint32_t)i ^ seed) & 0xffffu;
-        return u >> 16;
-    } else {
-        const __half h = __float2half_rn(v);
-        return (uint32_t)*reinterpret_cast<const unsigned short *>(&h);
-    }
-}
-
-// store four values (times `scale` at 16-bit storage) at element c, c % 4 == 0
-template <class T>
-__device__ __forceinline__ void stg4(float *base, int64_t c, float4 v, float scale, uint32_t stp, uint32_t array)
-{
-    if constexpr (sizeof(T) == 4) {
-        *reinterpret_cast<float4 *>(base + c) = v;
-    } else {
-        const uint32_t seed = Stor<T>::stochastic ? sr_seed(stp, array) : 0u;
-        const uint32_t a = bits16<T>(v.x * scale, c, seed), b = bits16<T>(v.y * scale, c + 1, seed);
-        const uint32_t d = bits16<T>(v.z * scale, c + 2, seed), e = bits16<T>(v.w * scale, c + 3, seed);
-        *reinterpret_cast<uint2 *>(reinterpret_cast<T *>(base) + c) = make_uint2(a | (b << 16), d | (e << 16));
-    }
-}
-
-// the same as arrays of four floats
-template <class T>
-__device__ __forceinline__ void lds4a(float (&d)[4], const T *p)
-{
-    const float4 v = lds4<T>(p);
-    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-}
-template <class T>
-__device__ __forceinline__ void ldg4a(float (&d)[4], const float *base, int64_t c)
-{
-    const float4 v = ldg4<T>(base, c);
-    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-}
-template <class T>
-__device__ __forceinline__ void stg4a(float *base, int64_t c, const float (&v)[4], float scale, uint32_t stp, uint32_t array)
-{
-    stg4<T>(base, c, make_float4(v[0], v[1], v[2], v[3]), scale, stp, array);
-}
-// FP32 state arrays (ADE)
-__device__ __forceinline__ void ldq4a(float (&d)[4], const float *p)
-{
-    const float4 v = *reinterpret_cast<const float4 *>(p);
-    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-}
-__device__ __forceinline__ void stq4a(float *p, const float (&v)[4]) { *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]); }
-
 // ------------------------------------------------------------- kernel
 
 // Shared-memory layout: the TMA ring, the class table (ncls_layout entries),
