@@ -64,7 +64,10 @@ def parse():
     ap.add_argument("--res", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["rough512", "batched"], default="rough512",
+    ap.add_argument("--adj-steps", type=int, default=4000, help="adjoint workload: forward steps")
+    ap.add_argument("--fd-cells", type=int, default=16, help="adjoint workload: cells checked by finite differences")
+    ap.add_argument("--fd-h", type=float, default=0.1, help="adjoint workload: finite-difference step on eps_r")
+    ap.add_argument("--workload", choices=["rough512", "batched", "adjoint"], default="rough512",
                     help="batched: 48 uneven rough-surface instances in one batch against the same run one by one")
     return ap.parse_args()
 
@@ -423,10 +426,77 @@ def run_batched(a):
     return 0
 
 
+def run_adjoint(a):
+    """The adjoint workload: 256 x 256 x 128 cells of 10 nm, 12-cell CPML,
+    4000 steps, a 64 x 64 x 16 design region of per-cell eps_r (seeded
+    uniform in [1.5, 4.0]) on a glass slab, 550 nm TSF at normal incidence,
+    J = far-field power in a 10 deg cone about theta = 20 deg.  Times the
+    forward run alone and the checkpointed gradient (forward, recompute and
+    adjoint sweep; checkpoints every 200 steps), and checks --fd-cells seeded
+    cells against central differences of J (h = --fd-h on eps_r)."""
+    import numpy as np
+    from gsvit_copy_b200 import plan
+    from gsvit_copy_b200.solver import Solver
+    n = a.adj_steps
+    s = plan.adjoint_scene(nsteps=n)
+    obj = plan.cone_objective(s)
+    g = Solver(s)
+    init = g.snapshot()
+    g.step(1)
+    g.sync()
+    g.restore(init)
+    t0 = time.perf_counter()
+    g.step(n)
+    g.sync()
+    fwd_s = time.perf_counter() - t0
+    J0 = g.objective_value(obj)
+    g.restore(init)
+    t0 = time.perf_counter()
+    J, grad = g.adjoint_gradient(obj, n, 200)
+    adj_s = time.perf_counter() - t0
+    fd = None
+    if a.fd_cells > 0:
+        rng = np.random.default_rng(16)
+        cells = [tuple(int(rng.integers(0, m)) for m in grad.shape) for _ in range(a.fd_cells)]
+        eps0 = s.design["eps"].copy()
+        vals = []
+        for q in cells:
+            jj = []
+            for sgn in (1, -1):
+                e = eps0.copy()
+                e[q] += sgn * a.fd_h
+                g.restore(init)
+                g.set_design_eps(e)
+                g.step(n)
+                jj.append(g.objective_value(obj))
+            vals.append((jj[0] - jj[1]) / (2 * a.fd_h))
+        g.set_design_eps(eps0)
+        fdv = np.array(vals)
+        adv = np.array([grad[q] for q in cells])
+        fd = {"cells": len(cells), "h": a.fd_h, "max_err_over_max_grad": float(np.abs(adv - fdv).max() / np.abs(grad).max()),
+              "max_rel_err": float((np.abs(adv - fdv) / np.abs(adv)).max())}
+    line = {
+        "metric": METRIC, "value": s.ncells * n / fwd_s / 1e9, "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": 1,
+        "ms_per_step": fwd_s / n * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded design permittivities)",
+        "config": {"workload": "adjoint: 256x256x128 cells 10 nm, 12-cell CPML, 64x64x16 design cells eps_r U[1.5,4] on "
+                               "glass eps_r 2.1, 550 nm TSF normal incidence, J = far-field power in a 10 deg cone "
+                               "about theta 20 deg, checkpoints every 200 steps", "cells": s.ncells,
+                   "design_cells": int(grad.size), "cone_points": int(len(obj["points"]))},
+        "adjoint": {"J": J, "J_forward_only": J0, "forward_s": fwd_s, "gradient_s": adj_s, "gradient_over_forward": adj_s / fwd_s,
+                    "grad_min": float(grad.min()), "grad_max": float(grad.max()), "fd": fd},
+        "timing": "host clock around synchronised device work",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.workload == "batched":
         return run_batched(a)
+    if a.workload == "adjoint":
+        return run_adjoint(a)
     if a.impl == "reference":
         return run_reference(a)
     return run_b200(a)

@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 ERRORS = {
@@ -81,6 +81,15 @@ class Nfff(C.Structure):
     ]
 
 
+class Design(C.Structure):
+    _fields_ = [("enabled", C.c_int32), ("i0", C.c_int32), ("i1", C.c_int32), ("j0", C.c_int32), ("j1", C.c_int32),
+                ("k0", C.c_int32), ("k1", C.c_int32), ("reserved", C.c_int32), ("eps_r", C.POINTER(C.c_double))]
+
+
+class Objective(C.Structure):
+    _fields_ = [("freq", C.c_int32), ("npoints", C.c_int32), ("points", _ip), ("weights", C.POINTER(C.c_double))]
+
+
 class Desc(C.Structure):
     _fields_ = [
         ("abi_version", C.c_int32), ("xres", C.c_int32), ("yres", C.c_int32), ("zres", C.c_int32),
@@ -90,6 +99,7 @@ class Desc(C.Structure):
         ("epsilon", _fp), ("sigma", _fp), ("mu", _fp), ("sigast", _fp),
         ("cpml", CpmlFace * 6), ("tsf", Tsf), ("nfff", Nfff),
         ("nprobes", C.c_int32), ("reserved", C.c_int32), ("probes", _ip),
+        ("design", Design),
     ]
 
 
@@ -156,6 +166,10 @@ def load_library():
         "fdtd_batch_sync": ([P], C.c_int),
         "fdtd_batch_tune": ([P, C.c_int, _dp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "fdtd_batch_config": ([P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "fdtd_set_design_eps": ([P, _dp], C.c_int),
+        "fdtd_objective_value": ([P, C.POINTER(Objective), _dp], C.c_int),
+        "fdtd_adjoint_gradient": ([P, C.POINTER(Objective), C.c_int, C.c_int, _dp, _dp], C.c_int),
+        "fdtd_adjoint_transpose": ([P, C.c_int, C.POINTER(_dp)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -174,6 +188,7 @@ HEADER_SYMBOLS = [
     "fdtd_last_error", "fdtd_step_bytes",
     "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_size", "fdtd_batch_plan", "fdtd_batch_step",
     "fdtd_batch_step_graph", "fdtd_batch_sync", "fdtd_batch_tune", "fdtd_batch_config",
+    "fdtd_set_design_eps", "fdtd_objective_value", "fdtd_adjoint_gradient", "fdtd_adjoint_transpose",
 ]
 
 

@@ -23,6 +23,7 @@
 #include "fdtd_internal.h"
 #include "fdtd_bulk.cuh"
 #include "fdtd_kernels.cuh"
+#include "fdtd_adjoint.cuh"
 #include "plan_host.h"
 
 namespace {
@@ -315,6 +316,12 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     CA(upload(P->mem, &classes, hp.classes.data(), hp.classes.size()), "class table");
     d.classes = classes;
     d.nclasses = (int)hp.classes.size();
+    if (hp.design) {
+        float *dc;
+        CA(upload(P->mem, &dc, hp.dcoef.data(), hp.dcoef.size()), "design coefficients");
+        d.dcoef = dc;
+        for (int q = 0; q < 6; q++) d.dbox[q] = hp.abox[q];
+    }
     double bytes = (12.0 * esz + 1.0) * (double)n;   // 6 field reads + 6 writes + class byte
     if (hp.has_ade) {
         DevAde *ade;
@@ -622,7 +629,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         lo[2] = std::max(4, (lo[2] + 3) / 4 * 4);   // the k halo group k0-4..k0-1 stays in the grid
         hi[2] = hi[2] / 4 * 4;
         const char *nob = getenv("GSVIT_B200_NO_BULK");
-        P->bulk_on = ((size_t)Z * esz % 16 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
+        P->bulk_on = !hp.design && ((size_t)Z * esz % 16 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
         std::vector<SlabBox> boxes;
         std::vector<BulkItem> blk;
         long long nblk = 0;
@@ -819,6 +826,21 @@ int fdtd_set_fields(fdtd_plan *P, int mask, const double *const comps[6])
         int rc = upload_comp(P, c, tmp.data(), true);
         if (rc != FDTD_OK) return rc;
     }
+    return FDTD_OK;
+}
+
+int fdtd_set_design_eps(fdtd_plan *P, const double *eps_r)
+{
+    if (!P || !eps_r) return fail(FDTD_E_INVALID, "NULL argument");
+    if (!P->hp.design) return fail(FDTD_E_INVALID, "the plan has no design region");
+    const int *b = P->hp.dbox;
+    const size_t nd = (size_t)(b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]);
+    for (size_t q = 0; q < nd; q++)
+        if (!(eps_r[q] >= 1e-3 && eps_r[q] < 1e6)) return fail(FDTD_E_INVALID, "design eps_r must be positive and finite");
+    CK(cudaSetDevice(P->device));
+    CK(cudaStreamSynchronize(P->stream));
+    design_coefficients(&P->hp, eps_r);
+    CK(cudaMemcpy(const_cast<float *>(P->dp.dcoef), P->hp.dcoef.data(), P->hp.dcoef.size() * sizeof(float), cudaMemcpyHostToDevice));
     return FDTD_OK;
 }
 
@@ -1607,3 +1629,255 @@ int fdtd_batch_config(const fdtd_batch *B, int *planes_per_item, int *persistent
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ adjoint
+// (no counterpart in the reference)
+
+namespace {
+
+struct AdjBufs {             // adjoint state of one plan, zero-initialised
+    DevBuf mem;
+    DevAdj a;
+    ~AdjBufs() { mem.free_all(); }
+};
+
+cudaError_t adj_alloc(fdtd_plan *P, AdjBufs &B)
+{
+    std::memset(&B.a, 0, sizeof(B.a));
+    const size_t n = P->hp.n;
+    cudaError_t e;
+    for (int c = 0; c < 3; c++) {
+        if ((e = B.mem.alloc(&B.a.eb[c], n)) != cudaSuccess) return e;
+        if ((e = B.mem.alloc(&B.a.hb[c], n)) != cudaSuccess) return e;
+    }
+    for (int q = 0; q < 6; q++)
+        if ((e = B.mem.alloc(&B.a.dd[q], n)) != cudaSuccess) return e;
+    const HostPlan &hp = P->hp;
+    for (int f = 0; f < 6; f++) {
+        if (!hp.cp[f].enabled) continue;
+        const int dep = hp.cp[f].depth;
+        const size_t cnt = (f < 2) ? (size_t)dep * hp.yr * hp.zr : (f < 4) ? (size_t)hp.xr * dep * hp.zr : (size_t)hp.xr * hp.yr * dep;
+        for (int q = 0; q < 2; q++) {
+            if ((e = B.mem.alloc(&B.a.pe[f][q], cnt)) != cudaSuccess) return e;
+            if ((e = B.mem.alloc(&B.a.ph[f][q], cnt)) != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+// transpose of the step with index `step`: the objective's dJ/dE of that step,
+// the design accumulation, then the E and H half steps in reverse order
+void adj_step_back(fdtd_plan *P, AdjBufs &B, const DevObjective *obj, int step, const DevGrad *g, int slot)
+{
+    if (obj) launch_adjoint_source(*obj, B.a, step, P->stream);
+    if (g) launch_design_accumulate(B.a, P->dp, *g, slot, P->stream);
+    launch_adjoint_e(P->dp, B.a, P->stream);
+    launch_adjoint_h(P->dp, B.a, P->stream);
+}
+
+struct DevCheckpoints {      // device copies of the stepping state
+    DevBuf mem;
+    size_t bytes = 0;
+    std::vector<unsigned char *> slot;
+    std::vector<int> cur, step;
+    ~DevCheckpoints() { mem.free_all(); }
+};
+
+cudaError_t ckpt_alloc(fdtd_plan *P, DevCheckpoints &K, int nslots)
+{
+    for (auto &s : P->snap) K.bytes += (s.bytes + 255) / 256 * 256;
+    for (int q = 0; q < nslots; q++) {
+        unsigned char *p;
+        cudaError_t e = K.mem.alloc(&p, K.bytes);
+        if (e != cudaSuccess) return e;
+        K.slot.push_back(p);
+    }
+    K.cur.assign(nslots, 0);
+    K.step.assign(nslots, 0);
+    return cudaSuccess;
+}
+
+cudaError_t ckpt_save(fdtd_plan *P, DevCheckpoints &K, int q)
+{
+    size_t off = 0;
+    for (auto &s : P->snap) {
+        cudaError_t e = cudaMemcpyAsync(K.slot[q] + off, s.ptr, s.bytes, cudaMemcpyDeviceToDevice, P->stream);
+        if (e != cudaSuccess) return e;
+        off += (s.bytes + 255) / 256 * 256;
+    }
+    K.cur[q] = P->cur;
+    K.step[q] = P->host_step;
+    return cudaSuccess;
+}
+
+cudaError_t ckpt_restore(fdtd_plan *P, DevCheckpoints &K, int q)
+{
+    size_t off = 0;
+    for (auto &s : P->snap) {
+        cudaError_t e = cudaMemcpyAsync(s.ptr, K.slot[q] + off, s.bytes, cudaMemcpyDeviceToDevice, P->stream);
+        if (e != cudaSuccess) return e;
+        off += (s.bytes + 255) / 256 * 256;
+    }
+    P->cur = K.cur[q];
+    P->host_step = K.step[q];
+    return cudaSuccess;
+}
+
+int check_objective(const fdtd_plan *P, const fdtd_objective *obj)
+{
+    if (!obj) return fail(FDTD_E_INVALID, "objective is NULL");
+    if (!P->nfff || P->nfff_nfreq <= 0) return fail(FDTD_E_STATE, "the objective needs the running-DFT far field (nfff.nfreq > 0)");
+    if (obj->freq < 0 || obj->freq >= P->nfff_nfreq) return fail(FDTD_E_INVALID, "objective frequency index out of range");
+    if (obj->npoints < 1 || !obj->points || !obj->weights) return fail(FDTD_E_INVALID, "objective without far points");
+    for (int t = 0; t < obj->npoints; t++) {
+        if (obj->points[t] < 0 || obj->points[t] >= P->nfff_npoints) return fail(FDTD_E_INVALID, "objective far point out of range");
+        if (!std::isfinite(obj->weights[t])) return fail(FDTD_E_INVALID, "objective weight not finite");
+    }
+    return FDTD_OK;
+}
+
+// J of the spectrum now in P->ff.out (host copy of the objective's points)
+int objective_from_spectrum(fdtd_plan *P, const fdtd_objective *obj, double *J)
+{
+    const size_t n = (size_t)P->nfff_npoints * P->nfff_nfreq * 3;
+    std::vector<double2> spec(n);
+    CK(cudaMemcpyAsync(spec.data(), P->ff.out, n * sizeof(double2), cudaMemcpyDeviceToHost, P->stream));
+    CK(cudaStreamSynchronize(P->stream));
+    double j = 0;
+    for (int t = 0; t < obj->npoints; t++)
+        for (int c = 0; c < 3; c++) {
+            const double2 f = spec[((size_t)obj->points[t] * P->nfff_nfreq + obj->freq) * 3 + c];
+            j += obj->weights[t] * (f.x * f.x + f.y * f.y);
+        }
+    *J = j;
+    return FDTD_OK;
+}
+
+int check_adjoint_plan(const fdtd_plan *P)
+{
+    if (P->hp.has_ade) return fail(FDTD_E_UNSUPPORTED, "the adjoint covers non-dispersive materials only");
+    if (P->storage != FDTD_STORE_F32) return fail(FDTD_E_UNSUPPORTED, "the adjoint needs FP32 field storage");
+    return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_objective_value(fdtd_plan *P, const fdtd_objective *obj, double *J)
+{
+    if (!P || !J) return fail(FDTD_E_INVALID, "NULL argument");
+    int rc = check_objective(P, obj);
+    if (rc != FDTD_OK) return rc;
+    CK(cudaSetDevice(P->device));
+    launch_farfield_finalize(P->ff, P->stream);
+    CK(cudaGetLastError());
+    return objective_from_spectrum(P, obj, J);
+}
+
+int fdtd_adjoint_transpose(fdtd_plan *P, int nsteps, double *const comps[6])
+{
+    if (!P || !comps || nsteps < 0) return fail(FDTD_E_INVALID, "bad argument");
+    for (int c = 0; c < 6; c++)
+        if (!comps[c]) return fail(FDTD_E_INVALID, "component pointer is NULL");
+    int rc = check_adjoint_plan(P);
+    if (rc != FDTD_OK) return rc;
+    CK(cudaSetDevice(P->device));
+    AdjBufs B;
+    CK(adj_alloc(P, B));
+    const size_t n = P->hp.n;
+    std::vector<float> tmp(n);
+    for (int c = 0; c < 6; c++) {
+        for (size_t q = 0; q < n; q++) tmp[q] = (float)comps[c][q];
+        CK(cudaMemcpy(c < 3 ? B.a.eb[c] : B.a.hb[c - 3], tmp.data(), n * 4, cudaMemcpyHostToDevice));
+    }
+    for (int s = 0; s < nsteps; s++) adj_step_back(P, B, nullptr, 0, nullptr, 0);
+    CK(cudaGetLastError());
+    for (int c = 0; c < 6; c++) {
+        CK(cudaMemcpyAsync(tmp.data(), c < 3 ? B.a.eb[c] : B.a.hb[c - 3], n * 4, cudaMemcpyDeviceToHost, P->stream));
+        CK(cudaStreamSynchronize(P->stream));
+        for (size_t q = 0; q < n; q++) comps[c][q] = (double)tmp[q];
+    }
+    return FDTD_OK;
+}
+
+int fdtd_adjoint_gradient(fdtd_plan *P, const fdtd_objective *obj, int nsteps, int checkpoint, double *J, double *grad)
+{
+    if (!P || !J || !grad || nsteps < 1 || checkpoint < 1) return fail(FDTD_E_INVALID, "bad argument");
+    if (!P->hp.design) return fail(FDTD_E_STATE, "the plan has no design region");
+    int rc = check_objective(P, obj);
+    if (rc == FDTD_OK) rc = check_adjoint_plan(P);
+    if (rc != FDTD_OK) return rc;
+    CK(cudaSetDevice(P->device));
+    const int K = std::min(checkpoint, nsteps), nseg = (nsteps + K - 1) / K;
+    DevCheckpoints ck;
+    {
+        cudaError_t e = ckpt_alloc(P, ck, nseg + 1);
+        if (e != cudaSuccess) return fail(FDTD_E_NOMEM, std::string("adjoint checkpoints: ") + cudaGetErrorString(e));
+    }
+    // forward pass with a checkpoint at the start of every segment
+    for (int m = 0; m < nsteps; m++) {
+        if (m % K == 0) CK(ckpt_save(P, ck, m / K));
+        rc = launch_step(P, P->stream);
+        if (rc != FDTD_OK) return rc;
+        P->host_step++;
+    }
+    final_probes(P, P->stream);
+    CK(ckpt_save(P, ck, nseg));
+    launch_farfield_finalize(P->ff, P->stream);
+    CK(cudaGetLastError());
+    rc = objective_from_spectrum(P, obj, J);
+    if (rc != FDTD_OK) return rc;
+    // objective weights, adjoint state, design accumulators
+    DevBuf mem;
+    struct Free { DevBuf &m; ~Free() { m.free_all(); } } guard{mem};
+    int32_t *dpts;
+    double *dw;
+    double2 *ae, *ad;
+    const int ns = P->nf.ns;
+    CK(upload(mem, &dpts, obj->points, (size_t)obj->npoints));
+    CK(upload(mem, &dw, obj->weights, (size_t)obj->npoints));
+    CK(mem.alloc(&ae, (size_t)3 * ns));
+    CK(mem.alloc(&ad, (size_t)3 * ns));
+    launch_objective_weights(P->ff, obj->freq, obj->npoints, dpts, dw, P->ff.out, ae, ad, P->stream);
+    DevObjective o;
+    o.ns = ns;
+    o.cell = P->nf.cell;
+    o.nstride = P->nf.nstride;
+    o.inv2dx = P->nf.inv2dx;
+    o.omega_dt = P->omega[obj->freq] * P->hp.dt;
+    o.ae = ae;
+    o.ad = ad;
+    DevGrad g;
+    for (int q = 0; q < 6; q++) g.box[q] = P->hp.abox[q];
+    g.ncell = (int64_t)(g.box[1] - g.box[0]) * (g.box[3] - g.box[2]) * (g.box[5] - g.box[4]);
+    CK(mem.alloc(&g.g, (size_t)3 * g.ncell));
+    {
+        cudaError_t e = mem.alloc(&g.curl, (size_t)K * 3 * g.ncell);
+        if (e != cudaSuccess) return fail(FDTD_E_NOMEM, std::string("adjoint curl buffer: ") + cudaGetErrorString(e));
+    }
+    AdjBufs B;
+    CK(adj_alloc(P, B));
+    // backward: recompute each segment from its checkpoint, then its steps in reverse
+    for (int seg = nseg - 1; seg >= 0; seg--) {
+        const int m0 = seg * K, m1 = std::min(nsteps, m0 + K);
+        CK(ckpt_restore(P, ck, seg));
+        for (int m = m0; m < m1; m++) {
+            rc = launch_step(P, P->stream);
+            if (rc != FDTD_OK) return rc;
+            P->host_step++;
+            launch_design_curl(plan_for(P, 1 - P->cur), g, m - m0, P->stream);
+        }
+        for (int m = m1 - 1; m >= m0; m--) adj_step_back(P, B, &o, m, &g, m - m0);
+        CK(cudaGetLastError());
+    }
+    CK(ckpt_restore(P, ck, nseg));
+    std::vector<double> dcb((size_t)3 * g.ncell);
+    CK(cudaMemcpyAsync(dcb.data(), g.g, dcb.size() * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
+    CK(cudaStreamSynchronize(P->stream));
+    design_gradient(&P->hp, dcb.data(), grad);
+    return FDTD_OK;
+}
+
+}  // extern "C"
+

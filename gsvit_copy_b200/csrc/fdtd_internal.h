@@ -27,6 +27,7 @@
 #define CF_PEC_X      0x010u   // PEC rule zeroes Ex (yee.c:1138-1237)
 #define CF_PEC_Y      0x020u
 #define CF_PEC_Z      0x040u
+#define CF_DESIGN     0x080u   // E coefficients per cell (DevPlan::dcoef), adjoint design region
 
 struct alignas(16) DevClass {
     // float4 0: ordinary update E = ca*E + cb*curl (get_cabs, yee.c:1397-1493)
@@ -84,6 +85,9 @@ struct DevPlan {
     int cpitch;
     const DevClass *classes;
     int nclasses;
+    // design region: ca[3], cb[3] per cell of the box dbox (i0 i1 j0 j1 k0 k1)
+    const float *dcoef;
+    int dbox[6];
     // ADE
     int nade;
     const DevAde *ade;

@@ -155,7 +155,12 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
     const float4 c0 = scls[cls * 4 + 0], c1 = scls[cls * 4 + 1], c2 = scls[cls * 4 + 2], c3 = scls[cls * 4 + 3];
     const unsigned fl = __float_as_uint(c0.w);
-    const float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z}, cba[3] = {c3.x, c3.y, c3.z};
+    float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z};
+    const float cba[3] = {c3.x, c3.y, c3.z};
+    if (fl & CF_DESIGN) {   // adjoint design region: coefficients per cell
+        const int64_t q = ((int64_t)(i - P.dbox[0]) * (P.dbox[3] - P.dbox[2]) + (j - P.dbox[2])) * (P.dbox[5] - P.dbox[4]) + (k - P.dbox[4]);
+        for (int a = 0; a < 3; a++) { ca[a] = __ldg(P.dcoef + 6 * q + a); cb[a] = __ldg(P.dcoef + 6 * q + 3 + a); }
+    }
     const int ade_set = __float_as_int(c2.z);
     const int xr = P.xr, yr = P.yr, zr = P.zr;
     const float ikx = __ldg(P.ike[0] + i), iky = __ldg(P.ike[1] + j), ikz = __ldg(P.ike[2] + k);

@@ -42,6 +42,16 @@ struct Grid {
     int xr, yr, zr;
     std::vector<float> veps, vsig, vmu, vsigast;   // voxel arrays present per matmode
     bool has_e = false, has_m = false;
+    const fdtd_design *ds = nullptr;               // design region (epsilon per cell, lossless)
+
+    bool in_design(int i, int j, int k) const
+    {
+        return ds && i >= ds->i0 && i < ds->i1 && j >= ds->j0 && j < ds->j1 && k >= ds->k0 && k < ds->k1;
+    }
+    double design_eps(int i, int j, int k) const
+    {
+        return ds->eps_r[((size_t)(i - ds->i0) * (ds->j1 - ds->j0) + (j - ds->j0)) * (ds->k1 - ds->k0) + (k - ds->k0)] * EPS0;
+    }
 
     size_t idx(int i, int j, int k) const { return ((size_t)i * yr + j) * zr + k; }
     int mat(int i, int j, int k) const
@@ -54,7 +64,9 @@ struct Grid {
     {
         int m = mat(i, j, k);
         double ee = EPS0, gg = 0;
-        if (m > 0 && is_tab(d->mats[m].type)) {
+        if (in_design(i, j, k)) {
+            ee = design_eps(i, j, k);
+        } else if (m > 0 && is_tab(d->mats[m].type)) {
             ee = d->mats[m].epsilon;
             gg = d->mats[m].sigma;
         } else if (has_e) {
@@ -69,6 +81,7 @@ struct Grid {
     // sv_yee_data_get_epsilon, yee.c:1266-1289
     double eps(int i, int j, int k) const
     {
+        if (in_design(i, j, k)) return design_eps(i, j, k);
         int m = mat(i, j, k);
         if (m > 0 && is_tab(d->mats[m].type)) return d->mats[m].epsilon;
         if (has_e) return veps[idx(i, j, k)];
@@ -82,6 +95,7 @@ struct Grid {
     // sv_yee_data_get_tsf_mattype, yee.c:1686-1707
     int tsf_mattype(int i, int j, int k) const
     {
+        if (in_design(i, j, k)) return std::fabs(1.0 - design_eps(i, j, k) / EPS0) < 0.001 ? 0 : 1;
         int m = mat(i, j, k);
         if (m == 0 || m == -1) {
             if (has_e && (d->matmode == FDTD_MATMODE_FULL || d->matmode == FDTD_MATMODE_ELECTRIC) &&
@@ -206,6 +220,38 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
 
     Grid g;
     g.d = d; g.xr = xr; g.yr = yr; g.zr = zr;
+    // design region: the box, its affected box (one cell more above on each
+    // axis: those cells average epsilon with the box) and the context box
+    // (one cell more below: the cells the affected ones average over)
+    hp->design = d->design.enabled != 0;
+    if (hp->design) {
+        const fdtd_design &ds = d->design;
+        const int lo[3] = {ds.i0, ds.j0, ds.k0}, hi[3] = {ds.i1, ds.j1, ds.k1}, res[3] = {xr, yr, zr};
+        if (!ds.eps_r) { *err = "design region without eps_r"; return FDTD_E_INVALID; }
+        for (int ax = 0; ax < 3; ax++) {
+            if (lo[ax] < 1 || hi[ax] > res[ax] - 2 || lo[ax] >= hi[ax]) {
+                *err = "design box must lie inside [1, res-2) on every axis"; return FDTD_E_INVALID;
+            }
+            hp->dbox[2 * ax] = lo[ax]; hp->dbox[2 * ax + 1] = hi[ax];
+            hp->abox[2 * ax] = lo[ax]; hp->abox[2 * ax + 1] = hi[ax] + 1;
+            hp->cbox[2 * ax] = lo[ax] - 1; hp->cbox[2 * ax + 1] = hi[ax] + 1;
+            const fdtd_cpml_face &c0 = d->cpml[2 * ax], &c1 = d->cpml[2 * ax + 1];
+            if ((c0.enabled && hp->abox[2 * ax] < c0.depth) || (c1.enabled && hp->abox[2 * ax + 1] > res[ax] - c1.depth)) {
+                *err = "design region (and the cells above it) must lie outside the CPML slabs"; return FDTD_E_INVALID;
+            }
+        }
+        const size_t nd = (size_t)(ds.i1 - ds.i0) * (ds.j1 - ds.j0) * (ds.k1 - ds.k0);
+        for (size_t q = 0; q < nd; q++)
+            if (!(ds.eps_r[q] >= 1e-3 && ds.eps_r[q] < 1e6)) { *err = "design eps_r must be positive and finite"; return FDTD_E_INVALID; }
+        if (d->tsf.enabled) {
+            const int t0[3] = {d->tsf.i0, d->tsf.j0, d->tsf.k0}, t1[3] = {d->tsf.in, d->tsf.jn, d->tsf.kn};
+            for (int ax = 0; ax < 3; ax++)
+                if (!(hp->abox[2 * ax] > t0[ax] && hp->abox[2 * ax + 1] <= t1[ax])) {
+                    *err = "design region (and the cells above it) must lie strictly inside the TSF box"; return FDTD_E_INVALID;
+                }
+        }
+        g.ds = &ds;
+    }
     g.has_e = (d->matmode == FDTD_MATMODE_FULL || d->matmode == FDTD_MATMODE_ELECTRIC);
     g.has_m = (d->matmode == FDTD_MATMODE_FULL || d->matmode == FDTD_MATMODE_MAGNETIC);
     try {
@@ -393,6 +439,13 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
                 c.da = (float)da;
                 c.db = (float)db;
                 c.tsfe = (float)(ecor / g.eps(i, j, k));
+                const bool affected = hp->design && i >= hp->abox[0] && i < hp->abox[1] && j >= hp->abox[2] &&
+                                      j < hp->abox[3] && k >= hp->abox[4] && k < hp->abox[5];
+                if (affected) {   // E coefficients per cell (design_coefficients); no TSF face here
+                    for (int a = 0; a < 3; a++) { c.ca[a] = 0.f; c.cb[a] = 0.f; }
+                    c.tsfe = 0.f;
+                    c.flags |= CF_DESIGN;
+                }
                 // PEC rule, yee.c:1138-1237 (no SF source on this path)
                 if (m >= 0 && i > 0 && j > 0 && k > 0) {
                     const fdtd_material *M = d->mats;
@@ -485,6 +538,30 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
         }
     }
     // probes
+    if (hp->design) {
+        // context: epsilon and sigma of every cell of cbox (design cells
+        // included); the cells there must be lossless, non-magnetic and
+        // neither PEC nor dispersive
+        const int *b = hp->cbox;
+        const size_t nc = (size_t)(b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]);
+        hp->ctx_eps.assign(nc, 0.0);
+        hp->ctx_sig.assign(nc, 0.0);
+        size_t q = 0;
+        for (int i = b[0]; i < b[1]; i++)
+            for (int j = b[2]; j < b[3]; j++)
+                for (int k = b[4]; k < b[5]; k++, q++) {
+                    double e, s;
+                    const int m = g.eps_sig(i, j, k, &e, &s);
+                    if (s != 0 || (m > 0 && d->mats[m].type != FDTD_MAT_LINTAB) ||
+                        (m > 0 && d->mats[m].sigast != 0) || (g.has_m && g.vsigast[g.idx(i, j, k)] != 0)) {
+                        *err = "the design region and its neighbours must be lossless LINTAB or vacuum cells";
+                        return FDTD_E_INVALID;
+                    }
+                    hp->ctx_eps[q] = e;
+                    hp->ctx_sig[q] = s;
+                }
+        design_coefficients(hp, d->design.eps_r);
+    }
     hp->probes.clear();
     if (d->nprobes > 0) {
         if (!d->probes) { *err = "nprobes > 0 but probes is NULL"; return FDTD_E_INVALID; }
@@ -496,3 +573,79 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
     }
     return FDTD_OK;
 }
+
+// get_cabs (yee.c:1397-1493) for the affected box from the context arrays,
+// after writing the design cells' new permittivities into them
+void design_coefficients(HostPlan *hp, const double *eps_r)
+{
+    const int *b = hp->cbox, *dbx = hp->dbox, *a = hp->abox;
+    const int cj = b[3] - b[2], ck = b[5] - b[4];
+    auto cidx = [&](int i, int j, int k) { return ((size_t)(i - b[0]) * cj + (j - b[2])) * ck + (k - b[4]); };
+    size_t q = 0;
+    for (int i = dbx[0]; i < dbx[1]; i++)
+        for (int j = dbx[2]; j < dbx[3]; j++)
+            for (int k = dbx[4]; k < dbx[5]; k++, q++) hp->ctx_eps[cidx(i, j, k)] = eps_r[q] * EPS0;
+    const size_t na = (size_t)(a[1] - a[0]) * (a[3] - a[2]) * (a[5] - a[4]);
+    hp->dcoef.assign(6 * na, 0.f);
+    const double dt = hp->dt, dx = hp->dx;
+    q = 0;
+    for (int i = a[0]; i < a[1]; i++)
+        for (int j = a[2]; j < a[3]; j++)
+            for (int k = a[4]; k < a[5]; k++, q++) {
+                double ex, ey, ez, sx, sy, sz;
+                ex = ey = ez = hp->ctx_eps[cidx(i, j, k)];
+                sx = sy = sz = hp->ctx_sig[cidx(i, j, k)];
+                if (hp->bnds[((size_t)i * hp->yr + j) * hp->zr + k] > 0) {   // i, j, k >= 1 here
+                    auto e = [&](int ii, int jj, int kk) { return hp->ctx_eps[cidx(ii, jj, kk)]; };
+                    auto s = [&](int ii, int jj, int kk) { return hp->ctx_sig[cidx(ii, jj, kk)]; };
+                    ey += e(i - 1, j, k); sy += s(i - 1, j, k); ez += e(i - 1, j, k); sz += s(i - 1, j, k);
+                    ex += e(i, j - 1, k); sx += s(i, j - 1, k); ez += e(i, j - 1, k); sz += s(i, j - 1, k);
+                    ex += e(i, j, k - 1); sx += s(i, j, k - 1); ey += e(i, j, k - 1); sy += s(i, j, k - 1);
+                    ex += e(i, j - 1, k - 1); sx += s(i, j - 1, k - 1);
+                    ey += e(i - 1, j, k - 1); sy += s(i - 1, j, k - 1);
+                    ez += e(i - 1, j - 1, k); sz += s(i - 1, j - 1, k);
+                    ex /= 4; sx /= 4; ey /= 4; sy /= 4; ez /= 4; sz /= 4;
+                }
+                const double E[3] = {ex, ey, ez}, S[3] = {sx, sy, sz};
+                for (int c = 0; c < 3; c++) {
+                    hp->dcoef[6 * q + c] = (float)((1 - S[c] * dt / 2 / E[c]) / (1 + S[c] * dt / 2 / E[c]));
+                    hp->dcoef[6 * q + 3 + c] = (float)((dt / E[c] / dx) / (1 + S[c] * dt / 2 / E[c]));
+                }
+            }
+}
+
+void design_gradient(const HostPlan *hp, const double *dcb, double *grad)
+{
+    const int *b = hp->cbox, *dbx = hp->dbox, *a = hp->abox;
+    const int cj = b[3] - b[2], ck = b[5] - b[4];
+    const int dj = dbx[3] - dbx[2], dk = dbx[5] - dbx[4];
+    auto cidx = [&](int i, int j, int k) { return ((size_t)(i - b[0]) * cj + (j - b[2])) * ck + (k - b[4]); };
+    auto in_design = [&](int i, int j, int k) {
+        return i >= dbx[0] && i < dbx[1] && j >= dbx[2] && j < dbx[3] && k >= dbx[4] && k < dbx[5];
+    };
+    const size_t nd = (size_t)(dbx[1] - dbx[0]) * dj * dk;
+    for (size_t q = 0; q < nd; q++) grad[q] = 0.0;
+    const double dt = hp->dt, dx = hp->dx;
+    size_t q = 0;
+    for (int i = a[0]; i < a[1]; i++)
+        for (int j = a[2]; j < a[3]; j++)
+            for (int k = a[4]; k < a[5]; k++, q++) {
+                const bool avg = hp->bnds[((size_t)i * hp->yr + j) * hp->zr + k] > 0;
+                // the cells each component averages over (get_cabs), own cell first
+                const int sets[3][4][3] = {{{i, j, k}, {i, j - 1, k}, {i, j, k - 1}, {i, j - 1, k - 1}},
+                                           {{i, j, k}, {i - 1, j, k}, {i, j, k - 1}, {i - 1, j, k - 1}},
+                                           {{i, j, k}, {i - 1, j, k}, {i, j - 1, k}, {i - 1, j - 1, k}}};
+                const int nc = avg ? 4 : 1;
+                for (int c = 0; c < 3; c++) {
+                    double e = 0;
+                    for (int m = 0; m < nc; m++) e += hp->ctx_eps[cidx(sets[c][m][0], sets[c][m][1], sets[c][m][2])];
+                    e /= nc;
+                    const double w = dcb[3 * q + c] * (-dt / (e * e * dx)) / nc * EPS0;
+                    for (int m = 0; m < nc; m++) {
+                        const int ii = sets[c][m][0], jj = sets[c][m][1], kk = sets[c][m][2];
+                        if (in_design(ii, jj, kk)) grad[((size_t)(ii - dbx[0]) * dj + (jj - dbx[2])) * dk + (kk - dbx[4])] += w;
+                    }
+                }
+            }
+}
+

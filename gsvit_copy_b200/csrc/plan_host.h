@@ -29,6 +29,23 @@ struct HostPlan {
     std::vector<uint8_t> tmap[6];
     int tmap_dims[6][2];
     std::vector<int64_t> probes;         // linear cell indices
+    // adjoint design region: per-cell epsilon of the box dbox; the E
+    // coefficients of the affected box abox (dbox plus one cell above on each
+    // axis) are per cell, 6 floats (ca[3], cb[3]) each, from the epsilon and
+    // sigma of the context box (abox plus one cell below on each axis)
+    bool design = false;
+    int dbox[6] = {0, 0, 0, 0, 0, 0}, abox[6] = {0, 0, 0, 0, 0, 0}, cbox[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<double> ctx_eps, ctx_sig;
+    std::vector<float> dcoef;
 };
+
+// recompute the per-cell coefficients of the design region for new relative
+// permittivities of its cells (eps_r, dbox order, k fastest)
+void design_coefficients(HostPlan *hp, const double *eps_r);
+
+// dJ/d eps_r of every design cell (dbox order) from dJ/dcb of the affected
+// cells (3 per cell, abox order): the chain rule through the edge averaging
+// of get_cabs (yee.c:1397-1493) of lossless cells, cb = dt / (eps dx)
+void design_gradient(const HostPlan *hp, const double *dcb, double *grad);
 
 int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err);

@@ -252,6 +252,7 @@ class Scene:
     nfff: Optional[dict] = None
     probes: Optional[np.ndarray] = None
     storage: int = abi.STORE_F32
+    design: Optional[dict] = None       # adjoint design region: box=(i0,i1,j0,j1,k0,k1), eps=array of the box
     meta: dict = field(default_factory=dict)
 
     @property
@@ -334,7 +335,33 @@ class Scene:
             keep.append(p)
             d.nprobes = len(p)
             d.probes = abi.as_ptr(p, C.c_int32)
+        if self.design:
+            b = self.design["box"]
+            e = np.ascontiguousarray(self.design["eps"], dtype=np.float64).reshape(-1)
+            keep.append(e)
+            d.design.enabled = 1
+            d.design.i0, d.design.i1, d.design.j0, d.design.j1, d.design.k0, d.design.k1 = b
+            d.design.eps_r = abi.as_ptr(e, C.c_double)
         return d, keep
+
+    def expanded(self) -> "Scene":
+        """The same scene with every design cell as a LINTAB material of its
+        own (epsilon = eps_r * EPS0 in double precision): the form the
+        reference's material table takes, for CPU paths that have no design
+        region."""
+        if not self.design:
+            return self
+        import copy
+        s = copy.copy(self)
+        i0, i1, j0, j1, k0, k1 = self.design["box"]
+        eps = np.asarray(self.design["eps"], dtype=np.float64).reshape(i1 - i0, j1 - j0, k1 - k0)
+        base = len(self.mats)
+        s.mats = list(self.mats) + [_mat(type=abi.MAT_LINTAB, epsilon=float(e) * EPS0, mu=1 * MU0, sigma=0.0, sigast=0.0)
+                                    for e in eps.reshape(-1)]
+        s.mat = np.array(self.mat, dtype=np.int32, copy=True)
+        s.mat[i0:i1, j0:j1, k0:k1] = base + np.arange(eps.size, dtype=np.int32).reshape(eps.shape)
+        s.design = None
+        return s
 
 
 def cpml_all(depth: int, m: int, sigma: float, kappa: float, a: float, dx: float) -> Dict[int, tuple]:
@@ -513,3 +540,73 @@ def small_scene(kind: str, shape=(24, 20, 28), nsteps: int = 40, seed: int = 1) 
                   omega=np.array([2 * G_PI * C0 / 300e-9, 2 * G_PI * C0 / 450e-9]))
     s.probes = np.asarray([(xr // 2, yr // 2, zr // 2), (3, 4, 5), (xr - 2, yr - 3, zr - 2)], dtype=np.int32)
     return s
+
+
+def cone_objective(scene: Scene, theta_deg: float = 20.0, half_deg: float = 10.0, phi_deg: float = 0.0,
+                   nth: int = 9, nph: int = 13, freq: int = 0) -> dict:
+    """Far points of a cone of directions within `half_deg` of (theta, phi)
+    and their solid-angle weights sin(theta) dtheta dphi, appended to the
+    scene's far points; returns the objective {freq, points, weights} (point
+    indices into scene.nfff["points"])."""
+    f = scene.nfff
+    th0, ph0, hw = math.radians(theta_deg), math.radians(phi_deg), math.radians(half_deg)
+    ths = np.linspace(max(0.0, th0 - hw), th0 + hw, nth)
+    dth = ths[1] - ths[0]
+    dphw = hw / max(math.sin(th0), 1e-3)
+    phs = np.linspace(ph0 - dphw, ph0 + dphw, nph)
+    dph = phs[1] - phs[0]
+    n0 = np.array([math.sin(th0) * math.cos(ph0), math.sin(th0) * math.sin(ph0), math.cos(th0)])
+    radius = 10 * max(scene.xres, scene.yres, scene.zres)
+    pts, w = [], []
+    for th in ths:
+        for ph in phs:
+            n = np.array([math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)])
+            if math.acos(min(1.0, float(n @ n0))) > hw + 1e-12:
+                continue
+            pts.append((int(radius * n[0]) + scene.xres // 2, int(radius * n[1]) + scene.yres // 2,
+                        int(radius * n[2]) + scene.zres // 2))
+            w.append(math.sin(th) * dth * dph)
+    old = np.asarray(f["points"], dtype=np.int32).reshape(-1, 3)
+    new = np.asarray(pts, dtype=np.int32)
+    f["points"] = np.concatenate([old, new]) if len(old) else new
+    f["istart"] = nfff_istart(f["points"], scene.dt, scene.dx, shared=False)
+    return dict(freq=freq, points=np.arange(len(old), len(old) + len(new), dtype=np.int32),
+                weights=np.asarray(w, dtype=np.float64))
+
+
+def adjoint_scene(shape=(256, 256, 128), dx: float = 10e-9, cpml_depth: int = 12, nsteps: int = 4000,
+                  design_shape=(64, 64, 16), seed: int = 5, eps_range=(1.5, 4.0), glass_eps: float = 2.1,
+                  glass_cells: int = 20, wavelength: float = 550e-9, margin: int = 4,
+                  pulse_delay: float = 15e-15, pulse_width: float = 5e-15) -> Scene:
+    """Adjoint workload: a design box of per-cell permittivity (seeded uniform
+    in eps_range) on a glass slab (eps_r 2.1) inside the TSF box, lit at
+    normal incidence (theta = 0, x-polarised) by a 550 nm Gaussian pulse
+    (width 5 fs, delay 15 fs by default); NFFF box between the CPML and the TSF box with
+    a running DFT at 550 nm.  Default: 256 x 256 x 128 cells of 10 nm, 12-cell
+    CPML, 64 x 64 x 16 design cells, 4000 steps, DT_MULT 0.5."""
+    xr, yr, zr = shape
+    dt = plan_dt(dx, dx, dx, 0.5)
+    s = Scene(name=f"adjoint{xr}x{yr}x{zr}", xres=xr, yres=yr, zres=zr, dx=dx, dt=dt, nsteps=nsteps)
+    s.mats = [vacuum_material(), lintab_material(glass_eps)]
+    s.mat = np.zeros(shape, dtype=np.int32)
+    lo = cpml_depth + margin
+    g0 = lo + margin
+    gk1 = g0 + glass_cells
+    s.mat[g0:xr - g0, g0:yr - g0, g0:gk1] = 1
+    dxs, dys, dzs = design_shape
+    i0, j0 = xr // 2 - dxs // 2, yr // 2 - dys // 2
+    box = (i0, i0 + dxs, j0, j0 + dys, gk1, gk1 + dzs)
+    if not (i0 > lo and i0 + dxs < xr - lo and j0 > lo and j0 + dys < yr - lo and gk1 + dzs < zr - lo):
+        raise ValueError("the design box (and the cells above it) must lie strictly inside the TSF box")
+    rng = np.random.default_rng(seed)
+    s.design = dict(box=box, eps=rng.uniform(eps_range[0], eps_range[1], size=design_shape))
+    s.cpml = cpml_all(cpml_depth, 3, -1, 1.0, 0.0, dx)
+    s.tsf = dict(box=((lo, lo, lo), (xr - lo, yr - lo, zr - lo)), theta=0.0, phi=0.0, psi=0.0,
+                 skip=[0] * 6, skipdepth=-1,
+                 wave=gaussian_pulse(nsteps + 1, dt, wavelength, pulse_delay, pulse_width))
+    nlo = cpml_depth + 2
+    s.nfff = dict(box=((nlo, nlo, nlo), (xr - nlo, yr - nlo, zr - nlo)), points=np.zeros((0, 3), dtype=np.int32),
+                  omega=np.array([2 * G_PI * C0 / wavelength]))
+    s.probes = np.asarray([(xr // 2, yr // 2, min(zr - lo - 2, gk1 + dzs + 4))], dtype=np.int32)
+    return s
+

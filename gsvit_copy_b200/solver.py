@@ -150,6 +150,50 @@ class Solver:
         cbuf = (C.c_char * len(buf)).from_buffer(buf)
         abi.check(self.lib.fdtd_snapshot_restore(self.h, C.cast(cbuf, C.c_void_p), len(buf)), "fdtd_snapshot_restore")
 
+    # -- adjoint (design region, far-field objective)
+    def set_design_eps(self, eps: np.ndarray):
+        """New relative permittivities of the design cells (shape of the box)."""
+        e = np.ascontiguousarray(eps, dtype=np.float64).reshape(-1)
+        abi.check(self.lib.fdtd_set_design_eps(self.h, e.ctypes.data_as(C.POINTER(C.c_double))), "fdtd_set_design_eps")
+        self.scene.design = dict(self.scene.design, eps=np.array(eps, dtype=np.float64).reshape(self._design_shape()))
+
+    def _design_shape(self):
+        i0, i1, j0, j1, k0, k1 = self.scene.design["box"]
+        return (i1 - i0, j1 - j0, k1 - k0)
+
+    @staticmethod
+    def _objective(obj: dict):
+        pts = np.ascontiguousarray(obj["points"], dtype=np.int32)
+        w = np.ascontiguousarray(obj["weights"], dtype=np.float64)
+        o = abi.Objective(freq=int(obj.get("freq", 0)), npoints=len(pts), points=abi.as_ptr(pts, C.c_int32),
+                          weights=abi.as_ptr(w, C.c_double))
+        return o, (pts, w)
+
+    def objective_value(self, obj: dict) -> float:
+        """J = sum_t w_t |F(p_t)|^2 of the far field accumulated so far."""
+        o, keep = self._objective(obj)
+        J = C.c_double()
+        abi.check(self.lib.fdtd_objective_value(self.h, C.byref(o), C.byref(J)), "fdtd_objective_value")
+        return J.value
+
+    def adjoint_gradient(self, obj: dict, nsteps: int, checkpoint: int = 200):
+        """Forward nsteps (checkpointed), J, and dJ/d eps_r of the design cells
+        by the discrete adjoint; returns (J, grad with the design box shape)."""
+        o, keep = self._objective(obj)
+        J = C.c_double()
+        grad = np.zeros(self._design_shape())
+        abi.check(self.lib.fdtd_adjoint_gradient(self.h, C.byref(o), nsteps, checkpoint, C.byref(J),
+                                                 grad.ctypes.data_as(C.POINTER(C.c_double))), "fdtd_adjoint_gradient")
+        return J.value, grad
+
+    def adjoint_transpose(self, comps: Sequence[np.ndarray], nsteps: int):
+        """The transposed step applied nsteps times to an adjoint state (E then
+        H components); returns the six new components."""
+        arrs = [np.ascontiguousarray(c, dtype=np.float64).copy() for c in comps]
+        ptrs = (C.POINTER(C.c_double) * 6)(*[a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs])
+        abi.check(self.lib.fdtd_adjoint_transpose(self.h, nsteps, ptrs), "fdtd_adjoint_transpose")
+        return arrs
+
 
 class Batch:
     """Many scenes stepped in lockstep, one launch per kernel for all of them

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define FDTD_ABI_VERSION 1
+#define FDTD_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define FDTD_OK              0
@@ -163,6 +163,22 @@ typedef struct fdtd_nfff {
     const double *omega;                /* nfreq angular frequencies (rad/s)  */
 } fdtd_nfff;
 
+/* Design region of the adjoint (no counterpart in the reference, which takes
+ * per-cell permittivity only through voxel arrays or one material per cell):
+ * the relative permittivity of every cell of a box of lossless, non-magnetic
+ * dielectric cells, in double precision.  The cells keep their material
+ * index (vacuum or a LINTAB material, whose epsilon is then ignored).  The
+ * E coefficients of the box and of the cells one step above it on each axis
+ * (which average epsilon over the cells sharing an edge, yee.c:1397-1493)
+ * are held per cell; that box must lie outside every CPML slab and strictly
+ * inside the TSF box, and the bulk kernel stays off for such plans. */
+typedef struct fdtd_design {
+    int32_t enabled;
+    int32_t i0, i1, j0, j1, k0, k1;     /* half-open cell ranges            */
+    int32_t reserved;
+    const double *eps_r;                /* (i1-i0)*(j1-j0)*(k1-k0), k fastest */
+} fdtd_design;
+
 typedef struct fdtd_desc {
     int32_t abi_version;                /* FDTD_ABI_VERSION                  */
     int32_t xres, yres, zres;
@@ -181,6 +197,7 @@ typedef struct fdtd_desc {
     int32_t nprobes;
     int32_t reserved;
     const int32_t *probes;              /* 3*nprobes cells (i,j,k)           */
+    fdtd_design design;                 /* adjoint design region (optional)  */
 } fdtd_desc;
 
 typedef struct fdtd_plan fdtd_plan;
@@ -219,6 +236,10 @@ int fdtd_get_fields_f32(fdtd_plan *plan, int mask, float *const comps[6]);
 
 /* Host -> device copy from FP32 arrays (used by end-to-end timing with
  * pinned host buffers). */
+/* New relative permittivities of the design region's cells (dbox order, k
+ * fastest); takes effect from the next step.  No counterpart in the reference. */
+int fdtd_set_design_eps(fdtd_plan *plan, const double *eps_r);
+
 int fdtd_set_fields_f32(fdtd_plan *plan, int mask, const float *const comps[6]);
 
 /* ---- stepping ------------------------------------------------------------ */
@@ -350,6 +371,39 @@ const char *fdtd_last_error(void);
  * map, CPML slabs, ADE state, NFFF accumulators) -- the numerator of the
  * roofline figure. */
 int fdtd_step_bytes(const fdtd_plan *plan, double *bytes);
+
+/* ---- adjoint (no counterpart in the reference) --------------------------
+ * Objective: far-field power at one running-DFT frequency over selected far
+ * points, J = sum_t w_t (|F_x(p_t)|^2 + |F_y(p_t)|^2 + |F_z(p_t)|^2), with F
+ * the spectrum of fdtd_nfff_spectrum(). */
+typedef struct fdtd_objective {
+    int32_t freq;                       /* index into nfff.omega             */
+    int32_t npoints;
+    const int32_t *points;              /* indices into nfff.points          */
+    const double *weights;              /* npoints weights (e.g. solid angle) */
+} fdtd_objective;
+
+/* J of the far field accumulated so far. */
+int fdtd_objective_value(fdtd_plan *plan, const fdtd_objective *obj, double *J);
+
+/* Runs nsteps forward steps from the plan's current state, keeping a device
+ * checkpoint of the full stepping state every `checkpoint` steps, evaluates
+ * J, then the discrete adjoint of those steps backwards, recomputing each
+ * segment of the forward run from its checkpoint (the lossy CPML makes the
+ * step irreversible).  grad[c] = dJ/d eps_r of every design cell (dbox
+ * order, k fastest).  Needs a design region, FP32 storage, no dispersive
+ * material and the running-DFT far field.  On return the plan holds the
+ * forward state after nsteps.  Device memory: (nsteps/checkpoint + 1) copies
+ * of the stepping state (fdtd_snapshot_size) plus checkpoint x 12 bytes per
+ * cell of the design box. */
+int fdtd_adjoint_gradient(fdtd_plan *plan, const fdtd_objective *obj, int nsteps, int checkpoint,
+                          double *J, double *grad);
+
+/* The transposed step applied nsteps times to an adjoint state (E then H
+ * components, N values each, in place; psi adjoints start at zero): the
+ * operator the gradient runs, exposed for checking against an independent
+ * transpose. */
+int fdtd_adjoint_transpose(fdtd_plan *plan, int nsteps, double *const comps[6]);
 
 #ifdef __cplusplus
 }

@@ -1386,3 +1386,138 @@ int oracle_get_aux(const oracle_state *s, double *e, double *h)
 }
 
 int oracle_get_step(const oracle_state *s) { return s->step; }
+
+/* ------------------------------------------------- linear-step coefficients */
+
+/* The coefficients of the source-free step as the loops above apply them,
+ * for the FP64 adjoint restatement (oracle/adjoint.py).  Per cell c (N cells,
+ * component a): ca[a*N + c], cb[a*N + c] (get_cabs, yee.c:1397-1493), da[c],
+ * db[c] (ystep_h, yee.c:219-243), flags[c]: bits 0-2 the tbc of get_tbc,
+ * bits 3-5 the components the PEC rule of ystep_e zeroes (yee.c:1138-1237),
+ * bit 6 a cell of the dispersive branch. */
+int oracle_get_coeffs(const oracle_state *s, double *ca, double *cb, double *da, double *db, int32_t *flags)
+{
+    const int xr = s->xres, yr = s->yres, zr = s->zres;
+    const size_t N = (size_t)xr * yr * zr, sj = (size_t)zr, si = (size_t)yr * zr;
+    int i, j, k;
+    for (i = 0; i < xr; i++)
+        for (j = 0; j < yr; j++)
+            for (k = 0; k < zr; k++) {
+                size_t c = IDX(s, i, j, k);
+                double a3[3], b3[3], dt = s->dt;
+                int xt, yt, zt, m, f = 0, a;
+                m = matidx(s, i, j, k);
+                if (m > 0 && is_tab(s->mats[m].type)) {
+                    const fdtd_material *q = &s->mats[m];
+                    da[c] = (1 - q->sigast * dt / 2 / q->mu) / (1 + q->sigast * dt / 2 / q->mu);
+                    db[c] = (dt / q->mu / s->dx) / (1 + q->sigast * dt / 2 / q->mu);
+                } else if (s->matmode == FDTD_MATMODE_FULL || s->matmode == FDTD_MATMODE_MAGNETIC) {
+                    double mu = s->vmu[c], sa = s->vsigast[c];
+                    da[c] = (1 - sa * dt / 2 / mu) / (1 + sa * dt / 2 / mu);
+                    db[c] = (dt / mu / s->dx) / (1 + sa * dt / 2 / mu);
+                } else {
+                    da[c] = 1;
+                    db[c] = dt / MU0 / s->dx;
+                }
+                m = get_tbc(s, i, j, k, &xt, &yt, &zt);
+                get_cabs(s, i, j, k, a3, b3);
+                for (a = 0; a < 3; a++) { ca[a * N + c] = a3[a]; cb[a * N + c] = b3[a]; }
+                f = (xt ? 1 : 0) | (yt ? 2 : 0) | (zt ? 4 : 0);
+                if (s->nmat > 0 && s->disp && xt * yt * zt == 0) f |= 64;
+                if (m >= 0 && i > 0 && j > 0 && k > 0) {
+                    const int *mt = s->mat;
+                    int t0 = s->mats[mt[c]].type, tx = s->mats[mt[c - si]].type, ty = s->mats[mt[c - sj]].type;
+                    int tz = s->mats[mt[c - 1]].type, txy = s->mats[mt[c - si - sj]].type;
+                    int tyz = s->mats[mt[c - sj - 1]].type, txz = s->mats[mt[c - si - 1]].type;
+                    int txyz = s->mats[mt[c - si - sj - 1]].type;
+                    const int P = FDTD_MAT_PEC;
+                    if (s->mats[m].type == P || tx == P || ty == P || tz == P || txy == P || tyz == P || txz == P || txyz == P) {
+                        if ((tx != P && t0 == P) || (tx == P && t0 != P)) f |= 16 | 32;
+                        if ((ty != P && t0 == P) || (ty == P && t0 != P)) f |= 8 | 32;
+                        if ((tz != P && t0 == P) || (tz == P && t0 != P)) f |= 8 | 16;
+                        if (txy == P && t0 != P) f |= 32;
+                        if (txz == P && t0 != P) f |= 16;
+                        if (tyz == P && t0 != P) f |= 8;
+                    }
+                }
+                flags[c] = f;
+            }
+    return 0;
+}
+
+/* CPML profiles of one face (cpml_grade): depth entries each; returns the
+ * depth, 0 for a disabled face. */
+int oracle_get_cpml(const oracle_state *s, int face, double *be, double *ce, double *bh, double *ch, double *ke, double *kh)
+{
+    int i, d;
+    if (face < 0 || face > 5 || !s->cp[face].enabled)
+        return 0;
+    d = s->cp[face].depth;
+    for (i = 0; i < d; i++) {
+        be[i] = s->be[face][i]; ce[i] = s->ce[face][i];
+        bh[i] = s->bh[face][i]; ch[i] = s->ch[face][i];
+        ke[i] = s->ke[face][i]; kh[i] = s->kh[face][i];
+    }
+    return d;
+}
+
+/* Transpose of farfield() for the E set of the step whose far-field call saw
+ * s->step == step: for the far points pts[0..npts), out[a*N + c] += the sum
+ * over the taps of farfield() that read E[a][c] of their coefficient times
+ * lam[(p*3 + a)*ndata + m] (lam = dJ/dF of the time-domain series). */
+int oracle_farfield_transpose(const oracle_state *s, int step, int npts, const int32_t *pts, const double *lam, double *out)
+{
+    const int i0 = s->ff.i0, i1 = s->ff.in, j0 = s->ff.j0, j1 = s->ff.jn, k0 = s->ff.k0, k1 = s->ff.kn;
+    const int ix = i1 - i0, iy = j1 - j0, iz = k1 - k0;
+    const double dx = s->dx, dy = s->dy, dz = s->dz, dt = s->dt;
+    const int nd = s->ndata;
+    const size_t N = (size_t)s->xres * s->yres * s->zres;
+    int t;
+    if (!s->nfff) return -1;
+    for (t = 0; t < npts; t++) {
+        const int n = pts[t];
+        int f;
+        for (f = 0; f < 3; f++) {
+            int ua, ub, na, nb;
+            double size = (f == 0) ? dy * dz : (f == 1) ? dx * dz : dx * dy;
+            if (f == 0) { na = iy; nb = iz; } else if (f == 1) { na = ix; nb = iz; } else { na = ix; nb = iy; }
+            for (ua = 0; ua < na; ua++)
+                for (ub = 0; ub < nb; ub++) {
+                    int side;
+                    for (side = 0; side < 2; side++) {
+                        int face = 2 * f + side;
+                        int lo0, lo1, pos, ci, cj, ck, a, nn;
+                        size_t tab = (size_t)n * (size_t)na * nb + (size_t)ua * nb + ub;
+                        double r, ct, a1, b1, c1;
+                        size_t cc, cp, cm;
+                        if (f == 0) { ci = side ? i1 : i0; cj = j0 + ua; ck = k0 + ub; lo0 = cj; lo1 = ck; }
+                        else if (f == 1) { ci = i0 + ua; cj = side ? j1 : j0; ck = k0 + ub; lo0 = ci; lo1 = ck; }
+                        else { ci = i0 + ua; cj = j0 + ub; ck = side ? k1 : k0; lo0 = ci; lo1 = cj; }
+                        if (s->ff.skip[face] && lo0 >= s->ff.skip_lo[face][0] && lo1 >= s->ff.skip_lo[face][1] &&
+                            lo0 <= s->ff.skip_hi[face][0] && lo1 <= s->ff.skip_hi[face][1])
+                            continue;
+                        r = s->ffr[face][tab] * dx;
+                        ct = s->ffct[face][tab];
+                        nn = (int)(step + 1 + r / (C0 * dt)) - s->ffistart[n];
+                        if (nn < 3 || nn >= nd)
+                            continue;
+                        a1 = 1.0 / (4.0 * PI_D * r);
+                        b1 = -1.0 / (4.0 * PI_D) * ct / (r * r);
+                        c1 = -1.0 / (4.0 * PI_D) * ct / (C0 * r);
+                        cc = IDX(s, ci, cj, ck);
+                        if (f == 0) { cp = IDX(s, ci + 1, cj, ck); cm = IDX(s, ci - 1, cj, ck); }
+                        else if (f == 1) { cp = IDX(s, ci, cj + 1, ck); cm = IDX(s, ci, cj - 1, ck); }
+                        else { cp = IDX(s, ci, cj, ck + 1); cm = IDX(s, ci, cj, ck - 1); }
+                        pos = side ? 1 : -1;
+                        for (a = 0; a < 3; a++) {
+                            const double *L = lam + ((size_t)n * 3 + a) * nd;
+                            out[a * N + cc] += (-c1 / 2.0 / dt * L[nn] + b1 * L[nn - 1] + c1 / 2.0 / dt * L[nn - 2]) * size;
+                            out[a * N + cp] += pos * a1 / 2.0 / dx * L[nn - 1] * size;
+                            out[a * N + cm] -= pos * a1 / 2.0 / dx * L[nn - 1] * size;
+                        }
+                    }
+                }
+        }
+    }
+    return 0;
+}

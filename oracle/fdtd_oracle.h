@@ -56,6 +56,17 @@ int oracle_get_aux(const oracle_state *s, double *e, double *h);
 
 int oracle_get_step(const oracle_state *s);
 
+/* Coefficients of the source-free linear step (for the FP64 adjoint):
+ * ca, cb: 3*N component-major; da, db: N; flags: N (bits 0-2 tbc, 3-5 PEC
+ * zeroed components, 6 dispersive cell). */
+int oracle_get_coeffs(const oracle_state *s, double *ca, double *cb, double *da, double *db, int32_t *flags);
+/* Transpose of the far-field series of one step (the step index its
+ * far-field call saw): out[a*N + c] += sum over the far points pts of the tap
+ * coefficients that read E[a][c] times lam[(p*3 + a)*ndata + m]. */
+int oracle_farfield_transpose(const oracle_state *s, int step, int npts, const int32_t *pts, const double *lam, double *out);
+/* CPML profiles of a face; returns its depth (0 when disabled). */
+int oracle_get_cpml(const oracle_state *s, int face, double *be, double *ce, double *bh, double *ch, double *ke, double *kh);
+
 #ifdef __cplusplus
 }
 #endif
