@@ -213,10 +213,6 @@ std::vector<BulkItem> bulk_items(const int lo[3], const int hi[3], int len, int 
     return blk;
 }
 
-int bulk_tiles(const int lo[3], const int hi[3])
-{
-    return ((hi[1] - lo[1] + BULK_TJ - 1) / BULK_TJ) * ((hi[2] - lo[2] + BULK_TK - 1) / BULK_TK);
-}
 
 int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool pole_arrays);
 
@@ -617,8 +613,6 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     // kernel when the k rows are 16-byte multiples; the rest (slabs, edge
     // planes) to the general kernel
     {
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         const int X = hp.xr, Y = hp.yr, Z = hp.zr;
         int lo[3], hi[3];
         const int res[3] = {X, Y, Z};
@@ -638,10 +632,15 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             boxes.push_back({i0, i1, j0, j1, k0, k1, nblk, 0, 0});
             nblk += ((long long)(i1 - i0) * (j1 - j0) * (k1 - k0) + 255) / 256;
         };
-        auto chunks = [&](int a0, int a1, int tiles, int *len) {
-            int planes = a1 - a0;
-            int want = std::max(1, (8 * sms + tiles - 1) / std::max(tiles, 1));
-            int nch = std::max(1, std::min(want, planes / 24));
+        // planes per work item: about 10.  CTAs of neighbouring tiles then stay
+        // within a few planes of each other, so that the halo rows and columns
+        // one reads are still in L2 when the other reads them (the tiles of the
+        // Drude-metal half run about 2x slower than the vacuum half: with 96
+        // planes per item their drift evicted the halos; 512^3 rough surface,
+        // bulk kernel 2.24 ms at 96 planes, 1.72 ms at 8-12, 1.79 ms at 4)
+        auto chunks = [&](int a0, int a1, int *len) {
+            const int planes = a1 - a0;
+            const int nch = std::max(1, (planes + 9) / 10);
             *len = (planes + nch - 1) / nch;
         };
         if (P->bulk_on) {
@@ -652,7 +651,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             add_box(lo[0], hi[0], lo[1], hi[1], 0, lo[2]);
             add_box(lo[0], hi[0], lo[1], hi[1], hi[2], Z);
             int len;
-            chunks(lo[0], hi[0], bulk_tiles(lo, hi), &len);
+            chunks(lo[0], hi[0], &len);
             blk = bulk_items(lo, hi, len, 0);
             P->bulk_len = len;
             for (int ax = 0; ax < 3; ax++) { P->region[2 * ax] = lo[ax]; P->region[2 * ax + 1] = hi[ax]; }
