@@ -99,6 +99,8 @@ struct fdtd_plan {
     SlabBox *d_boxes = nullptr;     // slab boxes (one thread per cell)
     int nboxes = 0;
     long long nslab_blocks = 0;
+    SlabBox *d_boxes4 = nullptr;    // the same numbered in 4-cell groups (H kernel), when all are 4-aligned
+    long long nslab_blocks4 = 0;
     BulkItem *d_bulk = nullptr;
     int nbulk = 0;
     bool bulk_on = false;
@@ -155,7 +157,7 @@ int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
         e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
     }
-    e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
+    e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->d_boxes4, P->nslab_blocks4, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
     if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
     return FDTD_OK;
 }
@@ -688,6 +690,20 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             P->bulk_bytes = P->bulk_on ? cell_bytes(lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]) : 0;
         }
         CA(upload(P->mem, &P->d_boxes, boxes.data(), boxes.size()), "slab boxes");
+        {   // 4-cell groups for the H kernel when every box's k bounds and the row length allow
+            bool w4 = (Z % 4 == 0);
+            for (auto &b : boxes) w4 = w4 && b.k0 % 4 == 0 && b.k1 % 4 == 0;
+            if (w4 && !boxes.empty()) {
+                std::vector<SlabBox> b4 = boxes;
+                long long nb = 0;
+                for (auto &b : b4) {
+                    b.first_block = nb;
+                    nb += ((long long)(b.i1 - b.i0) * (b.j1 - b.j0) * ((b.k1 - b.k0) / 4) + 255) / 256;
+                }
+                CA(upload(P->mem, &P->d_boxes4, b4.data(), b4.size()), "slab boxes");
+                P->nslab_blocks4 = nb;
+            }
+        }
         P->h_boxes = boxes;
         P->h_bulk = blk;
         P->nboxes = (int)boxes.size();
@@ -1088,7 +1104,7 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
             if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
         }
         CK(cudaEventRecord(E[2], st));
-        cudaError_t e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
+        cudaError_t e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->d_boxes4, P->nslab_blocks4, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
         CK(cudaEventRecord(E[3], st));
         launch_nfff(P, in, st);

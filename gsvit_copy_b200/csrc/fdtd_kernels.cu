@@ -37,7 +37,7 @@ enum { X0 = 0, XN = 1, Y0 = 2, YN = 3, Z0 = 4, ZN = 5 };
 // zeroed by boundary_hstep (boundary.c:418-420, 455-457, 490-492), applied to
 // H after ystep_h.  `owner` cells write their psi_H.
 template <class T>
-__device__ __noinline__ float3 h_special(const DevPlan &P, int i, int j, int k, bool owner, float db, float dey_i,
+__device__ __forceinline__ float3 h_special(const DevPlan &P, int i, int j, int k, bool owner, float db, float dey_i,
                                          float dez_i, float dex_j, float dez_j, float dex_k, float dey_k, float3 hin)
 {
     const uint32_t stp = sr_step<T>(P);
@@ -389,6 +389,76 @@ __device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int 
     stH<T>(P, P.fout[3], c, h[0], stp, 3);
     stH<T>(P, P.fout[4], c, h[1], stp, 4);
     stH<T>(P, P.fout[5], c, h[2], stp, 5);
+}
+
+// Four consecutive k cells per thread (boxes whose k bounds and row length
+// are multiples of 4, as all of them are next to the bulk kernel): 16-byte
+// loads of E and H, the same per-cell update as slab_h_cell with the four
+// cells' loads in flight together, 16-byte stores.
+__device__ __forceinline__ bool box_group4(const SlabBox *boxes, int nboxes, int &i, int &j, int &k)
+{
+    int b = 0;
+    while (b + 1 < nboxes && (long long)blockIdx.x >= boxes[b + 1].first_block) b++;
+    const SlabBox B = boxes[b];
+    long long t = ((long long)blockIdx.x - B.first_block) * blockDim.x + threadIdx.x;
+    const int nk = (B.k1 - B.k0) / 4, nj = B.j1 - B.j0;
+    if (t >= (long long)(B.i1 - B.i0) * nj * nk) return false;
+    k = B.k0 + 4 * (int)(t % nk);
+    t /= nk;
+    j = B.j0 + (int)(t % nj);
+    i = B.i0 + (int)(t / nj);
+    return true;
+}
+
+template <class T>
+__device__ __forceinline__ void slab_h_cell4(const DevPlan &P, int i, int j, int k)
+{
+    const uint32_t stp = sr_step<T>(P);
+    const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
+    const float *EX = P.fin[0], *EY = P.fin[1], *EZ = P.fin[2];
+    const bool il = (i == P.xr - 1), jl = (j == P.yr - 1), kl = (k + 3 == P.zr - 1);
+    float ex[4], ey[4], ez[4], exj[4], ezj[4], eyi[4], ezi[4], hx[4], hy[4], hz[4];
+    lds4a_f(ex, ldg4_ro<T>(EX, c));
+    lds4a_f(ey, ldg4_ro<T>(EY, c));
+    lds4a_f(ez, ldg4_ro<T>(EZ, c));
+    if (jl) {
+        for (int q = 0; q < 4; q++) exj[q] = ezj[q] = 0.f;
+    } else {
+        lds4a_f(exj, ldg4_ro<T>(EX, c + P.sj));
+        lds4a_f(ezj, ldg4_ro<T>(EZ, c + P.sj));
+    }
+    if (il) {
+        for (int q = 0; q < 4; q++) eyi[q] = ezi[q] = 0.f;
+    } else {
+        lds4a_f(eyi, ldg4_ro<T>(EY, c + P.si));
+        lds4a_f(ezi, ldg4_ro<T>(EZ, c + P.si));
+    }
+    const float exk4 = kl ? 0.f : ldgE<T>(EX, c + 4), eyk4 = kl ? 0.f : ldgE<T>(EY, c + 4);
+    lds4a_f(hx, ldg4_ro<T>(P.fin[3], c));
+    lds4a_f(hy, ldg4_ro<T>(P.fin[4], c));
+    lds4a_f(hz, ldg4_ro<T>(P.fin[5], c));
+    const uint32_t cw = __ldg(reinterpret_cast<const uint32_t *>(P.cls + ((int64_t)i * P.yr + j) * P.cpitch + k));
+    const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        float h[3] = {hx[q], hy[q], hz[q]};
+        if (Stor<T>::scaled) { h[0] *= P.ihs; h[1] *= P.ihs; h[2] *= P.ihs; }
+        const float eyk = q < 3 ? ey[q + 1] : eyk4, exk = q < 3 ? ex[q + 1] : exk4;
+        h_update<T>(P, cl, (cw >> (8 * q)) & 0xff, i, j, k + q, true, true, eyi[q] - ey[q], ezi[q] - ez[q],
+                    exj[q] - ex[q], ezj[q] - ez[q], exk - ex[q], eyk - ey[q], h);
+        hx[q] = h[0]; hy[q] = h[1]; hz[q] = h[2];
+    }
+    const float s = Stor<T>::scaled ? P.hs : 1.f;
+    stg4<T>(P.fout[3], c, make_float4(hx[0], hx[1], hx[2], hx[3]), s, stp, 3);
+    stg4<T>(P.fout[4], c, make_float4(hy[0], hy[1], hy[2], hy[3]), s, stp, 4);
+    stg4<T>(P.fout[5], c, make_float4(hz[0], hz[1], hz[2], hz[3]), s, stp, 5);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256, 2) slab_h4_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
+{
+    int i, j, k;
+    if (box_group4(boxes, nboxes, i, j, k)) slab_h_cell4<T>(P, i, j, k);
 }
 
 template <class T>
@@ -795,10 +865,13 @@ void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st)
 }
 
 template <class T>
-cudaError_t slab_steps_t(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
-                         cudaStream_t st)
+cudaError_t slab_steps_t(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
+                         long long nblocks4, bool ade, int npoles, cudaStream_t st)
 {
-    slab_h_kernel<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    if (nblocks4 > 0)
+        slab_h4_kernel<T><<<(unsigned)nblocks4, 256, 0, st>>>(p, boxes4, nboxes);
+    else
+        slab_h_kernel<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     if (!ade)
         slab_e_kernel<false, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     else if (npoles == 0)
@@ -808,13 +881,14 @@ cudaError_t slab_steps_t(const DevPlan &p, const SlabBox *boxes, int nboxes, lon
     return cudaGetLastError();
 }
 
-cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
-                              int storage, cudaStream_t st)
+cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
+                              long long nblocks4, bool ade, int npoles, int storage, cudaStream_t st)
 {
     if (nblocks <= 0) return cudaSuccess;
-    if (storage == FDTD_STORE_F16) return slab_steps_t<__half>(p, boxes, nboxes, nblocks, ade, npoles, st);
-    if (storage == FDTD_STORE_BF16) return slab_steps_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, ade, npoles, st);
-    return slab_steps_t<float>(p, boxes, nboxes, nblocks, ade, npoles, st);
+    if (storage == FDTD_STORE_F16) return slab_steps_t<__half>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
+    if (storage == FDTD_STORE_BF16)
+        return slab_steps_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
+    return slab_steps_t<float>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
 }
 
 void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st)

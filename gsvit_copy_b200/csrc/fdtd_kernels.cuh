@@ -56,8 +56,10 @@ cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int 
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st);
 void launch_probe_capture(const DevAux &a, cudaStream_t st);
 void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st);
-cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
-                              int storage, cudaStream_t st);
+// boxes4 / nblocks4: the same boxes numbered in 4-cell groups (every k bound
+// and the row length multiples of 4); nblocks4 = 0 runs H one cell per thread
+cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
+                              long long nblocks4, bool ade, int npoles, int storage, cudaStream_t st);
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st);
 
 struct DevFarfield {
