@@ -1296,8 +1296,10 @@ struct fdtd_batch {
     int nitems[3] = {0, 0, 0}, bulk_grid[3] = {0, 0, 0}, chunk_len = 0;
     bool persistent = true;
     SlabBox *d_boxes[3] = {nullptr, nullptr, nullptr};
+    SlabBox *d_boxes4[3] = {nullptr, nullptr, nullptr};   // 4-cell groups when every box of the group is 4-aligned
     int nboxes[3] = {0, 0, 0};
     long long nslab_blocks[3] = {0, 0, 0};
+    long long nslab_blocks4[3] = {0, 0, 0};
     int max_tsf = 0, max_nfff = 0;
     int *d_err = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -1364,8 +1366,8 @@ int batch_launch_step(fdtd_batch *B, cudaStream_t st)
         cudaError_t e = launch_bulk_batch(B->d_plans[in], B->d_maps[in], B->d_items[g], B->nitems[g], B->bulk_grid[g], B->ncls,
                                           B->d_err, ade, npoles, B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched bulk launch: ") + cudaGetErrorString(e));
-        e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], ade, npoles, B->storage,
-                                    st);
+        e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], B->d_boxes4[g],
+                                    B->nslab_blocks4[g], ade, npoles, B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
     }
     if (B->max_nfff) launch_nfff_accumulate_batch(B->d_nfff[in], n, B->max_nfff, st);
@@ -1464,6 +1466,15 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
         if (B->nslab_blocks[g] > 0x7fffffffLL) { fail(FDTD_E_UNSUPPORTED, "too many slab cells for one launch"); return bail(FDTD_E_UNSUPPORTED); }
         BA(upload(B->mem, &B->d_boxes[g], boxes.data(), boxes.size()), "batch slab boxes");
         B->nboxes[g] = (int)boxes.size();
+        bool w4 = !boxes.empty();
+        for (auto &b : boxes) w4 = w4 && B->plans[b.inst]->hp.zr % 4 == 0 && b.k0 % 4 == 0 && b.k1 % 4 == 0;
+        if (w4) {
+            for (auto &b : boxes) {
+                b.first_block = B->nslab_blocks4[g];
+                B->nslab_blocks4[g] += ((long long)(b.i1 - b.i0) * (b.j1 - b.j0) * ((b.k1 - b.k0) / 4) + 255) / 256;
+            }
+            BA(upload(B->mem, &B->d_boxes4[g], boxes.data(), boxes.size()), "batch slab boxes");
+        }
     }
     BA(B->mem.alloc(&B->d_err, 1), "error word");
     BA(batch_set_items(B, 0, true), "batch work list");

@@ -1,22 +1,21 @@
 // fdtd_kernels.cu -- sm_100a kernels of one GSvit FDTD time step.
 //
 // One step = aux_step (1D TSF grid, 1 CTA) -> bulk kernel (fdtd_bulk.cu,
-// fused H+E over the slab-free box) -> slab_h -> slab_e (the CPML slabs and
-// grid edges, one thread per cell) -> nfff_accumulate (running DFT).
+// fused H+E over the slab-free box) -> slab H -> slab E (the CPML slabs and
+// grid edges left outside the bulk box) -> nfff_accumulate (running DFT).
 //
-// fused_step marches along i (the slowest axis of the reference layout
-// data[i][j][k]) over a (j,k) tile.  For plane i it first forms H^{n+1/2}(i)
-// -- ystep_h (yee.c:146-265), the TSF H corrections (source.c:1464-1672),
-// the CPML psi_H update and corrections (boundary.c:347-519) -- on the tile
-// plus the j0-1 row and k0-1 column that the E update needs, keeps it in
-// shared memory, and then forms E^{n+1}(i) -- ystep_e with the ADE branch,
-// its embedded CPML, the ordinary update and the PEC rule (yee.c:530-1247),
+// The slab kernels walk a list of boxes (SlabBox) with a flat block index.
+// slab_h_kernel updates one cell per thread: ystep_h (yee.c:146-265), then
+// h_special -- the CPML psi_H update and corrections (boundary.c:347-519),
+// the TSF H corrections (source.c:1464-1672) and the zeroed outer planes.
+// slab_h4_kernel is the same update on four consecutive k cells per thread
+// with 16-byte loads, used when every box is 4-aligned in k.  slab_e_kernel
+// updates one cell per thread: ystep_e with the ADE branch, its embedded CPML,
+// the ordinary update and the PEC rule (yee.c:530-1247), then e_special --
 // the CPML psi_E update and corrections (boundary.c:691-884) and the TSF E
-// corrections (source.c:547-771).  H^{n+1/2}(i-1) stays in registers from the
-// previous plane.  Reads come from one field set and writes go to the other,
-// so the recomputed halo row never races with the CTA that owns it.
-// Per cell-update the pass moves 6 field reads + 6 field writes + 1 class
-// byte through HBM (49 B); halo reads are served by L1/L2.
+// corrections (source.c:547-771).  Each half step reads one field set and
+// writes the other, so blocks never race on a shared cell.  The *_batch
+// forms take a per-box plan index and serve many plans in one launch.
 #include <cuda_runtime.h>
 
 #include "../../include/gsvit_b200.h"
@@ -354,11 +353,25 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
 // path; slab_e then forms E^{n+1} from the H^{n+1/2} that slab_h and the bulk
 // kernel wrote.  Both read E^n/H^n from the input set only.
 
+// The box of this block: the last one whose first_block is not above
+// blockIdx.x (boxes are numbered in ascending first_block; an empty box shares
+// its successor's first_block and is skipped).  Binary search: a batch lists
+// every instance's boxes, a hundred or more.
+__device__ __forceinline__ int box_of_block(const SlabBox *boxes, int nboxes)
+{
+    const long long bid = blockIdx.x;
+    int lo = 0, hi = nboxes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (boxes[mid].first_block <= bid) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &i, int &j, int &k, int &inst)
 {
-    int b = 0;
-    while (b + 1 < nboxes && (long long)blockIdx.x >= boxes[b + 1].first_block) b++;
-    const SlabBox B = boxes[b];
+    const SlabBox B = boxes[box_of_block(boxes, nboxes)];
     long long t = ((long long)blockIdx.x - B.first_block) * blockDim.x + threadIdx.x;
     const int nk = B.k1 - B.k0, nj = B.j1 - B.j0;
     if (t >= (long long)(B.i1 - B.i0) * nj * nk) return false;
@@ -395,11 +408,9 @@ __device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int 
 // are multiples of 4, as all of them are next to the bulk kernel): 16-byte
 // loads of E and H, the same per-cell update as slab_h_cell with the four
 // cells' loads in flight together, 16-byte stores.
-__device__ __forceinline__ bool box_group4(const SlabBox *boxes, int nboxes, int &i, int &j, int &k)
+__device__ __forceinline__ bool box_group4(const SlabBox *boxes, int nboxes, int &i, int &j, int &k, int &inst)
 {
-    int b = 0;
-    while (b + 1 < nboxes && (long long)blockIdx.x >= boxes[b + 1].first_block) b++;
-    const SlabBox B = boxes[b];
+    const SlabBox B = boxes[box_of_block(boxes, nboxes)];
     long long t = ((long long)blockIdx.x - B.first_block) * blockDim.x + threadIdx.x;
     const int nk = (B.k1 - B.k0) / 4, nj = B.j1 - B.j0;
     if (t >= (long long)(B.i1 - B.i0) * nj * nk) return false;
@@ -407,6 +418,7 @@ __device__ __forceinline__ bool box_group4(const SlabBox *boxes, int nboxes, int
     t /= nk;
     j = B.j0 + (int)(t % nj);
     i = B.i0 + (int)(t / nj);
+    inst = B.inst;
     return true;
 }
 
@@ -457,8 +469,15 @@ __device__ __forceinline__ void slab_h_cell4(const DevPlan &P, int i, int j, int
 template <class T>
 __global__ void __launch_bounds__(256, 2) slab_h4_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
 {
-    int i, j, k;
-    if (box_group4(boxes, nboxes, i, j, k)) slab_h_cell4<T>(P, i, j, k);
+    int i, j, k, inst;
+    if (box_group4(boxes, nboxes, i, j, k, inst)) slab_h_cell4<T>(P, i, j, k);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256, 2) slab_h4_batch(const DevPlan *plans, const SlabBox *boxes, int nboxes)
+{
+    int i, j, k, inst;
+    if (box_group4(boxes, nboxes, i, j, k, inst)) slab_h_cell4<T>(plans[inst], i, j, k);
 }
 
 template <class T>
@@ -475,11 +494,47 @@ __global__ void __launch_bounds__(256, 3) slab_h_batch(const DevPlan *plans, con
     if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell<T>(plans[inst], i, j, k);
 }
 
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// L2 prefetches of the words e_special loads only after its class lookup and
+// the field loads: the psi_E pairs of this cell's CPML faces (the same face
+// tests and indices as e_special) and, in the dispersive variants, the ADE
+// state of all three components (allocated over the whole grid whenever the
+// plan has an ADE material).  Their DRAM latency then overlaps the field
+// loads instead of following them; vacuum cells fetch the ADE words in vain
+// (24 B per cell against ~80 B of traffic).
+template <bool ADE, int NPOLES, class T>
+__device__ __forceinline__ void e_prefetch(const DevPlan &P, int i, int j, int k, int64_t c)
+{
+    const int xr = P.xr, yr = P.yr, zr = P.zr;
+    if ((P.cp_on[X0] && i == 0) || (P.cp_on[Y0] && j == 0) || (P.cp_on[Z0] && k == 0)) return;
+    auto face = [&](int f, int64_t q) {
+        prefetch_l2(reinterpret_cast<const T *>(P.psie[f][0]) + q);
+        prefetch_l2(reinterpret_cast<const T *>(P.psie[f][1]) + q);
+    };
+    if (P.cp_on[X0] && i < P.cp_d[X0]) face(X0, ((int64_t)i * yr + j) * zr + k);
+    if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1) face(XN, ((int64_t)(i - (xr - P.cp_d[XN])) * yr + j) * zr + k);
+    if (P.cp_on[Y0] && j < P.cp_d[Y0]) face(Y0, ((int64_t)i * P.cp_d[Y0] + j) * zr + k);
+    if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1) face(YN, ((int64_t)i * P.cp_d[YN] + (j - (yr - P.cp_d[YN]))) * zr + k);
+    if (P.cp_on[Z0] && k < P.cp_d[Z0]) face(Z0, ((int64_t)i * yr + j) * P.cp_d[Z0] + k);
+    if (P.cp_on[ZN] && k >= zr - P.cp_d[ZN] + 1) face(ZN, ((int64_t)i * yr + j) * P.cp_d[ZN] + (k - (zr - P.cp_d[ZN])));
+    if (ADE) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            prefetch_l2(P.q[a] + c);
+            prefetch_l2(reinterpret_cast<const T *>(P.fout[a]) + c);
+#pragma unroll
+            for (int n = 0; n < NPOLES; n++) { prefetch_l2(P.pc[a][n] + c); prefetch_l2(P.qc[a][n] + c); }
+        }
+    }
+}
+
 template <bool ADE, int NPOLES, class T>
 __device__ __forceinline__ void slab_e_cell(const DevPlan &P, int i, int j, int k)
 {
     const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
+    e_prefetch<ADE, NPOLES, T>(P, i, j, k, c);
     const float *HX = P.fout[3], *HY = P.fout[4], *HZ = P.fout[5];   // H^{n+1/2}, written this step
     const float3 eo = make_float3(ldgE<T>(P.fin[0], c), ldgE<T>(P.fin[1], c), ldgE<T>(P.fin[2], c));
     const float3 h = make_float3(ldH<T>(P, HX, c), ldH<T>(P, HY, c), ldH<T>(P, HZ, c));
@@ -902,10 +957,13 @@ void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStr
 }
 
 template <class T>
-cudaError_t slab_steps_batch_t(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade, int npoles,
-                               cudaStream_t st)
+cudaError_t slab_steps_batch_t(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
+                               long long nblocks4, bool ade, int npoles, cudaStream_t st)
 {
-    slab_h_batch<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    if (nblocks4 > 0)
+        slab_h4_batch<T><<<(unsigned)nblocks4, 256, 0, st>>>(p, boxes4, nboxes);
+    else
+        slab_h_batch<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     if (!ade)
         slab_e_batch<false, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
     else if (npoles == 0)
@@ -915,13 +973,16 @@ cudaError_t slab_steps_batch_t(const DevPlan *p, const SlabBox *boxes, int nboxe
     return cudaGetLastError();
 }
 
-cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade,
-                                    int npoles, int storage, cudaStream_t st)
+cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks,
+                                    const SlabBox *boxes4, long long nblocks4, bool ade, int npoles, int storage,
+                                    cudaStream_t st)
 {
     if (nblocks <= 0) return cudaSuccess;
-    if (storage == FDTD_STORE_F16) return slab_steps_batch_t<__half>(p, boxes, nboxes, nblocks, ade, npoles, st);
-    if (storage == FDTD_STORE_BF16) return slab_steps_batch_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, ade, npoles, st);
-    return slab_steps_batch_t<float>(p, boxes, nboxes, nblocks, ade, npoles, st);
+    if (storage == FDTD_STORE_F16)
+        return slab_steps_batch_t<__half>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
+    if (storage == FDTD_STORE_BF16)
+        return slab_steps_batch_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
+    return slab_steps_batch_t<float>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
 }
 
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st)

@@ -51,8 +51,10 @@ void launch_aux_step(const DevAux &a, cudaStream_t st);
 // device tables (of this step's parity), indexed by the plan number.
 void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st);
 void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStream_t st);
-cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, bool ade,
-                                    int npoles, int storage, cudaStream_t st);
+// boxes4 / nblocks4 as for launch_slab_steps, over every instance of the batch
+cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks,
+                                    const SlabBox *boxes4, long long nblocks4, bool ade, int npoles, int storage,
+                                    cudaStream_t st);
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st);
 void launch_probe_capture(const DevAux &a, cudaStream_t st);
 void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st);
