@@ -494,47 +494,11 @@ __global__ void __launch_bounds__(256, 3) slab_h_batch(const DevPlan *plans, con
     if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell<T>(plans[inst], i, j, k);
 }
 
-__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
-// L2 prefetches of the words e_special loads only after its class lookup and
-// the field loads: the psi_E pairs of this cell's CPML faces (the same face
-// tests and indices as e_special) and, in the dispersive variants, the ADE
-// state of all three components (allocated over the whole grid whenever the
-// plan has an ADE material).  Their DRAM latency then overlaps the field
-// loads instead of following them; vacuum cells fetch the ADE words in vain
-// (24 B per cell against ~80 B of traffic).
-template <bool ADE, int NPOLES, class T>
-__device__ __forceinline__ void e_prefetch(const DevPlan &P, int i, int j, int k, int64_t c)
-{
-    const int xr = P.xr, yr = P.yr, zr = P.zr;
-    if ((P.cp_on[X0] && i == 0) || (P.cp_on[Y0] && j == 0) || (P.cp_on[Z0] && k == 0)) return;
-    auto face = [&](int f, int64_t q) {
-        prefetch_l2(reinterpret_cast<const T *>(P.psie[f][0]) + q);
-        prefetch_l2(reinterpret_cast<const T *>(P.psie[f][1]) + q);
-    };
-    if (P.cp_on[X0] && i < P.cp_d[X0]) face(X0, ((int64_t)i * yr + j) * zr + k);
-    if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1) face(XN, ((int64_t)(i - (xr - P.cp_d[XN])) * yr + j) * zr + k);
-    if (P.cp_on[Y0] && j < P.cp_d[Y0]) face(Y0, ((int64_t)i * P.cp_d[Y0] + j) * zr + k);
-    if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1) face(YN, ((int64_t)i * P.cp_d[YN] + (j - (yr - P.cp_d[YN]))) * zr + k);
-    if (P.cp_on[Z0] && k < P.cp_d[Z0]) face(Z0, ((int64_t)i * yr + j) * P.cp_d[Z0] + k);
-    if (P.cp_on[ZN] && k >= zr - P.cp_d[ZN] + 1) face(ZN, ((int64_t)i * yr + j) * P.cp_d[ZN] + (k - (zr - P.cp_d[ZN])));
-    if (ADE) {
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            prefetch_l2(P.q[a] + c);
-            prefetch_l2(reinterpret_cast<const T *>(P.fout[a]) + c);
-#pragma unroll
-            for (int n = 0; n < NPOLES; n++) { prefetch_l2(P.pc[a][n] + c); prefetch_l2(P.qc[a][n] + c); }
-        }
-    }
-}
-
 template <bool ADE, int NPOLES, class T>
 __device__ __forceinline__ void slab_e_cell(const DevPlan &P, int i, int j, int k)
 {
     const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
-    e_prefetch<ADE, NPOLES, T>(P, i, j, k, c);
     const float *HX = P.fout[3], *HY = P.fout[4], *HZ = P.fout[5];   // H^{n+1/2}, written this step
     const float3 eo = make_float3(ldgE<T>(P.fin[0], c), ldgE<T>(P.fin[1], c), ldgE<T>(P.fin[2], c));
     const float3 h = make_float3(ldH<T>(P, HX, c), ldH<T>(P, HY, c), ldH<T>(P, HZ, c));
