@@ -248,6 +248,28 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                     ldg4a<T>(aep[a], P.fout[a], c0i);
                 }
             }
+            // the next plane's dispersive state into L2 (its class word is
+            // already staged): under full HBM load the H phase alone does not
+            // cover a DRAM round trip, an L2 one it does
+            if (own && ok && i + 1 < ie) {
+                const uint32_t cwn = *reinterpret_cast<const uint32_t *>(cbox<T>(st1) + cb);
+                uint32_t mn = 0;
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const uint32_t fl = __float_as_uint(scls[((cwn >> (8 * c)) & 0xff) * 4].w);
+                    if (fl & CF_ADE_BRANCH) mn |= fl & (CF_ADE_X | CF_ADE_Y | CF_ADE_Z);
+                }
+                const int64_t cn = c0i + si;
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    if (mn & (1u << a)) {
+                        prefetch_l2(P.q[a] + cn);
+                        prefetch_l2(reinterpret_cast<const T *>(P.fout[a]) + cn);
+#pragma unroll
+                        for (int n = 0; n < NPOLES; n++) { prefetch_l2(P.pc[a][n] + cn); prefetch_l2(P.qc[a][n] + cn); }
+                    }
+                }
+            }
         }
         // ---- H phase: four cells per thread
         {

@@ -152,6 +152,9 @@ __device__ __forceinline__ void stPsiE(const DevPlan &P, float *p, int64_t i, fl
     st_any<T>(p, i, Stor<T>::scaled ? v * P.pse : v, stp, array);
 }
 
+// a hint that moves the line holding p into L2; no register, no wait
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // ---- 4-vectors of the storage type
 
 // four consecutive elements from shared memory (16- or 8-byte aligned)
