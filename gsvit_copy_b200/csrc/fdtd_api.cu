@@ -631,7 +631,10 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         long long nblk = 0;
         auto add_box = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
             if (i0 >= i1 || j0 >= j1 || k0 >= k1) return;
-            boxes.push_back({i0, i1, j0, j1, k0, k1, nblk, 0, 0});
+            // TSF corrections touch cells in [t0 - 1, t1] on every axis (tsf_add_h/e)
+            const bool meets = d.tsf_on && i0 <= d.t1[0] && i1 >= d.t0[0] && j0 <= d.t1[1] && j1 >= d.t0[1] &&
+                               k0 <= d.t1[2] && k1 >= d.t0[2];
+            boxes.push_back({i0, i1, j0, j1, k0, k1, nblk, 0, meets ? 1 : 0});
             nblk += ((long long)(i1 - i0) * (j1 - j0) * (k1 - k0) + 255) / 256;
         };
         // planes per work item: about 10.  CTAs of neighbouring tiles then stay

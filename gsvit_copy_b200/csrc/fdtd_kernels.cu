@@ -36,14 +36,14 @@ enum { X0 = 0, XN = 1, Y0 = 2, YN = 3, Z0 = 4, ZN = 5 };
 // zeroed by boundary_hstep (boundary.c:418-420, 455-457, 490-492), applied to
 // H after ystep_h.  `owner` cells write their psi_H.
 template <class T>
-__device__ __forceinline__ float3 h_special(const DevPlan &P, int i, int j, int k, bool owner, float db, float dey_i,
+__device__ __forceinline__ float3 h_special(const DevPlan &P, int i, int j, int k, bool owner, bool tsf, float db, float dey_i,
                                          float dez_i, float dex_j, float dez_j, float dex_k, float dey_k, float3 hin)
 {
     const uint32_t stp = sr_step<T>(P);
     float hx = hin.x, hy = hin.y, hz = hin.z;
     const int xr = P.xr, yr = P.yr, zr = P.zr;
     const bool il = (i == xr - 1), jl = (j == yr - 1), kl = (k == zr - 1);
-    if (P.tsf_on) tsf_add_h(P, i, j, k, hx, hy, hz);
+    if (tsf && P.tsf_on) tsf_add_h(P, i, j, k, hx, hy, hz);
     const bool jin = (j >= 1 && j < yr - 1), kin = (k >= 1 && k < zr - 1), iin = (i >= 1 && i < xr - 1);
     const float dbdx = db * P.dx;
     const float idx_ = 1.0f / P.dx;
@@ -122,7 +122,7 @@ __device__ __forceinline__ float3 h_special(const DevPlan &P, int i, int j, int 
 // yee.c:246-256, then h_special where the cell lies in a slab or on a face).
 template <class T>
 __device__ __forceinline__ void h_update(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k,
-                                         bool special, bool owner, float dey_i, float dez_i, float dex_j, float dez_j,
+                                         bool special, bool owner, bool tsf, float dey_i, float dez_i, float dex_j, float dez_j,
                                          float dex_k, float dey_k, float h[3])
 {
     const float4 hc = scls[cls * 4 + 2];     // da, db
@@ -133,7 +133,7 @@ __device__ __forceinline__ void h_update(const DevPlan &P, const float4 *scls, i
     if (!(il || kl)) h[1] = hc.x * h[1] + hc.y * (dez_i * ikx - dex_k * ikz);
     if (!(il || jl)) h[2] = hc.x * h[2] + hc.y * (dex_j * iky - dey_i * ikx);
     if (special) {
-        const float3 o = h_special<T>(P, i, j, k, owner, hc.y, dey_i, dez_i, dex_j, dez_j, dex_k, dey_k,
+        const float3 o = h_special<T>(P, i, j, k, owner, tsf, hc.y, dey_i, dez_i, dex_j, dez_j, dex_k, dey_k,
                                    make_float3(h[0], h[1], h[2]));
         h[0] = o.x; h[1] = o.y; h[2] = o.z;
     }
@@ -144,7 +144,7 @@ __device__ __forceinline__ void h_update(const DevPlan &P, const float4 *scls, i
 // (yee.c:1138-1237), boundary_estep zero planes, psi_E and corrections
 // (boundary.c:691-884) and TSF E (source.c:547-771).
 template <bool ADE, int NPOLES, class T>
-__device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k,
+__device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k, bool tsf,
                                          float3 eo3, float3 h3, float hx_jm, float hz_jm, float hx_km, float hy_km,
                                          float hy_im, float hz_im)
 {
@@ -342,7 +342,7 @@ __device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, i
             }
         }
     }
-    if (P.tsf_on) tsf_add_e(P, i, j, k, nx, ny, nz);
+    if (tsf && P.tsf_on) tsf_add_e(P, i, j, k, nx, ny, nz);
     return make_float3(nx, ny, nz);
 }
 
@@ -369,7 +369,7 @@ __device__ __forceinline__ int box_of_block(const SlabBox *boxes, int nboxes)
     return lo;
 }
 
-__device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &i, int &j, int &k, int &inst)
+__device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &i, int &j, int &k, int &inst, bool &tsf)
 {
     const SlabBox B = boxes[box_of_block(boxes, nboxes)];
     long long t = ((long long)blockIdx.x - B.first_block) * blockDim.x + threadIdx.x;
@@ -380,13 +380,14 @@ __device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &
     j = B.j0 + (int)(t % nj);
     i = B.i0 + (int)(t / nj);
     inst = B.inst;
+    tsf = B.tsf != 0;
     return true;
 }
 
 // 3 CTAs per SM: the slab kernels are latency-bound, and 24 resident warps
 // beat the register spill this costs e_special (1.95 -> 1.60 ms per 512^3 step)
 template <class T>
-__device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int k)
+__device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int k, bool tsf)
 {
     const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
@@ -398,7 +399,7 @@ __device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int 
     const float ezi = il ? 0.f : ldgE<T>(EZ, c + P.si), eyi = il ? 0.f : ldgE<T>(EY, c + P.si);
     float h[3] = {ldgH<T>(P, P.fin[3], c), ldgH<T>(P, P.fin[4], c), ldgH<T>(P, P.fin[5], c)};
     const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
-    h_update<T>(P, cl, cls_at(P, i, j, k), i, j, k, true, true, eyi - ey, ezi - ez, exj - ex, ezj - ez, exk - ex, eyk - ey, h);
+    h_update<T>(P, cl, cls_at(P, i, j, k), i, j, k, true, true, tsf, eyi - ey, ezi - ez, exj - ex, ezj - ez, exk - ex, eyk - ey, h);
     stH<T>(P, P.fout[3], c, h[0], stp, 3);
     stH<T>(P, P.fout[4], c, h[1], stp, 4);
     stH<T>(P, P.fout[5], c, h[2], stp, 5);
@@ -408,7 +409,7 @@ __device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int 
 // are multiples of 4, as all of them are next to the bulk kernel): 16-byte
 // loads of E and H, the same per-cell update as slab_h_cell with the four
 // cells' loads in flight together, 16-byte stores.
-__device__ __forceinline__ bool box_group4(const SlabBox *boxes, int nboxes, int &i, int &j, int &k, int &inst)
+__device__ __forceinline__ bool box_group4(const SlabBox *boxes, int nboxes, int &i, int &j, int &k, int &inst, bool &tsf)
 {
     const SlabBox B = boxes[box_of_block(boxes, nboxes)];
     long long t = ((long long)blockIdx.x - B.first_block) * blockDim.x + threadIdx.x;
@@ -419,11 +420,12 @@ __device__ __forceinline__ bool box_group4(const SlabBox *boxes, int nboxes, int
     j = B.j0 + (int)(t % nj);
     i = B.i0 + (int)(t / nj);
     inst = B.inst;
+    tsf = B.tsf != 0;
     return true;
 }
 
 template <class T>
-__device__ __forceinline__ void slab_h_cell4(const DevPlan &P, int i, int j, int k)
+__device__ __forceinline__ void slab_h_cell4(const DevPlan &P, int i, int j, int k, bool tsf)
 {
     const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
@@ -456,7 +458,7 @@ __device__ __forceinline__ void slab_h_cell4(const DevPlan &P, int i, int j, int
         float h[3] = {hx[q], hy[q], hz[q]};
         if (Stor<T>::scaled) { h[0] *= P.ihs; h[1] *= P.ihs; h[2] *= P.ihs; }
         const float eyk = q < 3 ? ey[q + 1] : eyk4, exk = q < 3 ? ex[q + 1] : exk4;
-        h_update<T>(P, cl, (cw >> (8 * q)) & 0xff, i, j, k + q, true, true, eyi[q] - ey[q], ezi[q] - ez[q],
+        h_update<T>(P, cl, (cw >> (8 * q)) & 0xff, i, j, k + q, true, true, tsf, eyi[q] - ey[q], ezi[q] - ez[q],
                     exj[q] - ex[q], ezj[q] - ez[q], exk - ex[q], eyk - ey[q], h);
         hx[q] = h[0]; hy[q] = h[1]; hz[q] = h[2];
     }
@@ -470,32 +472,36 @@ template <class T>
 __global__ void __launch_bounds__(256, 2) slab_h4_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_group4(boxes, nboxes, i, j, k, inst)) slab_h_cell4<T>(P, i, j, k);
+    bool tsf;
+    if (box_group4(boxes, nboxes, i, j, k, inst, tsf)) slab_h_cell4<T>(P, i, j, k, tsf);
 }
 
 template <class T>
 __global__ void __launch_bounds__(256, 2) slab_h4_batch(const DevPlan *plans, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_group4(boxes, nboxes, i, j, k, inst)) slab_h_cell4<T>(plans[inst], i, j, k);
+    bool tsf;
+    if (box_group4(boxes, nboxes, i, j, k, inst, tsf)) slab_h_cell4<T>(plans[inst], i, j, k, tsf);
 }
 
 template <class T>
 __global__ void __launch_bounds__(256, 3) slab_h_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell<T>(P, i, j, k);
+    bool tsf;
+    if (box_cell(boxes, nboxes, i, j, k, inst, tsf)) slab_h_cell<T>(P, i, j, k, tsf);
 }
 
 template <class T>
 __global__ void __launch_bounds__(256, 3) slab_h_batch(const DevPlan *plans, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_h_cell<T>(plans[inst], i, j, k);
+    bool tsf;
+    if (box_cell(boxes, nboxes, i, j, k, inst, tsf)) slab_h_cell<T>(plans[inst], i, j, k, tsf);
 }
 
 template <bool ADE, int NPOLES, class T>
-__device__ __forceinline__ void slab_e_cell(const DevPlan &P, int i, int j, int k)
+__device__ __forceinline__ void slab_e_cell(const DevPlan &P, int i, int j, int k, bool tsf)
 {
     const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
@@ -507,7 +513,7 @@ __device__ __forceinline__ void slab_e_cell(const DevPlan &P, int i, int j, int 
     const float hy_im = i > 0 ? ldH<T>(P, HY, c - P.si) : 0.f, hz_im = i > 0 ? ldH<T>(P, HZ, c - P.si) : 0.f;
     const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
     const float3 en =
-        e_special<ADE, NPOLES, T>(P, cl, cls_at(P, i, j, k), i, j, k, eo, h, hx_jm, hz_jm, hx_km, hy_km, hy_im, hz_im);
+        e_special<ADE, NPOLES, T>(P, cl, cls_at(P, i, j, k), i, j, k, tsf, eo, h, hx_jm, hz_jm, hx_km, hy_km, hy_im, hz_im);
     stE<T>(P.fout[0], c, en.x, stp, 0);
     stE<T>(P.fout[1], c, en.y, stp, 1);
     stE<T>(P.fout[2], c, en.z, stp, 2);
@@ -517,14 +523,16 @@ template <bool ADE, int NPOLES, class T>
 __global__ void __launch_bounds__(256, 3) slab_e_kernel(const __grid_constant__ DevPlan P, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_e_cell<ADE, NPOLES, T>(P, i, j, k);
+    bool tsf;
+    if (box_cell(boxes, nboxes, i, j, k, inst, tsf)) slab_e_cell<ADE, NPOLES, T>(P, i, j, k, tsf);
 }
 
 template <bool ADE, int NPOLES, class T>
 __global__ void __launch_bounds__(256, 3) slab_e_batch(const DevPlan *plans, const SlabBox *boxes, int nboxes)
 {
     int i, j, k, inst;
-    if (box_cell(boxes, nboxes, i, j, k, inst)) slab_e_cell<ADE, NPOLES, T>(plans[inst], i, j, k);
+    bool tsf;
+    if (box_cell(boxes, nboxes, i, j, k, inst, tsf)) slab_e_cell<ADE, NPOLES, T>(plans[inst], i, j, k, tsf);
 }
 
 // ------------------------------------------------------------ TSF face tables

@@ -42,7 +42,9 @@ struct DevNfff {
 struct SlabBox {
     int i0, i1, j0, j1, k0, k1;
     long long first_block;
-    int inst, pad;              // plan of the box in a batched launch
+    int inst;                   // plan of the box in a batched launch
+    int tsf;                    // 1 if the box meets the TSF correction region [t0 - 1, t1] on every axis;
+                                // the cells of other boxes skip the TSF test
 };
 
 void launch_aux_step(const DevAux &a, cudaStream_t st);
