@@ -531,6 +531,11 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             const size_t nacc = (size_t)f.nfreq * 6 * cell.size();
             CA(P->mem.alloc(&acc, nacc), "nfff accumulators");
             P->snap.push_back({acc, nacc * sizeof(double2)});
+            float *ring;   // samples not yet folded into acc: part of the state
+            const size_t nring = (size_t)NFFF_RING * 9 * cell.size();
+            CA(P->mem.alloc(&ring, nring), "nfff sample ring");
+            P->snap.push_back({ring, nring * sizeof(float)});
+            P->nf.ring = ring;
             CA(P->mem.alloc(&outp, (size_t)f.npoints * f.nfreq * 3), "nfff output");
             // exp(-i omega R dt) over every retarded index R the box can produce:
             // R <= 1 + (largest point-to-box-corner distance) / (c dt)
@@ -1159,6 +1164,7 @@ int fdtd_nfff_spectrum(fdtd_plan *P, double *out, size_t out_len)
     size_t need = (size_t)P->nfff_npoints * P->nfff_nfreq * 3 * 2;
     if (out_len < need) return fail(FDTD_E_INVALID, "spectrum buffer too small");
     CK(cudaSetDevice(P->device));
+    launch_nfff_fold_pending(P->nf, P->stream);
     launch_farfield_finalize(P->ff, P->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, P->ff.out, need * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
@@ -1799,6 +1805,7 @@ int fdtd_objective_value(fdtd_plan *P, const fdtd_objective *obj, double *J)
     int rc = check_objective(P, obj);
     if (rc != FDTD_OK) return rc;
     CK(cudaSetDevice(P->device));
+    launch_nfff_fold_pending(P->nf, P->stream);
     launch_farfield_finalize(P->ff, P->stream);
     CK(cudaGetLastError());
     return objective_from_spectrum(P, obj, J);
@@ -1853,6 +1860,7 @@ int fdtd_adjoint_gradient(fdtd_plan *P, const fdtd_objective *obj, int nsteps, i
     }
     final_probes(P, P->stream);
     CK(ckpt_save(P, ck, nseg));
+    launch_nfff_fold_pending(P->nf, P->stream);
     launch_farfield_finalize(P->ff, P->stream);
     CK(cudaGetLastError());
     rc = objective_from_spectrum(P, obj, J);

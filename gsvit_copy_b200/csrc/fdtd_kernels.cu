@@ -690,28 +690,66 @@ __global__ void probe_capture_kernel(const DevAux A)
 // ------------------------------------------------------------ NFFF running DFT
 
 // Per surface cell s and frequency f:  Ehat += E(step) w,  Dhat += dE/dn(step) w,
-// w = exp(-i omega step dt).  FP64 accumulators.
+// w = exp(-i omega step dt).  FP64 accumulators.  Each step stores the nine
+// raw E samples of the cell (E, E(c+st), E(c-st) per component) in ring slot
+// step % NFFF_RING; the step that fills the last slot folds the block into the
+// accumulators in step order, with the arithmetic of a per-step update, so the
+// sums are those of accumulating every step (the accumulators are read and
+// written once per NFFF_RING steps instead of every step).
+__device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_step, int nslots, bool clear)
+{
+    const size_t ns = (size_t)N.ns;
+    for (int f = 0; f < N.nfreq; f++) {
+        double2 A[6];
+        for (int q = 0; q < 6; q++) A[q] = N.acc[((size_t)f * 6 + q) * ns + s];
+        for (int j = 0; j < nslots; j++) {
+            const float *r = N.ring + (size_t)j * 9 * ns + s;
+            double v[6];
+            for (int a = 0; a < 3; a++) {
+                v[a] = (double)r[(3 * a) * ns];
+                v[3 + a] = ((double)r[(3 * a + 1) * ns] - (double)r[(3 * a + 2) * ns]) * N.inv2dx;
+            }
+            double sn, cs;
+            sincos(N.omega_dt[f] * (double)(first_step + j), &sn, &cs);
+            for (int q = 0; q < 6; q++) {
+                A[q].x += v[q] * cs;
+                A[q].y -= v[q] * sn;
+            }
+        }
+        for (int q = 0; q < 6; q++) N.acc[((size_t)f * 6 + q) * ns + s] = A[q];
+    }
+    if (clear)
+        for (int j = 0; j < nslots; j++)
+            for (int q = 0; q < 9; q++) N.ring[((size_t)j * 9 + q) * ns + s] = 0.f;
+}
+
 __device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
 {
-    if (s >= N.ns) return;
     const int step = *N.step - 1;
+    if (s >= N.ns || step < 0) return;
+    const int slot = step % NFFF_RING;
     const int64_t c = N.cell[s];
     const int64_t st = N.nstride[s];
-    double v[6];
+    const size_t ns = (size_t)N.ns;
+    float *r = N.ring + (size_t)slot * 9 * ns + s;
     for (int a = 0; a < 3; a++) {
         const float *E = N.e[a];
-        v[a] = (double)ld_any(E, c, N.storage);
-        v[3 + a] = ((double)ld_any(E, c + st, N.storage) - (double)ld_any(E, c - st, N.storage)) * N.inv2dx;
+        r[(3 * a) * ns] = ld_any(E, c, N.storage);
+        r[(3 * a + 1) * ns] = ld_any(E, c + st, N.storage);
+        r[(3 * a + 2) * ns] = ld_any(E, c - st, N.storage);
     }
-    for (int f = 0; f < N.nfreq; f++) {
-        double sn, cs;
-        sincos(N.omega_dt[f] * (double)step, &sn, &cs);
-        for (int q = 0; q < 6; q++) {
-            double2 &A = N.acc[((size_t)f * 6 + q) * N.ns + s];
-            A.x += v[q] * cs;
-            A.y -= v[q] * sn;
-        }
-    }
+    if (slot == NFFF_RING - 1) nfff_fold(N, s, step - (NFFF_RING - 1), NFFF_RING, false);
+}
+
+// the steps since the last full block (device step counter % NFFF_RING); their
+// slots are cleared, so the fold at the end of the block adds zeros for them
+__global__ void nfff_fold_pending_kernel(const DevNfff N)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N.ns) return;
+    const int done = *N.step;
+    const int pending = done % NFFF_RING;
+    if (pending > 0) nfff_fold(N, s, done - pending, pending, true);
 }
 
 __global__ void nfff_accumulate_kernel(const DevNfff N) { nfff_accumulate_cell(N, blockIdx.x * blockDim.x + threadIdx.x); }
@@ -966,6 +1004,12 @@ void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st)
 {
     if (n.ns <= 0) return;
     nfff_accumulate_kernel<<<(n.ns + 255) / 256, 256, 0, st>>>(n);
+}
+
+void launch_nfff_fold_pending(const DevNfff &n, cudaStream_t st)
+{
+    if (n.ns <= 0 || n.nfreq <= 0) return;
+    nfff_fold_pending_kernel<<<(n.ns + 255) / 256, 256, 0, st>>>(n);
 }
 
 void launch_farfield_finalize(const DevFarfield &f, cudaStream_t st)

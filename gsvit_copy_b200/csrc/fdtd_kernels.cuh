@@ -25,6 +25,10 @@ struct DevAux {                 // 1D auxiliary grid of the TSF source (1dpool.c
     float ihs;                  // 1 / H storage scale
 };
 
+// steps of E samples buffered per surface cell before they are folded into
+// the FP64 accumulators (one accumulator read/write per NFFF_RING steps)
+constexpr int NFFF_RING = 8;
+
 struct DevNfff {
     int ns;                     // surface cells
     int nfreq;
@@ -32,6 +36,7 @@ struct DevNfff {
     const int32_t *nstride;     // +/- stride along the face normal
     const float *const *e;      // 3 E field pointers (the set written by this step)
     double2 *acc;               // [(f*6 + q)*ns + s], q = Ex,Ey,Ez, dEx,dEy,dEz
+    float *ring;                // NFFF_RING steps of raw samples [(slot*9 + 3a + r)*ns + s], r: E(c), E(c+st), E(c-st)
     const double *omega_dt;     // nfreq
     const int *step;            // device step counter (already advanced)
     double inv2dx;
@@ -65,6 +70,9 @@ void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st);
 cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
                               long long nblocks4, bool ade, int npoles, int storage, cudaStream_t st);
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st);
+// folds the samples of the steps since the last multiple of NFFF_RING into the
+// accumulators and clears their ring slots; due before the accumulators are read
+void launch_nfff_fold_pending(const DevNfff &n, cudaStream_t st);
 
 struct DevFarfield {
     int npoints, nfreq, ns;
