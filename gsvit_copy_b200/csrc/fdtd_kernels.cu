@@ -696,7 +696,22 @@ __global__ void probe_capture_kernel(const DevAux A)
 // accumulators in step order, with the arithmetic of a per-step update, so the
 // sums are those of accumulating every step (the accumulators are read and
 // written once per NFFF_RING steps instead of every step).
-__device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_step, int nslots, bool clear)
+constexpr int NFFF_TW_MAXF = 16;   // frequencies whose twiddles a CTA tabulates in shared memory
+
+// exp(-i omega_f (first_step + j) dt) of the block's steps, computed once per
+// CTA: tw[f * nslots + j] = (cos, sin).  All threads of the CTA take part.
+__device__ __forceinline__ void nfff_twiddles(const DevNfff &N, int first_step, int nslots, double2 *tw)
+{
+    for (int t = threadIdx.x; t < nslots * N.nfreq; t += blockDim.x) {
+        double sn, cs;
+        sincos(N.omega_dt[t / nslots] * (double)(first_step + t % nslots), &sn, &cs);
+        tw[t] = make_double2(cs, sn);
+    }
+    __syncthreads();
+}
+
+// tw: the CTA's twiddle table, or nullptr to evaluate them per cell
+__device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_step, int nslots, bool clear, const double2 *tw)
 {
     const size_t ns = (size_t)N.ns;
     for (int f = 0; f < N.nfreq; f++) {
@@ -710,7 +725,8 @@ __device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_ste
                 v[3 + a] = ((double)r[(3 * a + 1) * ns] - (double)r[(3 * a + 2) * ns]) * N.inv2dx;
             }
             double sn, cs;
-            sincos(N.omega_dt[f] * (double)(first_step + j), &sn, &cs);
+            if (tw) { cs = tw[f * nslots + j].x; sn = tw[f * nslots + j].y; }
+            else sincos(N.omega_dt[f] * (double)(first_step + j), &sn, &cs);
             for (int q = 0; q < 6; q++) {
                 A[q].x += v[q] * cs;
                 A[q].y -= v[q] * sn;
@@ -723,22 +739,34 @@ __device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_ste
             for (int q = 0; q < 9; q++) N.ring[((size_t)j * 9 + q) * ns + s] = 0.f;
 }
 
+// the step counter, the slot and the fold decision are the same for every
+// thread of a launch (one plan per CTA in a batch), so the CTA-wide twiddle
+// table and its barrier are reached by all threads
 __device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
 {
+    if (N.ns <= 0 || N.nfreq <= 0) return;   // a batch instance without a running DFT: zeroed, no step counter
     const int step = *N.step - 1;
-    if (s >= N.ns || step < 0) return;
+    if (step < 0) return;
+    const bool live = s < N.ns;
     const int slot = step % NFFF_RING;
-    const int64_t c = N.cell[s];
-    const int64_t st = N.nstride[s];
     const size_t ns = (size_t)N.ns;
-    float *r = N.ring + (size_t)slot * 9 * ns + s;
-    for (int a = 0; a < 3; a++) {
-        const float *E = N.e[a];
-        r[(3 * a) * ns] = ld_any(E, c, N.storage);
-        r[(3 * a + 1) * ns] = ld_any(E, c + st, N.storage);
-        r[(3 * a + 2) * ns] = ld_any(E, c - st, N.storage);
+    if (live) {
+        const int64_t c = N.cell[s];
+        const int64_t st = N.nstride[s];
+        float *r = N.ring + (size_t)slot * 9 * ns + s;
+        for (int a = 0; a < 3; a++) {
+            const float *E = N.e[a];
+            r[(3 * a) * ns] = ld_any(E, c, N.storage);
+            r[(3 * a + 1) * ns] = ld_any(E, c + st, N.storage);
+            r[(3 * a + 2) * ns] = ld_any(E, c - st, N.storage);
+        }
     }
-    if (slot == NFFF_RING - 1) nfff_fold(N, s, step - (NFFF_RING - 1), NFFF_RING, false);
+    if (slot == NFFF_RING - 1) {
+        __shared__ double2 tw[NFFF_RING * NFFF_TW_MAXF];
+        const bool table = N.nfreq <= NFFF_TW_MAXF;
+        if (table) nfff_twiddles(N, step - (NFFF_RING - 1), NFFF_RING, tw);
+        if (live) nfff_fold(N, s, step - (NFFF_RING - 1), NFFF_RING, false, table ? tw : nullptr);
+    }
 }
 
 // the steps since the last full block (device step counter % NFFF_RING); their
@@ -746,10 +774,14 @@ __device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
 __global__ void nfff_fold_pending_kernel(const DevNfff N)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= N.ns) return;
+    if (N.ns <= 0 || N.nfreq <= 0) return;
     const int done = *N.step;
     const int pending = done % NFFF_RING;
-    if (pending > 0) nfff_fold(N, s, done - pending, pending, true);
+    if (pending == 0) return;
+    __shared__ double2 tw[NFFF_RING * NFFF_TW_MAXF];
+    const bool table = N.nfreq <= NFFF_TW_MAXF;
+    if (table) nfff_twiddles(N, done - pending, pending, tw);
+    if (s < N.ns) nfff_fold(N, s, done - pending, pending, true, table ? tw : nullptr);
 }
 
 __global__ void nfff_accumulate_kernel(const DevNfff N) { nfff_accumulate_cell(N, blockIdx.x * blockDim.x + threadIdx.x); }
