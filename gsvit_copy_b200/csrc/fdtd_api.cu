@@ -101,6 +101,7 @@ struct fdtd_plan {
     long long nslab_blocks = 0;
     SlabBox *d_boxes4 = nullptr;    // the same numbered in 4-cell groups (H kernel), when all are 4-aligned
     long long nslab_blocks4 = 0;
+    SlabLists slabs{};              // the lists above plus the E split (runs with / without dispersive cells)
     BulkItem *d_bulk = nullptr;
     int nbulk = 0;
     bool bulk_on = false;
@@ -157,7 +158,7 @@ int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
         e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
     }
-    e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->d_boxes4, P->nslab_blocks4, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
+    e = launch_slab_steps(d, P->slabs, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
     if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
     return FDTD_OK;
 }
@@ -716,6 +717,68 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         P->h_bulk = blk;
         P->nboxes = (int)boxes.size();
         P->nslab_blocks = nblk;
+        {   // E lists: each box split along k into runs of planes that hold a
+            // dispersive cell and runs that hold none; plain runs shorter than
+            // 8 planes stay with the dispersive list (its kernel handles plain
+            // cells the same way), so the split adds few boxes
+            std::vector<SlabBox> eb, pb;
+            long long neb = 0, npb = 0;
+            auto push = [&](const SlabBox &b0, int k0, int k1, bool disp) {
+                SlabBox b = b0;
+                b.k0 = k0;
+                b.k1 = k1;
+                long long &n = disp ? neb : npb;
+                b.first_block = n;
+                n += ((long long)(b.i1 - b.i0) * (b.j1 - b.j0) * (k1 - k0) + 255) / 256;
+                (disp ? eb : pb).push_back(b);
+            };
+            for (const SlabBox &b : boxes) {
+                if (!hp.has_ade) { push(b, b.k0, b.k1, true); continue; }
+                std::vector<char> dk(b.k1 - b.k0, 0);
+#pragma omp parallel for schedule(static)
+                for (int k = b.k0; k < b.k1; k++) {
+                    char any = 0;
+                    for (int i = b.i0; i < b.i1 && !any; i++)
+                        for (int j = b.j0; j < b.j1; j++)
+                            if (hp.classes[hp.cls[((size_t)i * Y + j) * Z + k]].flags & CF_ADE_BRANCH) { any = 1; break; }
+                    dk[k - b.k0] = any;
+                }
+                for (int k = b.k0; k < b.k1;) {   // short plain runs count as dispersive
+                    int e = k;
+                    while (e < b.k1 && dk[e - b.k0] == dk[k - b.k0]) e++;
+                    if (!dk[k - b.k0] && e - k < 8)
+                        for (int q = k; q < e; q++) dk[q - b.k0] = 1;
+                    k = e;
+                }
+                for (int k = b.k0; k < b.k1;) {
+                    int e = k;
+                    while (e < b.k1 && dk[e - b.k0] == dk[k - b.k0]) e++;
+                    push(b, k, e, dk[k - b.k0] != 0);
+                    k = e;
+                }
+            }
+            SlabLists &L = P->slabs;
+            L.h = P->d_boxes;
+            L.nh = P->nboxes;
+            L.hblocks = nblk;
+            L.h4 = P->d_boxes4;
+            L.h4blocks = P->nslab_blocks4;
+            if (pb.empty()) {
+                L.e = P->d_boxes;
+                L.ne = P->nboxes;
+                L.eblocks = nblk;
+            } else {
+                SlabBox *de = nullptr, *dp = nullptr;
+                if (!eb.empty()) CA(upload(P->mem, &de, eb.data(), eb.size()), "slab boxes");
+                CA(upload(P->mem, &dp, pb.data(), pb.size()), "slab boxes");
+                L.e = de;
+                L.ne = (int)eb.size();
+                L.eblocks = neb;
+                L.ep = dp;
+                L.nep = (int)pb.size();
+                L.epblocks = npb;
+            }
+        }
         CA(P->mem.alloc(&P->d_err, 1), "error word");
         if (P->bulk_on) {
             CA(upload(P->mem, &P->d_bulk, blk.data(), blk.size()), "work table");
@@ -1112,7 +1175,7 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
             if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
         }
         CK(cudaEventRecord(E[2], st));
-        cudaError_t e = launch_slab_steps(d, P->d_boxes, P->nboxes, P->nslab_blocks, P->d_boxes4, P->nslab_blocks4, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
+        cudaError_t e = launch_slab_steps(d, P->slabs, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
         CK(cudaEventRecord(E[3], st));
         launch_nfff(P, in, st);

@@ -962,30 +962,30 @@ void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st)
 }
 
 template <class T>
-cudaError_t slab_steps_t(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
-                         long long nblocks4, bool ade, int npoles, cudaStream_t st)
+cudaError_t slab_steps_t(const DevPlan &p, const SlabLists &L, bool ade, int npoles, cudaStream_t st)
 {
-    if (nblocks4 > 0)
-        slab_h4_kernel<T><<<(unsigned)nblocks4, 256, 0, st>>>(p, boxes4, nboxes);
+    if (L.h4blocks > 0)
+        slab_h4_kernel<T><<<(unsigned)L.h4blocks, 256, 0, st>>>(p, L.h4, L.nh);
     else
-        slab_h_kernel<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    if (!ade)
-        slab_e_kernel<false, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    else if (npoles == 0)
-        slab_e_kernel<true, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    else
-        slab_e_kernel<true, 2, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+        slab_h_kernel<T><<<(unsigned)L.hblocks, 256, 0, st>>>(p, L.h, L.nh);
+    if (L.eblocks > 0) {
+        if (!ade)
+            slab_e_kernel<false, 0, T><<<(unsigned)L.eblocks, 256, 0, st>>>(p, L.e, L.ne);
+        else if (npoles == 0)
+            slab_e_kernel<true, 0, T><<<(unsigned)L.eblocks, 256, 0, st>>>(p, L.e, L.ne);
+        else
+            slab_e_kernel<true, 2, T><<<(unsigned)L.eblocks, 256, 0, st>>>(p, L.e, L.ne);
+    }
+    if (L.epblocks > 0) slab_e_kernel<false, 0, T><<<(unsigned)L.epblocks, 256, 0, st>>>(p, L.ep, L.nep);
     return cudaGetLastError();
 }
 
-cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
-                              long long nblocks4, bool ade, int npoles, int storage, cudaStream_t st)
+cudaError_t launch_slab_steps(const DevPlan &p, const SlabLists &L, bool ade, int npoles, int storage, cudaStream_t st)
 {
-    if (nblocks <= 0) return cudaSuccess;
-    if (storage == FDTD_STORE_F16) return slab_steps_t<__half>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
-    if (storage == FDTD_STORE_BF16)
-        return slab_steps_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
-    return slab_steps_t<float>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
+    if (L.hblocks <= 0) return cudaSuccess;
+    if (storage == FDTD_STORE_F16) return slab_steps_t<__half>(p, L, ade, npoles, st);
+    if (storage == FDTD_STORE_BF16) return slab_steps_t<__nv_bfloat16>(p, L, ade, npoles, st);
+    return slab_steps_t<float>(p, L, ade, npoles, st);
 }
 
 void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st)

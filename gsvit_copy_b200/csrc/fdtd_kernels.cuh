@@ -65,10 +65,25 @@ cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int 
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st);
 void launch_probe_capture(const DevAux &a, cudaStream_t st);
 void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st);
-// boxes4 / nblocks4: the same boxes numbered in 4-cell groups (every k bound
-// and the row length multiples of 4); nblocks4 = 0 runs H one cell per thread
-cudaError_t launch_slab_steps(const DevPlan &p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
-                              long long nblocks4, bool ade, int npoles, int storage, cudaStream_t st);
+// The slab work lists of a plan.  H runs over every slab box, in 4-cell
+// groups when h4blocks > 0 (every k bound and the row length multiples of 4).
+// E runs over the same cells split along k: `e` holds the runs of k planes
+// with a dispersive cell (the plan's E variant), `ep` the runs without one
+// (the plain E variant, fewer registers); without a split `e` is every box.
+struct SlabLists {
+    const SlabBox *h;
+    int nh;
+    long long hblocks;
+    const SlabBox *h4;
+    long long h4blocks;
+    const SlabBox *e;
+    int ne;
+    long long eblocks;
+    const SlabBox *ep;
+    int nep;
+    long long epblocks;
+};
+cudaError_t launch_slab_steps(const DevPlan &p, const SlabLists &L, bool ade, int npoles, int storage, cudaStream_t st);
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st);
 // folds the samples of the steps since the last multiple of NFFF_RING into the
 // accumulators and clears their ring slots; due before the accumulators are read
