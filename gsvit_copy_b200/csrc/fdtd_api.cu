@@ -109,6 +109,8 @@ struct fdtd_plan {
     int *d_err = nullptr;
     int region[6] = {0, 0, 0, 0, 0, 0};   // bulk box Xlo Xhi Ylo Yhi Zlo Zhi
     std::vector<SlabBox> h_boxes;         // host copies of the work lists (batched launches)
+    std::vector<SlabBox> h_eboxes;        // E runs with a dispersive cell (every box when unsplit)
+    std::vector<SlabBox> h_epboxes;       // E runs without one
     std::vector<BulkItem> h_bulk;
     int bulk_len = 0;                     // planes per bulk item
     int tsf_cells = 0;                    // face cells of the TSF correction tables
@@ -757,6 +759,8 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
                     k = e;
                 }
             }
+            P->h_eboxes = pb.empty() ? boxes : eb;
+            P->h_epboxes = pb;
             SlabLists &L = P->slabs;
             L.h = P->d_boxes;
             L.nh = P->nboxes;
@@ -1372,6 +1376,12 @@ struct fdtd_batch {
     int nboxes[3] = {0, 0, 0};
     long long nslab_blocks[3] = {0, 0, 0};
     long long nslab_blocks4[3] = {0, 0, 0};
+    SlabBox *d_eboxes[3] = {nullptr, nullptr, nullptr};   // E: the instances' dispersive runs, per variant
+    int neboxes[3] = {0, 0, 0};
+    long long neblocks[3] = {0, 0, 0};
+    SlabBox *d_epboxes = nullptr;                         // E: every instance's plain runs, one launch
+    int nepboxes = 0;
+    long long nepblocks = 0;
     int max_tsf = 0, max_nfff = 0;
     int *d_err = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -1439,7 +1449,12 @@ int batch_launch_step(fdtd_batch *B, cudaStream_t st)
                                           B->d_err, ade, npoles, B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched bulk launch: ") + cudaGetErrorString(e));
         e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], B->d_boxes4[g],
-                                    B->nslab_blocks4[g], ade, npoles, B->storage, st);
+                                    B->nslab_blocks4[g], B->d_eboxes[g], B->neboxes[g], B->neblocks[g], ade, npoles,
+                                    B->storage, st);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
+    }
+    {   // E of every instance's plain runs (after all H half steps)
+        cudaError_t e = launch_slab_e_plain_batch(B->d_plans[in], B->d_epboxes, B->nepboxes, B->nepblocks, B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
     }
     if (B->max_nfff) launch_nfff_accumulate_batch(B->d_nfff[in], n, B->max_nfff, st);
@@ -1538,6 +1553,20 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
         if (B->nslab_blocks[g] > 0x7fffffffLL) { fail(FDTD_E_UNSUPPORTED, "too many slab cells for one launch"); return bail(FDTD_E_UNSUPPORTED); }
         BA(upload(B->mem, &B->d_boxes[g], boxes.data(), boxes.size()), "batch slab boxes");
         B->nboxes[g] = (int)boxes.size();
+        // E runs with a dispersive cell, numbered for this variant's launch
+        std::vector<SlabBox> ebx;
+        for (int q = 0; q < nplans; q++) {
+            if (B->group[q] != g) continue;
+            for (SlabBox b : B->plans[q]->h_eboxes) {
+                b.first_block = B->neblocks[g];
+                b.inst = q;
+                ebx.push_back(b);
+                B->neblocks[g] += ((long long)(b.i1 - b.i0) * (b.j1 - b.j0) * (b.k1 - b.k0) + 255) / 256;
+            }
+        }
+        if (B->neblocks[g] > 0x7fffffffLL) { fail(FDTD_E_UNSUPPORTED, "too many slab cells for one launch"); return bail(FDTD_E_UNSUPPORTED); }
+        if (!ebx.empty()) BA(upload(B->mem, &B->d_eboxes[g], ebx.data(), ebx.size()), "batch slab boxes");
+        B->neboxes[g] = (int)ebx.size();
         bool w4 = !boxes.empty();
         for (auto &b : boxes) w4 = w4 && B->plans[b.inst]->hp.zr % 4 == 0 && b.k0 % 4 == 0 && b.k1 % 4 == 0;
         if (w4) {
@@ -1547,6 +1576,19 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
             }
             BA(upload(B->mem, &B->d_boxes4[g], boxes.data(), boxes.size()), "batch slab boxes");
         }
+    }
+    {   // E runs without a dispersive cell, every instance in one launch
+        std::vector<SlabBox> pbx;
+        for (int q = 0; q < nplans; q++)
+            for (SlabBox b : B->plans[q]->h_epboxes) {
+                b.first_block = B->nepblocks;
+                b.inst = q;
+                pbx.push_back(b);
+                B->nepblocks += ((long long)(b.i1 - b.i0) * (b.j1 - b.j0) * (b.k1 - b.k0) + 255) / 256;
+            }
+        if (B->nepblocks > 0x7fffffffLL) { fail(FDTD_E_UNSUPPORTED, "too many slab cells for one launch"); return bail(FDTD_E_UNSUPPORTED); }
+        if (!pbx.empty()) BA(upload(B->mem, &B->d_epboxes, pbx.data(), pbx.size()), "batch slab boxes");
+        B->nepboxes = (int)pbx.size();
     }
     BA(B->mem.alloc(&B->d_err, 1), "error word");
     BA(batch_set_items(B, 0, true), "batch work list");

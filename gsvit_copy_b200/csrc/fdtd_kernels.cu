@@ -1000,31 +1000,48 @@ void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStr
 
 template <class T>
 cudaError_t slab_steps_batch_t(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
-                               long long nblocks4, bool ade, int npoles, cudaStream_t st)
+                               long long nblocks4, const SlabBox *eboxes, int neboxes, long long neblocks, bool ade,
+                               int npoles, cudaStream_t st)
 {
     if (nblocks4 > 0)
         slab_h4_batch<T><<<(unsigned)nblocks4, 256, 0, st>>>(p, boxes4, nboxes);
     else
         slab_h_batch<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    if (!ade)
-        slab_e_batch<false, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    else if (npoles == 0)
-        slab_e_batch<true, 0, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    else
-        slab_e_batch<true, 2, T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    if (neblocks > 0) {
+        if (!ade)
+            slab_e_batch<false, 0, T><<<(unsigned)neblocks, 256, 0, st>>>(p, eboxes, neboxes);
+        else if (npoles == 0)
+            slab_e_batch<true, 0, T><<<(unsigned)neblocks, 256, 0, st>>>(p, eboxes, neboxes);
+        else
+            slab_e_batch<true, 2, T><<<(unsigned)neblocks, 256, 0, st>>>(p, eboxes, neboxes);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks,
-                                    const SlabBox *boxes4, long long nblocks4, bool ade, int npoles, int storage,
-                                    cudaStream_t st)
+                                    const SlabBox *boxes4, long long nblocks4, const SlabBox *eboxes, int neboxes,
+                                    long long neblocks, bool ade, int npoles, int storage, cudaStream_t st)
 {
     if (nblocks <= 0) return cudaSuccess;
     if (storage == FDTD_STORE_F16)
-        return slab_steps_batch_t<__half>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
+        return slab_steps_batch_t<__half>(p, boxes, nboxes, nblocks, boxes4, nblocks4, eboxes, neboxes, neblocks, ade, npoles, st);
     if (storage == FDTD_STORE_BF16)
-        return slab_steps_batch_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
-    return slab_steps_batch_t<float>(p, boxes, nboxes, nblocks, boxes4, nblocks4, ade, npoles, st);
+        return slab_steps_batch_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, boxes4, nblocks4, eboxes, neboxes, neblocks, ade,
+                                                 npoles, st);
+    return slab_steps_batch_t<float>(p, boxes, nboxes, nblocks, boxes4, nblocks4, eboxes, neboxes, neblocks, ade, npoles, st);
+}
+
+cudaError_t launch_slab_e_plain_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, int storage,
+                                      cudaStream_t st)
+{
+    if (nblocks <= 0) return cudaSuccess;
+    if (storage == FDTD_STORE_F16)
+        slab_e_batch<false, 0, __half><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    else if (storage == FDTD_STORE_BF16)
+        slab_e_batch<false, 0, __nv_bfloat16><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    else
+        slab_e_batch<false, 0, float><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    return cudaGetLastError();
 }
 
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st)

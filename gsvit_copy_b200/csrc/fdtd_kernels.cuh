@@ -58,10 +58,14 @@ void launch_aux_step(const DevAux &a, cudaStream_t st);
 // device tables (of this step's parity), indexed by the plan number.
 void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st);
 void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStream_t st);
-// boxes4 / nblocks4 as for launch_slab_steps, over every instance of the batch
+// H over boxes (or boxes4 in 4-cell groups, nblocks4 > 0) and E over eboxes,
+// the instances' runs of k planes with a dispersive cell (SlabLists::e)
 cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks,
-                                    const SlabBox *boxes4, long long nblocks4, bool ade, int npoles, int storage,
-                                    cudaStream_t st);
+                                    const SlabBox *boxes4, long long nblocks4, const SlabBox *eboxes, int neboxes,
+                                    long long neblocks, bool ade, int npoles, int storage, cudaStream_t st);
+// E over every instance's runs without a dispersive cell (SlabLists::ep)
+cudaError_t launch_slab_e_plain_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, int storage,
+                                      cudaStream_t st);
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st);
 void launch_probe_capture(const DevAux &a, cudaStream_t st);
 void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st);
