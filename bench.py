@@ -317,7 +317,8 @@ def run_b200(a):
     ff_ms = (time.perf_counter() - t0) * 1e3
     step_bytes = g.step_bytes()
     step_gbs = step_bytes / (ms / K * 1e-3) / 1e9
-    gpu_launches = int(prof["launches_per_step"]) * K
+    # the step kernels of K steps, then the probe capture that closes fdtd_step
+    gpu_launches = int(prof["launches_per_step"]) * K + (1 if scene.probes is not None and len(scene.probes) else 0)
 
     # end to end through the public API with pinned host buffers
     shape = g.shape

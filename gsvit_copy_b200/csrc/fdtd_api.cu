@@ -1208,7 +1208,9 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
     out[4] = aux;
     out[5] = nf;
     out[6] = tot;
-    out[7] = 1 + (P->tsf_cells ? 1 : 0) + (P->bulk_on ? 1 : 0) + 2 + (P->nfff_nfreq > 0 ? 1 : 0) + (P->nfff_series ? 1 : 0);
+    const SlabLists &L = P->slabs;   // slab H, then E over the dispersive and the plain runs
+    const int nslab = L.hblocks > 0 ? 1 + (L.eblocks > 0 ? 1 : 0) + (L.epblocks > 0 ? 1 : 0) : 0;
+    out[7] = 1 + (P->tsf_cells ? 1 : 0) + (P->bulk_on ? 1 : 0) + nslab + (P->nfff_nfreq > 0 ? 1 : 0) + (P->nfff_series ? 1 : 0);
     return FDTD_OK;
 }
 
