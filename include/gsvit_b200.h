@@ -356,7 +356,8 @@ int fdtd_batch_config(const fdtd_batch *batch, int *planes_per_item, int *persis
 /* ---- checkpoint (forward snapshots) ---------------------------------------- */
 
 /* Bytes needed for one snapshot of the complete stepping state (fields, CPML
- * psi slabs, ADE state, 1D aux grid, NFFF accumulators, step counter). */
+ * psi slabs, ADE state, 1D aux grid, NFFF accumulators and the up to 8 steps
+ * of surface samples not yet folded into them, step counter). */
 int fdtd_snapshot_size(const fdtd_plan *plan, size_t *bytes);
 /* Save / restore the state into / from a caller buffer (host memory). */
 int fdtd_snapshot_save(fdtd_plan *plan, void *host_buf, size_t bytes);
