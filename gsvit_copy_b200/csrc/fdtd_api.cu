@@ -95,8 +95,8 @@ struct fdtd_plan {
     const float **d_fieldptrs[2] = {nullptr, nullptr};   // device copies of fields[s]
     int *d_step = nullptr;
     int host_step = 0;
-    // work decomposition: general kernel (CPML slabs, grid edges) and TMA bulk kernel
-    SlabBox *d_boxes = nullptr;     // slab boxes (one thread per cell)
+    // work decomposition: slab kernels (CPML slabs, grid edges) and TMA bulk kernel
+    SlabBox *d_boxes = nullptr;     // slab boxes (numbered one cell per thread)
     int nboxes = 0;
     long long nslab_blocks = 0;
     SlabBox *d_boxes4 = nullptr;    // the same numbered in 4-cell groups (H kernel), when all are 4-aligned
@@ -621,7 +621,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     // plane on the low sides so that its halo row/column/plane is slab-free,
     // off the grid's edge planes, k bounds multiples of 4) goes to the TMA
     // kernel when the k rows are 16-byte multiples; the rest (slabs, edge
-    // planes) to the general kernel
+    // planes) to the slab kernels
     {
         const int X = hp.xr, Y = hp.yr, Z = hp.zr;
         int lo[3], hi[3];
@@ -1540,7 +1540,7 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
         BA(upload(B->mem, &B->d_aux[in], ax.data(), ax.size()), "batch tables");
         BA(upload(B->mem, &B->d_nfff[in], nf.data(), nf.size()), "batch tables");
     }
-    // slab boxes of every instance, one thread per cell, per kernel variant
+    // slab boxes of every instance (numbered one cell per thread), per kernel variant
     for (int g = 0; g < 3; g++) {
         std::vector<SlabBox> boxes;
         for (int q = 0; q < nplans; q++) {

@@ -2,7 +2,7 @@
 //
 // The bulk region is every cell outside the CPML slabs and off the grid's
 // edge planes (their H/E updates, psi recursions and zeroed planes are done by
-// the general kernel).  Inside it a step is: ystep_h (yee.c:146-265) + TSF H
+// the slab kernels of fdtd_kernels.cu).  Inside it a step is: ystep_h (yee.c:146-265) + TSF H
 // (source.c:1464-1672), then ystep_e with the ADE branch and the PEC rule
 // (yee.c:530-1247) + TSF E (source.c:547-771).  kappa is 1 everywhere here and
 // no edge test of the reference applies.
@@ -19,7 +19,10 @@
 // planes through a 3-stage shared-memory ring with cp.async.bulk.tensor (TMA)
 // two planes ahead: E(p) box 17 rows, H(p) box 16 rows, class bytes 16 rows,
 // completion on one mbarrier per stage.  Every wait is bounded; a CTA that
-// gives up sets the error word and returns after draining its copies.
+// gives up sets the error word and returns after draining its copies.  The
+// dispersive state (Q, E^{n-1}; pole state) is read with plain global loads:
+// plane i's at the top of plane i, and plane i+1's lines are prefetched into
+// L2 at the same time for the components its staged class word marks.
 #include <cuda.h>
 #include <cuda_runtime.h>
 

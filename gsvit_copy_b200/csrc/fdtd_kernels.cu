@@ -13,7 +13,9 @@
 // updates one cell per thread: ystep_e with the ADE branch, its embedded CPML,
 // the ordinary update and the PEC rule (yee.c:530-1247), then e_special --
 // the CPML psi_E update and corrections (boundary.c:691-884) and the TSF E
-// corrections (source.c:547-771).  Each half step reads one field set and
+// corrections (source.c:547-771).  E runs over the runs of k planes that hold a
+// dispersive cell with the plan's variant and over the rest with the plain
+// variant (SlabLists).  Each half step reads one field set and
 // writes the other, so blocks never race on a shared cell.  The *_batch
 // forms take a per-box plan index and serve many plans in one launch.
 #include <cuda_runtime.h>

@@ -43,7 +43,8 @@ struct DevNfff {
     int storage;                // FDTD_STORE_* of the fields
 };
 
-// a box of cells handled one thread per cell; blocks [first_block, next box's first_block)
+// a box of cells; its blocks are [first_block, next box's first_block), one cell
+// (or one 4-cell group in a 4-cell list) per thread
 struct SlabBox {
     int i0, i1, j0, j1, k0, k1;
     long long first_block;
