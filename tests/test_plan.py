@@ -105,3 +105,50 @@ def test_electric_voxel_mode_oracle_vs_reference():
         assert np.array_equal(o.map(w), r.map(w))
     for a, b in zip(o.fields(), r.fields()):
         assert np.array_equal(a, b)
+
+
+def test_batch_scenes_follow_the_batched_workload():
+    """48 seeded instances: x, y in {64, 96, 128, 192}, z in {64, 96, 128},
+    8-cell CPML on every face, incidence 0-60 deg from +z, rms height 5-20 nm
+    (1-4 cells of 5 nm), Drude silver or the single-pole Lorentz substrate,
+    both present; the same seed gives the same instances."""
+    sc, again = plan.batch_scenes(48, nsteps=64), plan.batch_scenes(48, nsteps=64)
+    assert len(sc) == 48
+    kinds = set()
+    for s, t in zip(sc, again):
+        assert s.xres in (64, 96, 128, 192) and s.yres in (64, 96, 128, 192) and s.zres in (64, 96, 128)
+        assert all(s.cpml[f][0] == 8 for f in range(6))
+        assert 120.0 <= math.degrees(s.tsf["theta"]) <= 180.0
+        assert 1.0 - 1e-9 <= float(np.std(s.meta["height_map"])) <= 4.0 + 1e-9
+        m = s.mats[1]
+        if m.drude_omega_p > 0:
+            kinds.add("drude")
+            assert m.drude_omega_p == plan.f32(1.38e16) and m.drude_nu == plan.f32(2.73e13)
+        else:
+            kinds.add("lorentz")
+            a, _, big_omega, gamma = plan.lorentz_as_cp(5.0, 2.0, 4e15, 1e14)
+            assert m.cp_omega[0] == plan.f32(big_omega) and m.cp_gamma[0] == plan.f32(gamma)
+            assert m.cp_a[0] == plan.f32(a) and m.cp_a[1] == 0.0
+        assert (s.xres, s.yres, s.zres) == (t.xres, t.yres, t.zres)
+        assert np.array_equal(s.mat, t.mat)
+    assert kinds == {"drude", "lorentz"}
+
+
+def test_cone_objective_weights_cover_the_cone():
+    """The appended far points lie within the cone (10 deg about theta = 20
+    deg, up to the integer rounding of a point 640 cells out), the objective
+    indexes exactly them, istart covers every point, and the weights
+    sin(theta) dtheta dphi sum to the cone's solid angle 2 pi (1 - cos 10 deg)
+    within the quadrature error of the grid."""
+    for nth, nph, tol in ((9, 13, 0.02), (41, 61, 0.01)):
+        s = plan.rough_surface_scene(res=64, nsteps=10, nfff_angles=(4, 7))
+        n0 = len(s.nfff["points"])
+        obj = plan.cone_objective(s, nth=nth, nph=nph)
+        assert np.array_equal(obj["points"], np.arange(n0, len(s.nfff["points"])))
+        assert len(s.nfff["istart"]) == len(s.nfff["points"])
+        d = s.nfff["points"][obj["points"]] - np.array([32, 32, 32])
+        d = d / np.linalg.norm(d, axis=1)[:, None]
+        axis = np.array([math.sin(math.radians(20)), 0.0, math.cos(math.radians(20))])
+        assert np.degrees(np.arccos(np.clip(d @ axis, -1, 1))).max() < 10.05
+        cone = 2 * math.pi * (1 - math.cos(math.radians(10)))
+        assert abs(obj["weights"].sum() / cone - 1) < tol
