@@ -1,0 +1,28 @@
+// host_plan_probe.cpp -- test infrastructure: a C entry point over the
+// library's host planner (gsvit_copy_b200/csrc/plan_host.cpp), built with g++
+// by tests/test_host_plan.py, so that the CPU suite checks the planner's
+// integer maps and coefficient classes without a GPU.  Not part of the library.
+#include <cstdio>
+#include <string>
+
+#include "../gsvit_copy_b200/csrc/plan_host.h"
+
+// which: FDTD_MAP_BNDS, FDTD_MAP_SOURCESKIP or FDTD_MAP_CLASS (per-cell class
+// index); *nclasses receives the number of coefficient classes.  Returns 0, the
+// planner's status, or -1 when out_len is short; err receives its message.
+extern "C" int host_plan_map(const fdtd_desc *d, int which, int32_t *out, size_t out_len, int *nclasses, char *err,
+                             size_t err_len)
+{
+    HostPlan hp;
+    std::string e;
+    const int rc = build_host_plan(d, &hp, &e);
+    if (rc != 0) {
+        std::snprintf(err, err_len, "%s", e.c_str());
+        return rc;
+    }
+    if (out_len < hp.n) return -1;
+    for (size_t c = 0; c < hp.n; c++)
+        out[c] = which == FDTD_MAP_BNDS ? hp.bnds[c] : which == FDTD_MAP_SOURCESKIP ? hp.sskip[c] : hp.cls[c];
+    *nclasses = (int)hp.classes.size();
+    return 0;
+}
