@@ -3,6 +3,7 @@
 // by tests/test_host_plan.py, so that the CPU suite checks the planner's
 // integer maps and coefficient classes without a GPU.  Not part of the library.
 #include <cstdio>
+#include <cstring>
 #include <string>
 
 #include "../gsvit_copy_b200/csrc/plan_host.h"
@@ -25,4 +26,22 @@ extern "C" int host_plan_map(const fdtd_desc *d, int which, int32_t *out, size_t
         out[c] = which == FDTD_MAP_BNDS ? hp.bnds[c] : which == FDTD_MAP_SOURCESKIP ? hp.sskip[c] : hp.cls[c];
     *nclasses = (int)hp.classes.size();
     return 0;
+}
+
+// The planner's coefficient class table: up to max_classes DevClass records
+// (64 bytes each, layout of fdtd_internal.h) into out; returns the number of
+// classes, or a negative status.
+extern "C" int host_plan_classes(const fdtd_desc *d, void *out, int max_classes, char *err, size_t err_len)
+{
+    HostPlan hp;
+    std::string e;
+    const int rc = build_host_plan(d, &hp, &e);
+    if (rc != 0) {
+        std::snprintf(err, err_len, "%s", e.c_str());
+        return rc < 0 ? rc : -rc;
+    }
+    const int n = (int)hp.classes.size();
+    if (n > max_classes) return -1;
+    std::memcpy(out, hp.classes.data(), sizeof(DevClass) * n);
+    return n;
 }

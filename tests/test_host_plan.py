@@ -2,9 +2,14 @@
 
 The planner is plain C++; tests/host_plan_probe.cpp puts a C entry point over
 it, and this file compiles both with g++ into pytest's temporary directory.
-The integer maps GSvit derives before its loop -- `bnds` (plan.c:5387-5416)
-and `sourceskip` (plan.c:5298-5326) -- must equal the oracle's bit for bit;
-the per-cell coefficient classes must index the planner's class table."""
+- The integer maps GSvit derives before its loop -- `bnds`
+  (plan.c:5387-5416) and `sourceskip` (plan.c:5298-5326) -- equal the
+  oracle's bit for bit.
+- The per-cell coefficient classes index the planner's class table, and each
+  cell's FP32 coefficients are the oracle's FP64 ones rounded to FP32: the H
+  update da, db (yee.c:219-243), the ordinary E update ca, cb after get_cabs
+  averaging (yee.c:1397-1493) where get_tbc keeps it, the dispersive-branch
+  selection per component and the PEC zeroing rule (yee.c:1138-1237)."""
 import ctypes as C
 import os
 import shutil
@@ -32,6 +37,8 @@ def probe(tmp_path_factory):
     lib.host_plan_map.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.c_char_p,
                                   C.c_size_t]
     lib.host_plan_map.restype = C.c_int
+    lib.host_plan_classes.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]
+    lib.host_plan_classes.restype = C.c_int
     return lib
 
 
@@ -72,3 +79,39 @@ def test_planner_classes_index_the_table(probe, name):
     assert 1 <= ncls <= 256
     assert cls.min() >= 0 and cls.max() < ncls
     assert len(np.unique(cls)) == ncls      # every class of the table is used by some cell
+
+
+# DevClass (gsvit_copy_b200/csrc/fdtd_internal.h), 64 bytes
+DEV_CLASS = np.dtype([("ca", "<f4", 3), ("flags", "<u4"), ("cb", "<f4", 3), ("tsfe", "<f4"), ("da", "<f4"),
+                      ("db", "<f4"), ("ade", "<i4"), ("pad0", "<f4"), ("cba", "<f4", 3), ("pad1", "<f4")])
+CF_ADE_BRANCH, CF_PEC_SHIFT = 0x8, 4
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_planner_coefficients_are_the_oracle_rounded_to_fp32(probe, name):
+    from oracle import adjoint as A
+    assert DEV_CLASS.itemsize == 64
+    s = SCENES[name]()
+    cls, ncls = _map(probe, s, abi.MAP_CLASS)
+    desc, keep = s.desc()
+    table = np.zeros(256, dtype=DEV_CLASS)
+    err = C.create_string_buffer(512)
+    assert probe.host_plan_classes(C.addressof(desc), table.ctypes.data, 256, err, len(err)) == ncls
+    per_cell = table[:ncls][cls.ravel()]
+    o = CpuSolver(s)
+    n = cls.size
+    ca, cb, da, db = np.zeros(3 * n), np.zeros(3 * n), np.zeros(n), np.zeros(n)
+    fl = np.zeros(n, dtype=np.int32)
+    assert A._lib().oracle_get_coeffs(o.h, A._p(ca), A._p(cb), A._p(da), A._p(db), fl.ctypes.data_as(A._ip)) == 0
+    o.close()
+    f32 = lambda x: x.astype(np.float32)
+    assert np.array_equal(per_cell["da"], f32(da)) and np.array_equal(per_cell["db"], f32(db))
+    flags = per_cell["flags"]
+    branch = (fl & 64) != 0                             # the cell takes the dispersive branch
+    assert np.array_equal((flags & CF_ADE_BRANCH) != 0, branch)
+    for a in range(3):
+        ordinary = ((fl >> a) & 1) == 1                 # get_tbc keeps the ordinary update of component a
+        assert np.array_equal(per_cell["ca"][:, a][ordinary], f32(ca[a * n:(a + 1) * n])[ordinary])
+        assert np.array_equal(per_cell["cb"][:, a][ordinary], f32(cb[a * n:(a + 1) * n])[ordinary])
+        assert np.array_equal(((flags >> a) & 1) == 1, ~ordinary & branch)
+        assert np.array_equal(((flags >> (CF_PEC_SHIFT + a)) & 1) == 1, ((fl >> (3 + a)) & 1) == 1)
