@@ -45,3 +45,26 @@ extern "C" int host_plan_classes(const fdtd_desc *d, void *out, int max_classes,
     std::memcpy(out, hp.classes.data(), sizeof(DevClass) * n);
     return n;
 }
+
+// CPML profiles of one face (0..5: x0 xn y0 yn z0 zn) as the planner holds
+// them: be, ce, bh, ch (FP32) and kappa_e, kappa_h (FP64), `cap` entries at
+// most each; returns the face depth (0 for a disabled face) or a negative status.
+extern "C" int host_plan_cpml(const fdtd_desc *d, int face, float *be, float *ce, float *bh, float *ch, double *ke,
+                              double *kh, int cap)
+{
+    HostPlan hp;
+    std::string e;
+    if (build_host_plan(d, &hp, &e) != 0 || face < 0 || face > 5) return -1;
+    if (!hp.cp[face].enabled) return 0;
+    const int n = (int)hp.be[face].size();
+    if (n > cap) return -1;
+    for (int q = 0; q < n; q++) {
+        be[q] = hp.be[face][q];
+        ce[q] = hp.ce[face][q];
+        bh[q] = hp.bh[face][q];
+        ch[q] = hp.ch[face][q];
+        ke[q] = q < (int)hp.ke[face].size() ? hp.ke[face][q] : 0.0;
+        kh[q] = q < (int)hp.kh[face].size() ? hp.kh[face][q] : 0.0;
+    }
+    return n;
+}

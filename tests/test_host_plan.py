@@ -9,7 +9,9 @@ it, and this file compiles both with g++ into pytest's temporary directory.
   cell's FP32 coefficients are the oracle's FP64 ones rounded to FP32: the H
   update da, db (yee.c:219-243), the ordinary E update ca, cb after get_cabs
   averaging (yee.c:1397-1493) where get_tbc keeps it, the dispersive-branch
-  selection per component and the PEC zeroing rule (yee.c:1138-1237)."""
+  selection per component and the PEC zeroing rule (yee.c:1138-1237).
+- The CPML grading of every face (becebhch, boundary.c:34-99) is the
+  oracle's: b, c of E and H rounded to FP32, kappa exactly."""
 import ctypes as C
 import os
 import shutil
@@ -39,6 +41,9 @@ def probe(tmp_path_factory):
     lib.host_plan_map.restype = C.c_int
     lib.host_plan_classes.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]
     lib.host_plan_classes.restype = C.c_int
+    fp, dp = C.POINTER(C.c_float), C.POINTER(C.c_double)
+    lib.host_plan_cpml.argtypes = [C.c_void_p, C.c_int] + [fp] * 4 + [dp] * 2 + [C.c_int]
+    lib.host_plan_cpml.restype = C.c_int
     return lib
 
 
@@ -115,3 +120,24 @@ def test_planner_coefficients_are_the_oracle_rounded_to_fp32(probe, name):
         assert np.array_equal(per_cell["cb"][:, a][ordinary], f32(cb[a * n:(a + 1) * n])[ordinary])
         assert np.array_equal(((flags >> a) & 1) == 1, ~ordinary & branch)
         assert np.array_equal(((flags >> (CF_PEC_SHIFT + a)) & 1) == 1, ((fl >> (3 + a)) & 1) == 1)
+
+
+@pytest.mark.parametrize("name", ["full", "rough64", "sphere60"])
+def test_planner_cpml_grading_is_the_oracle(probe, name):
+    from oracle import adjoint as A
+    s = SCENES[name]()
+    desc, keep = s.desc()
+    o = CpuSolver(s)
+    fp, dp = C.POINTER(C.c_float), C.POINTER(C.c_double)
+    for face in range(6):
+        mine = [np.zeros(64, np.float32) for _ in range(4)] + [np.zeros(64) for _ in range(2)]
+        n = probe.host_plan_cpml(C.addressof(desc), face, *[a.ctypes.data_as(fp) for a in mine[:4]],
+                                 *[a.ctypes.data_as(dp) for a in mine[4:]], 64)
+        ref = [np.zeros(64) for _ in range(6)]
+        m = A._lib().oracle_get_cpml(o.h, face, *[A._p(a) for a in ref])
+        assert n == m and n > 0, (face, n, m)
+        for q in range(4):                               # be, ce, bh, ch
+            assert np.array_equal(mine[q][:n], ref[q][:m].astype(np.float32)), (face, q)
+        for q in (4, 5):                                 # kappa_e, kappa_h
+            assert np.array_equal(mine[q][:n], ref[q][:m]), (face, q)
+    o.close()
