@@ -68,3 +68,16 @@ extern "C" int host_plan_cpml(const fdtd_desc *d, int face, float *be, float *ce
     }
     return n;
 }
+
+// Scalars of the plan: aux-grid resolution (0 without TSF), whether an ADE
+// material exists, the critical-point pole count of the kernels.
+extern "C" int host_plan_scalars(const fdtd_desc *d, int *jres, int *has_ade, int *maxpoles)
+{
+    HostPlan hp;
+    std::string e;
+    if (build_host_plan(d, &hp, &e) != 0) return -1;
+    *jres = hp.tsf ? hp.jres : 0;
+    *has_ade = hp.has_ade ? 1 : 0;
+    *maxpoles = hp.maxpoles;
+    return 0;
+}

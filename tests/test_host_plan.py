@@ -11,7 +11,9 @@ it, and this file compiles both with g++ into pytest's temporary directory.
   averaging (yee.c:1397-1493) where get_tbc keeps it, the dispersive-branch
   selection per component and the PEC zeroing rule (yee.c:1138-1237).
 - The CPML grading of every face (becebhch, boundary.c:34-99) is the
-  oracle's: b, c of E and H rounded to FP32, kappa exactly."""
+  oracle's: b, c of E and H rounded to FP32, kappa exactly.
+- The TSF auxiliary grid has the oracle's resolution (plan.c:1584-1595), and
+  the dispersive variant is chosen exactly when an ADE material is used."""
 import ctypes as C
 import os
 import shutil
@@ -44,6 +46,8 @@ def probe(tmp_path_factory):
     fp, dp = C.POINTER(C.c_float), C.POINTER(C.c_double)
     lib.host_plan_cpml.argtypes = [C.c_void_p, C.c_int] + [fp] * 4 + [dp] * 2 + [C.c_int]
     lib.host_plan_cpml.restype = C.c_int
+    lib.host_plan_scalars.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 3
+    lib.host_plan_scalars.restype = C.c_int
     return lib
 
 
@@ -141,3 +145,21 @@ def test_planner_cpml_grading_is_the_oracle(probe, name):
         for q in (4, 5):                                 # kappa_e, kappa_h
             assert np.array_equal(mine[q][:n], ref[q][:m]), (face, q)
     o.close()
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_planner_aux_grid_and_variant(probe, name):
+    s = SCENES[name]()
+    desc, keep = s.desc()
+    jres, has_ade, maxpoles = C.c_int(), C.c_int(), C.c_int()
+    assert probe.host_plan_scalars(C.addressof(desc), C.byref(jres), C.byref(has_ade), C.byref(maxpoles)) == 0
+    o = CpuSolver(s)
+    aux_res = o._f("aux_res")
+    aux_res.argtypes = [C.c_void_p]
+    aux_res.restype = C.c_int
+    assert jres.value == (aux_res(o.h) if s.tsf else 0)
+    o.close()
+    used = np.unique(s.mat) if s.mat is not None else np.array([0])
+    uses_ade = any(s.mats[int(i)].type == abi.MAT_ADE for i in used)
+    assert has_ade.value == int(uses_ade)
+    assert maxpoles.value in (0, 2)
