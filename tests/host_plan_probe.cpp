@@ -81,3 +81,20 @@ extern "C" int host_plan_scalars(const fdtd_desc *d, int *jres, int *has_ade, in
     *maxpoles = hp.maxpoles;
     return 0;
 }
+
+// Design region of the plan: the affected box (abox, i0 i1 j0 j1 k0 k1) and
+// its per-cell E coefficients (ca[3], cb[3] per cell, abox order, k fastest),
+// recomputed for eps_r (dbox order) first when eps_r is not NULL; returns the
+// number of cells, 0 without a design region, or -1.
+extern "C" long long host_plan_design(const fdtd_desc *d, const double *eps_r, int abox[6], float *dcoef, size_t cap)
+{
+    HostPlan hp;
+    std::string e;
+    if (build_host_plan(d, &hp, &e) != 0) return -1;
+    if (!hp.design) return 0;
+    if (eps_r) design_coefficients(&hp, eps_r);
+    for (int q = 0; q < 6; q++) abox[q] = hp.abox[q];
+    if (hp.dcoef.size() > cap) return -1;
+    std::memcpy(dcoef, hp.dcoef.data(), sizeof(float) * hp.dcoef.size());
+    return (long long)(hp.dcoef.size() / 6);
+}

@@ -13,7 +13,11 @@ it, and this file compiles both with g++ into pytest's temporary directory.
 - The CPML grading of every face (becebhch, boundary.c:34-99) is the
   oracle's: b, c of E and H rounded to FP32, kappa exactly.
 - The TSF auxiliary grid has the oracle's resolution (plan.c:1584-1595), and
-  the dispersive variant is chosen exactly when an ADE material is used."""
+  the dispersive variant is chosen exactly when an ADE material is used.
+- An adjoint design region's per-cell E coefficients, at creation and after
+  new permittivities, are the oracle's for the same scene with every design
+  cell its own linear material (get_cabs averaging across the region's
+  edges), rounded to FP32."""
 import ctypes as C
 import os
 import shutil
@@ -48,6 +52,8 @@ def probe(tmp_path_factory):
     lib.host_plan_cpml.restype = C.c_int
     lib.host_plan_scalars.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 3
     lib.host_plan_scalars.restype = C.c_int
+    lib.host_plan_design.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_size_t]
+    lib.host_plan_design.restype = C.c_longlong
     return lib
 
 
@@ -163,3 +169,41 @@ def test_planner_aux_grid_and_variant(probe, name):
     uses_ade = any(s.mats[int(i)].type == abi.MAT_ADE for i in used)
     assert has_ade.value == int(uses_ade)
     assert maxpoles.value in (0, 2)
+
+
+def _oracle_coeffs(scene):
+    from oracle import adjoint as A
+    o = CpuSolver(scene)
+    n = scene.ncells
+    ca, cb, da, db = np.zeros(3 * n), np.zeros(3 * n), np.zeros(n), np.zeros(n)
+    fl = np.zeros(n, dtype=np.int32)
+    assert A._lib().oracle_get_coeffs(o.h, A._p(ca), A._p(cb), A._p(da), A._p(db), fl.ctypes.data_as(A._ip)) == 0
+    o.close()
+    shape = (3, scene.xres, scene.yres, scene.zres)
+    return ca.reshape(shape), cb.reshape(shape)
+
+
+def test_planner_design_coefficients_are_the_oracle(probe):
+    s = plan.adjoint_scene(shape=(32, 32, 32), cpml_depth=6, design_shape=(4, 4, 2), glass_cells=3, nsteps=10,
+                           pulse_delay=2e-15, pulse_width=0.7e-15, seed=5)
+    new_eps = np.random.default_rng(9).uniform(1.5, 4.0, s.design["eps"].shape)
+    for eps in (None, new_eps):
+        desc, keep = s.desc()
+        abox = (C.c_int * 6)()
+        buf = np.zeros(6 * 4096, np.float32)
+        arg = None if eps is None else np.ascontiguousarray(eps, dtype=np.float64).ctypes.data
+        n = probe.host_plan_design(C.addressof(desc), arg, abox, buf.ctypes.data, buf.size)
+        assert n > 0
+        mine = buf[:6 * n].reshape(-1, 6)
+        ref_scene = s
+        if eps is not None:
+            ref_scene = plan.adjoint_scene(shape=(32, 32, 32), cpml_depth=6, design_shape=(4, 4, 2), glass_cells=3,
+                                           nsteps=10, pulse_delay=2e-15, pulse_width=0.7e-15, seed=5)
+            ref_scene.design["eps"] = eps.copy()
+        ca, cb = _oracle_coeffs(ref_scene.expanded())
+        b = list(abox)
+        box = (slice(b[0], b[1]), slice(b[2], b[3]), slice(b[4], b[5]))
+        assert n == (b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4])
+        for a in range(3):
+            assert np.array_equal(mine[:, a], ca[a][box].ravel().astype(np.float32)), ("ca", a)
+            assert np.array_equal(mine[:, 3 + a], cb[a][box].ravel().astype(np.float32)), ("cb", a)
