@@ -98,3 +98,15 @@ extern "C" long long host_plan_design(const fdtd_desc *d, const double *eps_r, i
     std::memcpy(dcoef, hp.dcoef.data(), sizeof(float) * hp.dcoef.size());
     return (long long)(hp.dcoef.size() / 6);
 }
+
+// The chain rule of the design region at permittivities eps_r: grad (dbox
+// order) = dJ/d eps_r for dJ/dcb = dcb (3 per affected cell, abox order).
+extern "C" int host_plan_design_gradient(const fdtd_desc *d, const double *eps_r, const double *dcb, double *grad)
+{
+    HostPlan hp;
+    std::string e;
+    if (build_host_plan(d, &hp, &e) != 0 || !hp.design) return -1;
+    design_coefficients(&hp, eps_r);
+    design_gradient(&hp, dcb, grad);
+    return 0;
+}

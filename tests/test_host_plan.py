@@ -17,7 +17,8 @@ it, and this file compiles both with g++ into pytest's temporary directory.
 - An adjoint design region's per-cell E coefficients, at creation and after
   new permittivities, are the oracle's for the same scene with every design
   cell its own linear material (get_cabs averaging across the region's
-  edges), rounded to FP32."""
+  edges), rounded to FP32; the chain rule from dJ/dcb to dJ/d eps_r
+  (design_gradient) agrees with central differences of those coefficients."""
 import ctypes as C
 import os
 import shutil
@@ -54,6 +55,8 @@ def probe(tmp_path_factory):
     lib.host_plan_scalars.restype = C.c_int
     lib.host_plan_design.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_size_t]
     lib.host_plan_design.restype = C.c_longlong
+    lib.host_plan_design_gradient.argtypes = [C.c_void_p] + [C.c_void_p] * 3
+    lib.host_plan_design_gradient.restype = C.c_int
     return lib
 
 
@@ -207,3 +210,39 @@ def test_planner_design_coefficients_are_the_oracle(probe):
         for a in range(3):
             assert np.array_equal(mine[:, a], ca[a][box].ravel().astype(np.float32)), ("ca", a)
             assert np.array_equal(mine[:, 3 + a], cb[a][box].ravel().astype(np.float32)), ("cb", a)
+
+
+def test_planner_design_gradient_vs_central_differences(probe):
+    """J(eps) = sum w * cb(eps) over the affected cells: design_gradient(w) must
+    be dJ/d eps_r.  cb is FP32, so h = 1e-2 on eps_r in [1.5, 4] leaves a
+    rounding noise near 1e-5 and a truncation error near 1e-5 of the largest
+    derivative."""
+    s = plan.adjoint_scene(shape=(32, 32, 32), cpml_depth=6, design_shape=(4, 4, 2), glass_cells=3, nsteps=10,
+                           pulse_delay=2e-15, pulse_width=0.7e-15, seed=5)
+    rng = np.random.default_rng(21)
+    eps = np.ascontiguousarray(rng.uniform(1.5, 4.0, s.design["eps"].shape))
+    desc, keep = s.desc()
+    abox = (C.c_int * 6)()
+    buf = np.zeros(6 * 4096, np.float32)
+
+    def cb_of(e):
+        n = probe.host_plan_design(C.addressof(desc), np.ascontiguousarray(e).ctypes.data, abox, buf.ctypes.data,
+                                   buf.size)
+        assert n > 0
+        return buf[:6 * n].reshape(-1, 6)[:, 3:].astype(np.float64)
+
+    w = rng.standard_normal(cb_of(eps).shape)
+    w = np.ascontiguousarray(w / np.abs(cb_of(eps)).max())
+    grad = np.zeros(eps.size)
+    assert probe.host_plan_design_gradient(C.addressof(desc), eps.ctypes.data, w.ctypes.data, grad.ctypes.data) == 0
+    h = 1e-2
+    fd = np.zeros(eps.size)
+    flat = eps.ravel()
+    for q in range(eps.size):
+        up, dn = flat.copy(), flat.copy()
+        up[q] += h
+        dn[q] -= h
+        fd[q] = ((w * cb_of(up.reshape(eps.shape))).sum() - (w * cb_of(dn.reshape(eps.shape))).sum()) / (2 * h)
+    err = np.abs(grad - fd).max() / np.abs(fd).max()
+    print("design gradient vs central differences:", err)
+    assert err < 1e-3, err
