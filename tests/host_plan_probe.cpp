@@ -110,3 +110,17 @@ extern "C" int host_plan_design_gradient(const fdtd_desc *d, const double *eps_r
     design_gradient(&hp, dcb, grad);
     return 0;
 }
+
+// The planner's ADE coefficient sets (DevAde, in the order of the ADE
+// materials); *record receives sizeof(DevAde).  Returns the number of sets or -1.
+extern "C" int host_plan_ades(const fdtd_desc *d, void *out, int max_sets, int *record)
+{
+    HostPlan hp;
+    std::string e;
+    if (build_host_plan(d, &hp, &e) != 0) return -1;
+    *record = (int)sizeof(DevAde);
+    const int n = (int)hp.ades.size();
+    if (n > max_sets) return -1;
+    std::memcpy(out, hp.ades.data(), sizeof(DevAde) * n);
+    return n;
+}

@@ -18,7 +18,10 @@ it, and this file compiles both with g++ into pytest's temporary directory.
   new permittivities, are the oracle's for the same scene with every design
   cell its own linear material (get_cabs averaging across the region's
   edges), rounded to FP32; the chain rule from dJ/dcb to dJ/d eps_r
-  (design_gradient) agrees with central differences of those coefficients."""
+  (design_gradient) agrees with central differences of those coefficients.
+- The ADE coefficient sets restate GSvit's polarisation recursion
+  (yee.c:923-1082) in difference form (Q = P_D^n - P_D^{n-1}, per pole
+  p = P^n, q = P^n - P^{n-1}): driven alike, the two give the same E."""
 import ctypes as C
 import os
 import shutil
@@ -57,6 +60,8 @@ def probe(tmp_path_factory):
     lib.host_plan_design.restype = C.c_longlong
     lib.host_plan_design_gradient.argtypes = [C.c_void_p] + [C.c_void_p] * 3
     lib.host_plan_design_gradient.restype = C.c_int
+    lib.host_plan_ades.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    lib.host_plan_ades.restype = C.c_int
     return lib
 
 
@@ -246,3 +251,78 @@ def test_planner_design_gradient_vs_central_differences(probe):
     err = np.abs(grad - fd).max() / np.abs(fd).max()
     print("design gradient vs central differences:", err)
     assert err < 1e-3, err
+
+
+# DevAde (gsvit_copy_b200/csrc/fdtd_internal.h)
+DEV_ADE = np.dtype([("c0dx", "<f4"), ("c2", "<f4"), ("c3", "<f4"), ("qe", "<f4"), ("ma0", "<f4"), ("a2", "<f4"),
+                    ("pe", "<f4", 2), ("qpe", "<f4", 2), ("rp", "<f4", 2), ("rq", "<f4", 2), ("bp2", "<f4", 2),
+                    ("bp3", "<f4", 2), ("bp4", "<f4", 2)])
+
+
+def _reference_ade(m, dx, curl):
+    """GSvit's update of one dispersive component, FP64 (yee.c:923-929 for E,
+    yee.c:1070-1082 for P_D and the critical-point P, then the n-1 copies)."""
+    e = ep = 0.0
+    dp = dpp = 0.0
+    p, pp = [0.0, 0.0], [0.0, 0.0]
+    out = np.empty(len(curl))
+    for n, cu in enumerate(curl):
+        e1 = (m.ade_c0 * cu / dx + m.ade_c1 * (-m.ade_a0 * dpp + (1 - m.ade_a1) * dp)
+              + sum(m.ade_c1 * (-m.ade_bp0[q] * pp[q] + (1 - m.ade_bp1[q]) * p[q]) for q in range(2))
+              + m.ade_c2 * ep + m.ade_c3 * e)
+        dpn = m.ade_a0 * dpp + m.ade_a1 * dp + m.ade_a2 * (ep + 2 * e + e1)
+        pn = [m.ade_bp0[q] * pp[q] + m.ade_bp1[q] * p[q] + m.ade_bp2[q] * ep + m.ade_bp3[q] * e + m.ade_bp4[q] * e1
+              for q in range(2)]
+        dpp, dp, pp, p, ep, e = dp, dpn, p, pn, e, e1
+        out[n] = e1
+    return out
+
+
+def _difference_ade(a, curl):
+    """The difference form the kernels run, in FP64 arithmetic with the given coefficients."""
+    e = ep = 0.0
+    qd = 0.0
+    p, q = [0.0, 0.0], [0.0, 0.0]
+    out = np.empty(len(curl))
+    for n, cu in enumerate(curl):
+        v = (a["c0dx"] * cu + a["qe"] * qd + sum(a["qpe"][k] * q[k] + a["pe"][k] * p[k] for k in range(2))
+             + a["c2"] * ep + a["c3"] * e)
+        qd = a["ma0"] * qd + a["a2"] * (ep + 2 * e + v)
+        for k in range(2):
+            qn = a["rp"][k] * p[k] + a["rq"][k] * q[k] + a["bp2"][k] * ep + a["bp3"][k] * e + a["bp4"][k] * v
+            q[k] = qn
+            p[k] += qn
+        ep, e = e, v
+        out[n] = v
+    return out
+
+
+def _exact_sets(m, dx):
+    """The planner's formulas (plan_host.cpp) without the rounding to FP32."""
+    return {"c0dx": m.ade_c0 / dx, "c2": m.ade_c2, "c3": m.ade_c3, "qe": m.ade_c1 * m.ade_a0, "ma0": -m.ade_a0,
+            "a2": m.ade_a2, "pe": [m.ade_c1 * ((1.0 - m.ade_bp0[k]) - m.ade_bp1[k]) for k in range(2)],
+            "qpe": [m.ade_c1 * m.ade_bp0[k] for k in range(2)],
+            "rp": [(m.ade_bp0[k] + m.ade_bp1[k]) - 1.0 for k in range(2)], "rq": [-m.ade_bp0[k] for k in range(2)],
+            "bp2": list(m.ade_bp2), "bp3": list(m.ade_bp3), "bp4": list(m.ade_bp4)}
+
+
+@pytest.mark.parametrize("name", ["ade", "full", "rough64", "rough64_lorentz"])
+def test_planner_ade_sets_restate_the_recursion(probe, name):
+    s = (plan.rough_surface_scene(res=64, nsteps=10, nfff_angles=None, material="lorentz")
+         if name == "rough64_lorentz" else SCENES[name]())
+    desc, keep = s.desc()
+    sets = np.zeros(16, dtype=DEV_ADE)
+    record = C.c_int()
+    n = probe.host_plan_ades(C.addressof(desc), sets.ctypes.data, 16, C.byref(record))
+    assert record.value == DEV_ADE.itemsize
+    ade_mats = [m for m in s.mats[1:] if m.type == abi.MAT_ADE]
+    assert n == len(ade_mats) > 0
+    rng = np.random.default_rng(17)
+    for a, m in zip(sets[:n], ade_mats):
+        curl = rng.standard_normal(2000) * s.dx / m.ade_c0          # c0 * curl / dx of order 1
+        ref = _reference_ade(m, s.dx, curl)
+        exact = _difference_ade(_exact_sets(m, s.dx), curl)
+        fp32 = _difference_ade(a, curl)
+        scale = np.linalg.norm(ref)
+        assert np.linalg.norm(exact - ref) / scale < 1e-12    # the algebra of the restatement
+        assert np.linalg.norm(fp32 - ref) / scale < 1e-5      # with the coefficients the kernels get
