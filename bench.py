@@ -76,6 +76,48 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+class Replicas:
+    """Plumbing of an N-rank run (torchrun, one process per GPU).  The ranks
+    are independent replicas and exchange no data: a barrier on each side of
+    the timed region and the slowest rank's time are all they share.  The GPU
+    arm uses NCCL on its device; with one rank nothing is initialised."""
+
+    def __init__(self, backend="nccl", device=None):
+        import torch
+        self.rank, self.local, self.world = dist_env()
+        self.device = device if device is not None else torch.device("cpu")
+        self.dist = None
+        if self.world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            kw = {"device_id": self.device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=timedelta(seconds=300), **kw)
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x):
+        """The largest x over the ranks (every rank gets it)."""
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def whole_job_gcells(cells_per_rank, steps, world, seconds):
+    """Whole-job throughput: the cell updates of every rank over the slowest rank's time."""
+    return cells_per_rank * steps * world / seconds / 1e9
+
+
 def workload_scene(res, nsteps_planned):
     from gsvit_copy_b200 import plan
     return plan.rough_surface_scene(res=res, nsteps=nsteps_planned)
@@ -251,8 +293,6 @@ def run_reference(a):
 
 def run_b200(a):
     import torch
-    import torch.distributed as dist
-    from datetime import timedelta
     from gsvit_copy_b200 import abi
     from gsvit_copy_b200.solver import Solver
 
@@ -260,19 +300,8 @@ def run_b200(a):
     if not torch.cuda.is_available():
         raise SystemExit("bench.py: no CUDA device (the library has no CPU path)")
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Replicas("nccl", torch.device("cuda", local))
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     K, W = a.steps, a.warmup
     scene = workload_scene(a.res, max(4000, K + W + 64))
@@ -297,7 +326,7 @@ def run_b200(a):
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1))
     clocks = clk.summary()
-    value = scene.ncells * K * world / (ms * 1e-3) / 1e9
+    value = whole_job_gcells(scene.ncells, K, world, ms * 1e-3)
 
     # per-kernel profile of a few more steps (CUDA events around each launch)
     prof = g.step_profile(8)
@@ -339,7 +368,7 @@ def run_b200(a):
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     h2d = 6 * scene.ncells * 4
     d2h = 3 * scene.ncells * 4 + pr.nbytes
-    e2e = {"value": scene.ncells * K * world / e2e_s / 1e9, "unit": UNIT,
+    e2e = {"value": whole_job_gcells(scene.ncells, K, world, e2e_s), "unit": UNIT,
            "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
            "job": "upload 6 fields f32 from pinned host, K steps, read probes + final E (f32) to pinned host"}
     g.close()
@@ -365,8 +394,7 @@ def run_b200(a):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
