@@ -76,3 +76,38 @@ def test_keywords_outside_the_path(tmp_path, text, word):
     deck.write_text("POOL\n20 20 20 1e-8 1e-8 1e-8\n\nCOMP\n10\n\n" + text)
     with pytest.raises(parfile.ParError, match=word):
         parfile.load_par(str(deck))
+
+
+def test_killer_file_rule(tmp_path):
+    """GSvit's killcheck (svit.c:91-107): stop when the file exists and reads 1."""
+    from gsvit_copy_b200.run import killer_says_stop
+    f = tmp_path / "killer"
+    assert not killer_says_stop(str(f))            # absent
+    for text, stop in (("0", False), ("2", False), ("1", True), ("  1\n", True), ("1 0", True), ("x1", False),
+                       ("", False), ("-1", False)):
+        f.write_text(text)
+        assert killer_says_stop(str(f)) == stop, text
+
+
+def test_killer_file_stops_the_step_loop(tmp_path):
+    """The runner looks at the file after every `check_every` steps and stops
+    cleanly once it says 1; without a killer file one call does all steps."""
+    from gsvit_copy_b200.run import run_steps
+    f = tmp_path / "killer"
+    f.write_text("0")
+    calls = []
+
+    def step(k):
+        calls.append(k)
+        if sum(calls) >= 7:                      # an operator writes 1 after step 7
+            f.write_text("1")
+
+    assert run_steps(step, 100, str(f)) == 7 and calls == [1] * 7
+    calls.clear()
+    f.write_text("0")
+    assert run_steps(step, 100, str(f), check_every=5) == 10 and calls == [5, 5]
+    calls.clear()
+    assert run_steps(step, 12, None) == 12 and calls == [12]
+    calls.clear()
+    f.write_text("0")
+    assert run_steps(lambda k: calls.append(k), 9, str(f), check_every=4) == 9 and calls == [4, 4, 1]
