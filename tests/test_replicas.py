@@ -83,3 +83,25 @@ def test_reference_arm_runs_on_rank_zero_only():
                                   MASTER_PORT=_free_port()))
     assert out.returncode == 0, out.stderr
     assert out.stdout.strip() == ""
+
+
+def test_reference_arm_prints_the_contract_line():
+    """Rank 0 of the reference arm times GSvit's own CPU code on a bounded
+    sample and prints one JSON line with the bench contract's keys."""
+    import pytest
+    from oracle.pyoracle import reference_available
+    if not reference_available():
+        pytest.skip("GSvit's CPU build (oracle/_ref) is not built here")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "3"], cwd=ROOT, text=True, capture_output=True, timeout=600, env=_env())
+    assert out.returncode == 0, out.stderr
+    lines = [x for x in out.stdout.strip().splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    x = json.loads(lines[0])
+    assert x["impl"] == "reference" and x["metric"] == "Gcell-updates/s" and x["unit"] == "Gcell/s"
+    assert x["higher_is_better"] is True and x["steps"] == 1 and x["warmup"] == 3 and x["value"] > 0
+    cb = x["cpu_baseline"]
+    assert cb["value"] == x["value"] and cb["unit"] == x["unit"] and cb["cores"] >= 1
+    assert cb["kind"] in ("reference", "port") and cb["sample"]
+    assert x["e2e"] == {"value": x["value"], "unit": x["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert "workload" in x["config"]
