@@ -106,7 +106,9 @@ struct fdtd_plan {
     int nbulk = 0;
     bool bulk_on = false;
     BulkMaps bmaps[2];
-    int *d_err = nullptr;
+    int *d_err = nullptr;                 // set by a bulk CTA whose bounded wait expired
+    const int *batch_err = nullptr;       // the batch's error word, for an instance of a batch
+    bool failed = false;                  // an expired wait was reported: the plan only accepts destroy
     int region[6] = {0, 0, 0, 0, 0, 0};   // bulk box Xlo Xhi Ylo Yhi Zlo Zhi
     std::vector<SlabBox> h_boxes;         // host copies of the work lists (batched launches)
     std::vector<SlabBox> h_eboxes;        // E runs with a dispersive cell (every box when unsplit)
@@ -134,6 +136,28 @@ struct fdtd_plan {
 };
 
 namespace {
+
+// The device error words of a plan, read after its stream is synchronised.  A
+// bulk CTA whose bounded wait expired left its cells of that step unwritten,
+// so every later readback would return corrupt values: the readback reports
+// FDTD_E_TIMEOUT instead and the plan refuses further steps.
+int device_error(fdtd_plan *P)
+{
+    int err = 0;
+    CK(cudaMemcpy(&err, P->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!err && P->batch_err) CK(cudaMemcpy(&err, P->batch_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        P->failed = true;
+        return fail(FDTD_E_TIMEOUT, "a bounded wait of the bulk kernel expired; the fields are incomplete and the plan "
+                                    "must be destroyed");
+    }
+    return FDTD_OK;
+}
+
+int refuse_failed(const fdtd_plan *P)
+{
+    return fail(FDTD_E_STATE, "a bounded device wait of this plan expired earlier; destroy the plan");
+}
 
 DevPlan plan_for(const fdtd_plan *P, int in)
 {
@@ -898,10 +922,7 @@ int fdtd_sync(fdtd_plan *P)
     if (!P) return fail(FDTD_E_INVALID, "plan is NULL");
     CK(cudaSetDevice(P->device));
     CK(cudaStreamSynchronize(P->stream));
-    int err = 0;
-    CK(cudaMemcpy(&err, P->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err) return fail(FDTD_E_TIMEOUT, "a bounded wait of the bulk kernel expired");
-    return FDTD_OK;
+    return device_error(P);
 }
 
 int fdtd_set_fields(fdtd_plan *P, int mask, const double *const comps[6])
@@ -958,7 +979,7 @@ int fdtd_get_fields_f32(fdtd_plan *P, int mask, float *const comps[6])
         if (rc != FDTD_OK) return rc;
     }
     CK(cudaStreamSynchronize(P->stream));
-    return FDTD_OK;
+    return device_error(P);
 }
 
 int fdtd_get_fields(fdtd_plan *P, int mask, double *const comps[6])
@@ -974,12 +995,14 @@ int fdtd_get_fields(fdtd_plan *P, int mask, double *const comps[6])
         CK(cudaStreamSynchronize(P->stream));
         for (size_t q = 0; q < P->hp.n; q++) comps[c][q] = (double)tmp[q];
     }
-    return FDTD_OK;
+    CK(cudaStreamSynchronize(P->stream));
+    return device_error(P);
 }
 
 int fdtd_step(fdtd_plan *P, int nsteps)
 {
     if (!P || nsteps < 0) return fail(FDTD_E_INVALID, "bad argument");
+    if (P->failed) return refuse_failed(P);
     CK(cudaSetDevice(P->device));
     for (int s = 0; s < nsteps; s++) {
         int rc = launch_step(P, P->stream);
@@ -1001,6 +1024,9 @@ namespace {
 
 constexpr int kStaticDevices = 64;
 std::mutex g_static_mu;
+// the array's device address per device, looked up once and kept for the
+// life of the process: valid as long as the device is not reset
+// (cudaDeviceReset) while the library stays loaded
 void *g_static_addr[kStaticDevices] = {};
 
 // Device address of g_static_scratch on `device` (current), looked up once.
@@ -1026,6 +1052,7 @@ extern "C" {
 int fdtd_step_static_scratch(fdtd_plan *P, int nsteps)
 {
     if (!P || nsteps < 0) return fail(FDTD_E_INVALID, "bad argument");
+    if (P->failed) return refuse_failed(P);
     CK(cudaSetDevice(P->device));
     unsigned char *base = nullptr;
     int rc = static_scratch_addr(P->device, &base);
@@ -1071,6 +1098,7 @@ int fdtd_step_static_scratch(fdtd_plan *P, int nsteps)
 int fdtd_step_graph(fdtd_plan *P, int nsteps, int chunk)
 {
     if (!P || nsteps < 0) return fail(FDTD_E_INVALID, "bad argument");
+    if (P->failed) return refuse_failed(P);
     CK(cudaSetDevice(P->device));
     if (chunk < 2) chunk = 2;
     chunk &= ~1;   // an even number of steps returns the ping-pong parity
@@ -1125,6 +1153,7 @@ int fdtd_get_step(const fdtd_plan *P, int *step)
 int fdtd_step_timed(fdtd_plan *P, int nsteps, double *fused_ms, int *fused_launches)
 {
     if (!P || nsteps < 0) return fail(FDTD_E_INVALID, "bad argument");
+    if (P->failed) return refuse_failed(P);
     CK(cudaSetDevice(P->device));
     std::vector<cudaEvent_t> ev(2 * (size_t)nsteps);
     for (auto &e : ev) CK(cudaEventCreate(&e));
@@ -1159,6 +1188,7 @@ int fdtd_step_timed(fdtd_plan *P, int nsteps, double *fused_ms, int *fused_launc
 int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
 {
     if (!P || nsteps < 1 || !out) return fail(FDTD_E_INVALID, "bad argument");
+    if (P->failed) return refuse_failed(P);
     CK(cudaSetDevice(P->device));
     const int NE = 6;
     std::vector<cudaEvent_t> ev((size_t)NE * nsteps);
@@ -1223,7 +1253,7 @@ int fdtd_get_probes(fdtd_plan *P, double *out, size_t out_len)
     CK(cudaSetDevice(P->device));
     CK(cudaMemcpyAsync(out, P->aux.probe_out, need * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
     CK(cudaStreamSynchronize(P->stream));
-    return FDTD_OK;
+    return device_error(P);
 }
 
 int fdtd_nfff_spectrum(fdtd_plan *P, double *out, size_t out_len)
@@ -1238,7 +1268,7 @@ int fdtd_nfff_spectrum(fdtd_plan *P, double *out, size_t out_len)
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, P->ff.out, need * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
     CK(cudaStreamSynchronize(P->stream));
-    return FDTD_OK;
+    return device_error(P);
 }
 
 int fdtd_nfff_ndata(const fdtd_plan *P, int *ndata)
@@ -1258,7 +1288,7 @@ int fdtd_nfff_series(fdtd_plan *P, double *out, size_t out_len)
     CK(cudaSetDevice(P->device));
     CK(cudaMemcpyAsync(out, P->ns.series, need * sizeof(double), cudaMemcpyDeviceToHost, P->stream));
     CK(cudaStreamSynchronize(P->stream));
-    return FDTD_OK;
+    return device_error(P);
 }
 
 int fdtd_get_map(fdtd_plan *P, int which, int32_t *out, size_t out_len)
@@ -1314,7 +1344,7 @@ int fdtd_snapshot_save(fdtd_plan *P, void *host_buf, size_t bytes)
         p += s.bytes;
     }
     CK(cudaStreamSynchronize(P->stream));
-    return FDTD_OK;
+    return device_error(P);
 }
 
 int fdtd_snapshot_restore(fdtd_plan *P, const void *host_buf, size_t bytes)
@@ -1593,6 +1623,7 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
         B->nepboxes = (int)pbx.size();
     }
     BA(B->mem.alloc(&B->d_err, 1), "error word");
+    for (auto *P : B->plans) P->batch_err = B->d_err;   // the instances' readbacks check the batch's word too
     BA(batch_set_items(B, 0, true), "batch work list");
     BA(cudaDeviceSynchronize(), "batch set-up");
 #undef BA
@@ -1885,6 +1916,8 @@ int objective_from_spectrum(fdtd_plan *P, const fdtd_objective *obj, double *J)
     std::vector<double2> spec(n);
     CK(cudaMemcpyAsync(spec.data(), P->ff.out, n * sizeof(double2), cudaMemcpyDeviceToHost, P->stream));
     CK(cudaStreamSynchronize(P->stream));
+    const int rc = device_error(P);
+    if (rc != FDTD_OK) return rc;
     double j = 0;
     for (int t = 0; t < obj->npoints; t++)
         for (int c = 0; c < 3; c++) {
@@ -1948,6 +1981,7 @@ int fdtd_adjoint_gradient(fdtd_plan *P, const fdtd_objective *obj, int nsteps, i
 {
     if (!P || !J || !grad || nsteps < 1 || checkpoint < 1) return fail(FDTD_E_INVALID, "bad argument");
     if (!P->hp.design) return fail(FDTD_E_STATE, "the plan has no design region");
+    if (P->failed) return refuse_failed(P);
     int rc = check_objective(P, obj);
     if (rc == FDTD_OK) rc = check_adjoint_plan(P);
     if (rc != FDTD_OK) return rc;

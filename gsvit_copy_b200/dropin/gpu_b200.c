@@ -10,8 +10,17 @@
  * headers, with UCUDA defined so that SvPool carries its `gpu` member) in
  * place of gpu.c and gpu_kernels.cu, and linked with libgsvit_b200.
  *
- * Behaviour kept from gpu.c: the calls return 0 and print the error text on
- * failure (gpu_kernels.cu:6063-6068 prints and returns); copyfrom writes the
+ * Errors: gpu.c prints CUDA errors and carries on (gpu_kernels.cu:6063-6068);
+ * here a failed call prints the library's error text and returns 1, and
+ * sv_gpu_new returns NULL (so sv_pool_allocate_gpus leaves mp->gpu unset).
+ * sv_gpu_new also refuses, before any library or CUDA call, every deck that
+ * asks for something the library does not step: outer boundaries other than
+ * CPML or none (PEC walls, Liao, periodic), inner medium boundaries, sources
+ * other than the TSF plane wave (point, local, SF, LTSF, TSFF, LTSFF,
+ * sheet), subgrids, material types other than linear-tabulated, ADE
+ * (Drude / critical points) and PEC (the RC Drude / CP3 / CP and PLRC
+ * models), sums, forces and the periodic far field.
+ * Behaviour kept from gpu.c: copyfrom writes the
  * fields back into mp->d, the point outputs into mp->out->outpointdata
  * (output.c:341-352 layout) and the far-field series into
  * mp->farfield->rpoints[n].ex/ey/ez->data (farfield.c:175-405).  One whole time
@@ -95,17 +104,63 @@ static void cpml_face(fdtd_cpml_face *f, SvBoundaryType t, int depth, int m, dou
     f->kappa = kappa;
 }
 
+static int outer_ok(SvBoundaryType t) { return t == SV_BOUNDARY_NONE || t == SV_BOUNDARY_CPML; }
+
+/* The first feature of the deck that this library does not step, or NULL.
+ * Settings as the parser and planner leave them: SvSetBoundary /
+ * SvSetMBoundary (settings.h:529-590), SvSetSource (settings.h:491-508) and the
+ * planned SvSource (source.h:224-233), SvSetOutput sums/forces
+ * (settings.h:625-650), SvSetPFarfield (settings.h:827-864), SvSetSubgrid
+ * (settings.h:522-525), the material table (SvMatProp.type, settings.h:103-113). */
+static const char *b200_unsupported(const SvPool *mp, const SvSet *set)
+{
+    const SvSetBoundary *b = &set->sb;
+    const SvSetMBoundary *m = &set->smb;
+    int n;
+    if (!outer_ok(b->bx0) || !outer_ok(b->bxn) || !outer_ok(b->by0) || !outer_ok(b->byn) || !outer_ok(b->bz0) ||
+        !outer_ok(b->bzn))
+        return "outer boundary other than CPML or none (PEC wall, Liao or periodic)";
+    if (m->bx0 != SV_BOUNDARY_NONE || m->bxn != SV_BOUNDARY_NONE || m->by0 != SV_BOUNDARY_NONE ||
+        m->byn != SV_BOUNDARY_NONE || m->bz0 != SV_BOUNDARY_NONE || m->bzn != SV_BOUNDARY_NONE)
+        return "inner medium boundary";
+    /* sv_source_new (source.c:40-51) leaves sp and sl unset and the others
+     * NULL; the planner fills the latter only for sources the deck has */
+    if (set->ss.npnts > 0) return "point source";
+    if (set->ss.nlocals > 0) return "local source";
+    if (mp->src && mp->src->sf) return "SF source";
+    if (mp->src && mp->src->ltsf) return "LTSF source";
+    if (mp->src && mp->src->tsff) return "TSFF source";
+    if (mp->src && mp->src->ltsff) return "LTSFF source";
+    if (mp->src && mp->src->sh) return "sheet source";
+    if (set->sg.nsg > 0) return "subgrid";
+    if (set->so.nsums > 0) return "sum output";
+    if (set->so.nforces > 0) return "force output";
+    if (set->spf.nrs > 0) return "periodic far field";   /* mp->pfarfield exists even without points */
+    for (n = 1; n < mp->nmat; n++) {   /* mats[0] is vacuum (plan.c:78, 2418) */
+        const int t = mp->mats[n].type;
+        if (t != SV_MAT_LINTAB && t != SV_MAT_ADE && t != SV_MAT_PEC)
+            return "material type other than linear-tabulated, ADE (Drude / critical points) or PEC";
+    }
+    return NULL;
+}
+
 /* sv_gpu_new (gpu.c:1960): the planner's state as an fdtd_desc, one plan */
 SvGpu *sv_gpu_new(SvPool *mp, SvSet *set)
 {
     SvYeeData *d = mp->d;
-    B200Gpu *g = (B200Gpu *)calloc(1, sizeof(B200Gpu));
+    B200Gpu *g;
     fdtd_desc desc;
     fdtd_material *mats = NULL;
     int32_t *mat = NULL, *pts = NULL, *ist = NULL, *probes = NULL;
     float *eps = NULL, *sig = NULL, *mu = NULL, *sigast = NULL;
+    const char *unsupported = b200_unsupported(mp, set);
     int n, rc;
 
+    if (unsupported) {
+        fprintf(stderr, "Error: GSvit B200 does not step this deck: unsupported %s\n", unsupported);
+        return NULL;
+    }
+    g = (B200Gpu *)calloc(1, sizeof(B200Gpu));
     memset(&desc, 0, sizeof(desc));
     desc.abi_version = FDTD_ABI_VERSION;
     desc.xres = set->sp.xres; desc.yres = set->sp.yres; desc.zres = set->sp.zres;
@@ -306,7 +361,8 @@ int sv_pool_gpu_boundary_estep(SvPool *mp, SvSet *set) { (void)mp; (void)set; re
 int sv_pool_gpu_apply_farfield(SvPool *mp, SvSet *set) { (void)mp; (void)set; return 0; }
 int sv_pool_gpu_getpoints(SvPool *mp, SvSet *set) { (void)mp; (void)set; return 0; }
 
-/* sums, forces and the periodic far field are outside this library */
+/* sums, forces and the periodic far field: sv_gpu_new refuses decks that
+ * request them, so with a plan these have nothing to do */
 int sv_pool_gpu_getsum(SvPool *mp, SvSet *set) { (void)mp; (void)set; return 0; }
 int sv_pool_gpu_getforce(SvPool *mp, SvSet *set) { (void)mp; (void)set; return 0; }
 int sv_pool_gpu_apply_pfarfield(SvPool *mp, SvSet *set) { (void)mp; (void)set; return 0; }

@@ -43,7 +43,12 @@ extern "C" {
 #define FDTD_E_CUDA         -3   /* CUDA runtime / driver error */
 #define FDTD_E_NOMEM        -4   /* host or device allocation failed */
 #define FDTD_E_STATE        -5   /* call out of order (e.g. not initialised) */
-#define FDTD_E_TIMEOUT      -6   /* a bounded device wait gave up */
+#define FDTD_E_TIMEOUT      -6   /* a bounded device wait gave up: that step's
+                                  * fields are incomplete.  fdtd_sync and every
+                                  * call that reads results back (fields, probes,
+                                  * far field, snapshot, objective) report it;
+                                  * the plan then refuses to step
+                                  * (FDTD_E_STATE) and must be destroyed */
 
 /* ---- material / mode codes (values of src3d/settings.h:103-123) -------- */
 #define FDTD_MAT_LINEAR   0
@@ -265,8 +270,10 @@ int fdtd_step_graph(fdtd_plan *plan, int nsteps, int chunk);
  * (inputs and outputs); every GPU that loads the library holds the 32 MiB
  * array until the process exits.
  *  - The first call on a device does set-up: it looks up the array's device
- *    address (with that device current) and keeps it.  Make that first call
- *    before any stream capture.
+ *    address (with that device current) and keeps it for the life of the
+ *    process.  Make that first call before any stream capture.  The kept
+ *    address assumes the device is not reset (cudaDeviceReset) while the
+ *    library stays loaded.
  *  - A plan whose tables need more than FDTD_STATIC_SCRATCH_BYTES (2 x 8 bytes
  *    per TSF face cell, each table rounded up to 256 bytes) is rejected with
  *    FDTD_E_UNSUPPORTED; the fields are left untouched.

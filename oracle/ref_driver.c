@@ -473,6 +473,37 @@ int dropin_step(ref_state *r, int nsteps)
     return rc ? -1 : 0;
 }
 
+/* Marks the planned deck as asking for one feature the drop-in does not
+ * step (test of sv_gpu_new's refusal): 0 Liao boundary, 1 periodic boundary,
+ * 2 PEC wall, 3 inner medium boundary, 4 point source, 5 SF source, 6 LTSF
+ * source, 7 TSFF source, 8 subgrid, 9 sum output, 10 force output, 11
+ * periodic far field, 12 an RC Drude material.  Returns -1 for an unknown id. */
+int dropin_request(ref_state *r, int feature)
+{
+    SvPool *mp = r->mp;
+    SvSet *set = r->set;
+    switch (feature) {
+    case 0: set->sb.bx0 = SV_BOUNDARY_LIAO; break;
+    case 1: set->sb.bzn = SV_BOUNDARY_PERIODIC; break;
+    case 2: set->sb.byn = SV_BOUNDARY_PEC; break;
+    case 3: set->smb.bz0 = SV_BOUNDARY_CPML; break;
+    case 4: set->ss.npnts = 1; break;
+    case 5: mp->src->sf = (SvSourceSF *)g_malloc0(sizeof(SvSourceSF)); break;
+    case 6: mp->src->ltsf = (SvSourceLTSF *)g_malloc0(sizeof(SvSourceLTSF)); break;
+    case 7: mp->src->tsff = (SvSourceTSFF *)g_malloc0(sizeof(SvSourceTSFF)); break;
+    case 8: set->sg.nsg = 1; break;
+    case 9: set->so.nsums = 1; break;
+    case 10: set->so.nforces = 1; break;
+    case 11: set->spf.nrs = 1; break;
+    case 12:
+        if (mp->nmat < 2) return -1;
+        mp->mats[mp->nmat - 1].type = SV_MAT_DRUDE;
+        break;
+    default: return -1;
+    }
+    return 0;
+}
+
 /* sv_pool_gpu_copyfrom at output time (svit.c:251-253) */
 int dropin_finish(ref_state *r) { return sv_pool_gpu_copyfrom(r->mp, r->set, SV_SYNC_EH) ? -1 : 0; }
 

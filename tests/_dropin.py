@@ -26,7 +26,7 @@ def _lib():
                            ("ref_nfff_ndata", [P], C.c_int), ("ref_get_nfff_series", [P, _dp], C.c_int),
                            ("ref_get_probes", [P, _dp], C.c_int), ("dropin_start", [P], C.c_int),
                            ("dropin_step", [P, C.c_int], C.c_int), ("dropin_finish", [P], C.c_int),
-                           ("dropin_get_probes", [P, _dp], C.c_int)]:
+                           ("dropin_get_probes", [P, _dp], C.c_int), ("dropin_request", [P, C.c_int], C.c_int)]:
             f = getattr(lib, name)
             f.argtypes, f.restype = a, r
         _LIB = lib

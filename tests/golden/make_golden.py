@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 from gsvit_copy_b200 import abi, plan  # noqa: E402
 from oracle import pyoracle  # noqa: E402
 
-SELFTEST_DIR = "/root/reference/tests/selftests"
+SELFTEST_DIR = os.path.join(os.environ.get("GSVIT_REF", "/root/reference"), "tests", "selftests")
 # 10031111 is left out: its golden file predates the current far-field buffer
 # length (50000 rows instead of 2702) and GSvit's own stepping code, compiled
 # from its sources (oracle/_ref), misses it by 0.8 % under the tests.c metric,

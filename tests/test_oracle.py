@@ -78,7 +78,7 @@ def test_oracle_vs_reference_fixture(kind):
     assert rel_l2(o.nfff_series(), g["nfff_series"]) < 1e-12
 
 
-SELFTEST_DIR = "/root/reference/tests/selftests"
+SELFTEST_DIR = os.path.join(os.environ.get("GSVIT_REF", "/root/reference"), "tests", "selftests")
 
 
 @pytest.mark.parametrize("code", ["35011"])
