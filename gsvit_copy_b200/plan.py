@@ -577,13 +577,16 @@ def cone_objective(scene: Scene, theta_deg: float = 20.0, half_deg: float = 10.0
 def adjoint_scene(shape=(256, 256, 128), dx: float = 10e-9, cpml_depth: int = 12, nsteps: int = 4000,
                   design_shape=(64, 64, 16), seed: int = 5, eps_range=(1.5, 4.0), glass_eps: float = 2.1,
                   glass_cells: int = 20, wavelength: float = 550e-9, margin: int = 4,
-                  pulse_delay: float = 15e-15, pulse_width: float = 5e-15) -> Scene:
+                  pulse_delay: float = 15e-15, pulse_width: float = 5e-15, metal_cells: int = 0) -> Scene:
     """Adjoint workload: a design box of per-cell permittivity (seeded uniform
     in eps_range) on a glass slab (eps_r 2.1) inside the TSF box, lit at
     normal incidence (theta = 0, x-polarised) by a 550 nm Gaussian pulse
     (width 5 fs, delay 15 fs by default); NFFF box between the CPML and the TSF box with
     a running DFT at 550 nm.  Default: 256 x 256 x 128 cells of 10 nm, 12-cell
-    CPML, 64 x 64 x 16 design cells, 4000 steps, DT_MULT 0.5."""
+    CPML, 64 x 64 x 16 design cells, 4000 steps, DT_MULT 0.5.  metal_cells > 0
+    adds a Drude-silver layer of that many cells at the bottom of the grid
+    (inside the z0 CPML and across the x and y slabs): a dispersive problem
+    whose adjoint runs through the ADE branch and the CPML inside it."""
     xr, yr, zr = shape
     dt = plan_dt(dx, dx, dx, 0.5)
     s = Scene(name=f"adjoint{xr}x{yr}x{zr}", xres=xr, yres=yr, zres=zr, dx=dx, dt=dt, nsteps=nsteps)
@@ -593,6 +596,9 @@ def adjoint_scene(shape=(256, 256, 128), dx: float = 10e-9, cpml_depth: int = 12
     g0 = lo + margin
     gk1 = g0 + glass_cells
     s.mat[g0:xr - g0, g0:yr - g0, g0:gk1] = 1
+    if metal_cells > 0:
+        s.mats.append(ade_material(3.7, 0.0, 1.38e16, 2.73e13, [(0.0, 0.0, 0.0, 0.0)] * 2, dt))
+        s.mat[:, :, :metal_cells] = len(s.mats) - 1
     dxs, dys, dzs = design_shape
     i0, j0 = xr // 2 - dxs // 2, yr // 2 - dys // 2
     box = (i0, i0 + dxs, j0, j0 + dys, gk1, gk1 + dzs)

@@ -8,9 +8,11 @@ yee.c / boundary.c of GSvit) in double precision:
 
   H half step: ystep_h (yee.c:146-265), then CPML H (boundary.c:347-519 with
                the zero planes of boundary.c:418-492);
-  E half step: ystep_e (yee.c:530-1247, no dispersive branch), the PEC rule
-               (yee.c:1138-1237), then CPML E (boundary.c:691-884 with the
-               zero planes of boundary.c:522-690).
+  E half step: ystep_e (yee.c:530-1247) with its dispersive branch (the
+               Drude + critical-point ADE of yee.c:914-1108 and the CPML inside
+               it, yee.c:950-1057, in the reference's own state P^n, P^{n-1},
+               E^{n-1}), the PEC rule (yee.c:1138-1237), then CPML E
+               (boundary.c:691-884 with the zero planes of boundary.c:522-690).
 
 The TSF corrections are field-independent sources and are left out.  The
 coefficients (get_cabs, get_db, the CPML grading) come from the oracle
@@ -41,6 +43,8 @@ def _lib():
         lib.oracle_get_cpml.restype = C.c_int
         lib.oracle_farfield_transpose.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _dp, _dp]
         lib.oracle_farfield_transpose.restype = C.c_int
+        lib.oracle_get_ade_mat.argtypes = [C.c_void_p, _ip]
+        lib.oracle_get_ade_mat.restype = C.c_int
         lib._adjoint_bound = True
     return lib
 
@@ -65,10 +69,33 @@ class LinearStep:
         self.ca, self.cb = ca.reshape(3, X, Y, Z), cb.reshape(3, X, Y, Z)
         self.da, self.db = da.reshape(X, Y, Z), db.reshape(X, Y, Z)
         fl = fl.reshape(X, Y, Z)
-        if np.any(fl & 64):
-            raise ValueError("the adjoint restatement covers non-dispersive materials only")
         self.t = [(fl & (1 << a)) != 0 for a in range(3)]          # tbc: ordinary update
         self.pec = [(fl & (8 << a)) != 0 for a in range(3)]        # zeroed by the PEC rule
+        # dispersive branch: the cells, the material whose ADE coefficients they
+        # use, per-cell coefficient arrays, and the components it forms
+        am = np.zeros(n, dtype=np.int32)
+        lib.oracle_get_ade_mat(solver.h, am.ctypes.data_as(_ip))
+        am = am.reshape(X, Y, Z)
+        self.ade = am >= 0
+        self.has_ade = bool(self.ade.any())
+        if self.has_ade:
+            mats = sc.mats
+            def coef(name, idx=None):
+                v = np.array([(getattr(m, name)[idx] if idx is not None else getattr(m, name)) for m in mats])
+                return np.where(self.ade, v[np.maximum(am, 0)], 0.0)
+            self.c0, self.c1, self.c2, self.c3 = (coef(k) for k in ("ade_c0", "ade_c1", "ade_c2", "ade_c3"))
+            self.a0, self.a1, self.a2 = (coef(k) for k in ("ade_a0", "ade_a1", "ade_a2"))
+            self.bp = [[coef(k, q) for q in range(2)] for k in ("ade_bp0", "ade_bp1", "ade_bp2", "ade_bp3", "ade_bp4")]
+            eps, sig = coef("epsilon"), coef("sigma")
+            dt = sc.dt
+            with np.errstate(divide="ignore", invalid="ignore"):
+                self.cba = np.where(self.ade, (dt / eps / self.dx) / (1 + sig * dt / 2 / eps), 0.0)
+            ii, jj, kk = np.ogrid[:X, :Y, :Z]
+            idx = (ii > 0, jj > 0, kk > 0)
+            # the ADE value is formed where the component is dispersive (tbc == 0)
+            # and its curl exists (yee.c:914-1108)
+            self.go = [self.ade & ~self.t[0] & idx[1] & idx[2], self.ade & ~self.t[1] & idx[0] & idx[2],
+                       self.ade & ~self.t[2] & idx[0] & idx[1]]
         self.cp = {}
         res = (X, X, Y, Y, Z, Z)
         for f in range(6):
@@ -96,6 +123,11 @@ class LinearStep:
         sh = {X0: (X, Y, Z), XN: (X, Y, Z), Y0: (X, Y, Z), YN: (X, Y, Z), Z0: (X, Y, Z), ZN: (X, Y, Z)}
         st = {"E": [np.zeros(self.shape) for _ in range(3)], "H": [np.zeros(self.shape) for _ in range(3)],
               "pe": {}, "ph": {}}
+        if self.has_ade:   # E^{n-1}, P_D^n, P_D^{n-1}, P_cp^n, P_cp^{n-1} per component
+            for key in ("ep", "dp", "dpp"):
+                st[key] = [np.zeros(self.shape) for _ in range(3)]
+            for key in ("p", "pp"):
+                st[key] = [[np.zeros(self.shape) for _ in range(2)] for _ in range(3)]
         for f, c in self.cp.items():
             d = c[0]
             s = (d, Y, Z) if f < 2 else (X, d, Z) if f < 4 else (X, Y, d)
@@ -119,6 +151,8 @@ class LinearStep:
         r = (slice(0, X - 1), slice(0, Y - 1), slice(None))
         hz[r] = da[r] * hz[r] + db[r] * ((ex[:X - 1, 1:, :] - ex[r]) / kyh[:, :Y - 1, :] - (ey[1:, :Y - 1, :] - ey[r]) / kxh[:X - 1])
         self._cpml_h(st, ex, ey, ez, hx, hy, hz, forward=True)
+        if self.has_ade:
+            self._ade(st, forward=True)
         # ystep_e
         kxe, kye, kze = self.kxe, self.kye, self.kze
         ca, cb, t = self.ca, self.cb, self.t
@@ -169,6 +203,8 @@ class LinearStep:
         hbx[r] -= w / kye[:, 1:, :]
         hbx[1:, :Y - 1, :] += w / kye[:, 1:, :]
         ebz[r] = np.where(t[2][r], ca[2][r] * ebz[r], ebz[r])
+        if self.has_ade:
+            self._ade(ad, forward=False)
         # H half step, reversed: zero planes and CPML H, ystep_h
         self._cpml_h(ad, ebx, eby, ebz, hbx, hby, hbz, forward=False)
         da, db = self.da, self.db
@@ -194,6 +230,170 @@ class LinearStep:
         eby[1:, :Y - 1, :] -= w / kxh[:X - 1]
         eby[r] += w / kxh[:X - 1]
         hbz[r] = da[r] * hbz[r]
+
+    # ------------------------------------------------------------------- ADE
+    def _curls(self, H):
+        """curl H of ystep_e at every cell (zero where it is not formed)."""
+        X, Y, Z = self.shape
+        hx, hy, hz = H
+        kxe, kye, kze = self.kxe, self.kye, self.kze
+        cx, cy, cz = np.zeros(self.shape), np.zeros(self.shape), np.zeros(self.shape)
+        r = (slice(None), slice(1, Y), slice(1, Z))
+        cx[r] = (hz[r] - hz[:, :Y - 1, 1:]) / kye[:, 1:, :] - (hy[r] - hy[:, 1:, :Z - 1]) / kze[:, :, 1:]
+        r = (slice(1, X), slice(None), slice(1, Z))
+        cy[r] = (hx[r] - hx[1:, :, :Z - 1]) / kze[:, :, 1:] - (hz[r] - hz[:X - 1, :, 1:]) / kxe[1:]
+        r = (slice(1, X), slice(1, Y), slice(None))
+        cz[r] = (hy[r] - hy[:X - 1, 1:, :]) / kxe[1:] - (hx[r] - hx[1:, :Y - 1, :]) / kye[:, 1:, :]
+        return cx, cy, cz
+
+    def _curls_T(self, H, w):
+        """Add the transpose of _curls applied to the weights w (3 arrays)."""
+        X, Y, Z = self.shape
+        hx, hy, hz = H
+        kxe, kye, kze = self.kxe, self.kye, self.kze
+        r = (slice(None), slice(1, Y), slice(1, Z))
+        v = w[0][r]
+        hz[r] += v / kye[:, 1:, :]
+        hz[:, :Y - 1, 1:] -= v / kye[:, 1:, :]
+        hy[r] -= v / kze[:, :, 1:]
+        hy[:, 1:, :Z - 1] += v / kze[:, :, 1:]
+        r = (slice(1, X), slice(None), slice(1, Z))
+        v = w[1][r]
+        hx[r] += v / kze[:, :, 1:]
+        hx[1:, :, :Z - 1] -= v / kze[:, :, 1:]
+        hz[r] -= v / kxe[1:]
+        hz[:X - 1, :, 1:] += v / kxe[1:]
+        r = (slice(1, X), slice(1, Y), slice(None))
+        v = w[2][r]
+        hy[r] += v / kxe[1:]
+        hy[:X - 1, 1:, :] -= v / kxe[1:]
+        hx[r] -= v / kye[:, 1:, :]
+        hx[1:, :Y - 1, :] += v / kye[:, 1:, :]
+
+    def _ade_cpml_faces(self):
+        """The psi_E updates of the CPML inside the dispersive branch
+        (yee.c:950-1057), per face: (face, cells, previous cells along the
+        normal, psi cells, (psi index, H component, [(E component, sign)]) ...).
+        The x0 corrections are scaled by cb = 0 in the reference and vanish."""
+        X, Y, Z = self.shape
+        out = []
+        for f in (X0, Y0, Z0, XN, YN, ZN):
+            if f not in self.cp:
+                continue
+            d = self.cp[f][0]
+            ax = f // 2
+            n = (X, Y, Z)[ax]
+            lo, hi = (2, d) if f in (X0, Y0, Z0) else (n - d + 1, n)
+            if hi <= lo:
+                continue
+            plo = lo if f in (X0, Y0, Z0) else lo - (n - d)
+            cells = [slice(None)] * 3
+            cells[ax] = slice(lo, hi)
+            prv = list(cells)
+            prv[ax] = slice(lo - 1, hi - 1)
+            pc = list(cells)
+            pc[ax] = slice(plo, plo + hi - lo)
+            if ax == 0:
+                pairs = ((0, 2, [] if f == X0 else [(1, -1)]), (1, 1, [] if f == X0 else [(2, +1)]))
+            elif ax == 1:
+                pairs = ((0, 2, [(0, +1)]), (1, 0, [(2, -1)]))
+            else:
+                pairs = ((1, 0, [(1, +1)]), (0, 1, [(0, -1)]))
+            out.append((f, ax, tuple(cells), tuple(prv), tuple(pc), plo, hi - lo, pairs))
+        return out
+
+    def _ade(self, st, forward):
+        """The dispersive branch of ystep_e (yee.c:914-1108) on the cells that
+        take it: the ADE value of the dispersive components, the CPML inside the
+        branch, the polarisation recursions and the state shift.  Forward: in
+        place on the state.  Adjoint (forward=False): the transpose, on the
+        adjoint state (E: adjoint of the E the ordinary update read; ep, dp, dpp,
+        p, pp: adjoints of the state after the step on entry, before it on exit)."""
+        X, Y, Z = self.shape
+        dx = self.dx
+        E, H = st["E"], st["H"]
+        m = self.ade
+        a0, a1, a2, c0, c1, c2, c3 = self.a0, self.a1, self.a2, self.c0, self.c1, self.c2, self.c3
+        bp0, bp1, bp2, bp3, bp4 = self.bp
+        faces = self._ade_cpml_faces()
+        # the corrections' gate: the two other indices > 0 and the component dispersive
+        ii, jj, kk = np.ogrid[:X, :Y, :Z]
+        pos = (ii > 0, jj > 0, kk > 0)
+        def gate(ax, b):
+            g = m & ~self.t[b]
+            for o in range(3):
+                if o != ax:
+                    g = g & pos[o]
+            return g
+        if forward:
+            curl = self._curls(H)
+            ve = [e.copy() for e in E]
+            dp0 = [x.copy() for x in st["dp"]]
+            p0 = [[x.copy() for x in y] for y in st["p"]]
+            for a in range(3):
+                v = (c0 * curl[a] / dx + c1 * (-a0 * st["dpp"][a] + (1 - a1) * st["dp"][a])
+                     + c1 * (-bp0[0] * st["pp"][a][0] + (1 - bp1[0]) * st["p"][a][0])
+                     + c1 * (-bp0[1] * st["pp"][a][1] + (1 - bp1[1]) * st["p"][a][1])
+                     + c2 * st["ep"][a] + c3 * E[a])
+                E[a][:] = np.where(self.go[a], v, E[a])
+            for f, ax, cells, prv, pc, plo, ln, pairs in faces:
+                shp = [1, 1, 1]
+                shp[ax] = ln
+                be = self.cp[f][1][plo:plo + ln].reshape(shp)
+                ce = self.cp[f][2][plo:plo + ln].reshape(shp)
+                for q, hc, corr in pairs:
+                    p = st["pe"][f][q]
+                    p[pc] = np.where(m[cells], be * p[pc] + ce * (H[hc][cells] - H[hc][prv]) / dx, p[pc])
+                    for b, sg in corr:
+                        E[b][cells] += np.where(gate(ax, b)[cells], sg * dx * self.cba[cells] * p[pc], 0.0)
+            for a in range(3):
+                st["dp"][a][:] = np.where(m, a0 * st["dpp"][a] + a1 * dp0[a] + a2 * (st["ep"][a] + 2 * ve[a] + E[a]), st["dp"][a])
+                for q in range(2):
+                    st["p"][a][q][:] = np.where(m, bp0[q] * st["pp"][a][q] + bp1[q] * p0[a][q] + bp2[q] * st["ep"][a]
+                                                + bp3[q] * ve[a] + bp4[q] * E[a], st["p"][a][q])
+                st["ep"][a][:] = np.where(m, ve[a], st["ep"][a])
+                st["dpp"][a][:] = np.where(m, dp0[a], st["dpp"][a])
+                for q in range(2):
+                    st["pp"][a][q][:] = np.where(m, p0[a][q], st["pp"][a][q])
+            return
+        # adjoint: lam1 = adjoints of (E1, ep1, dp1, dpp1, p1, pp1) on entry
+        lE1 = [np.where(m, E[a], 0.0) for a in range(3)]
+        lep1, ldp1, ldpp1 = st["ep"], st["dp"], st["dpp"]
+        lp1, lpp1 = st["p"], st["pp"]
+        tot = [lE1[a] + a2 * ldp1[a] + bp4[0] * lp1[a][0] + bp4[1] * lp1[a][1] for a in range(3)]
+        # CPML inside the branch, reversed face order
+        for f, ax, cells, prv, pc, plo, ln, pairs in reversed(faces):
+            shp = [1, 1, 1]
+            shp[ax] = ln
+            be = self.cp[f][1][plo:plo + ln].reshape(shp)
+            ce = self.cp[f][2][plo:plo + ln].reshape(shp)
+            for q, hc, corr in reversed(pairs):
+                p = st["pe"][f][q]
+                lam = p[pc].copy()
+                for b, sg in corr:
+                    lam += np.where(gate(ax, b)[cells], sg * dx * self.cba[cells] * tot[b][cells], 0.0)
+                upd = m[cells]
+                p[pc] = np.where(upd, be * lam, lam)
+                w = np.where(upd, ce * lam / dx, 0.0)
+                H[hc][cells] += w
+                H[hc][prv] -= w
+        lv = [np.where(self.go[a], tot[a], 0.0) for a in range(3)]
+        self._curls_T(H, [c0 / dx * lv[a] for a in range(3)])
+        for a in range(3):
+            pas = np.where(m & ~self.go[a], tot[a], 0.0)   # E1 = E0 where no ADE value is formed
+            lE0 = (c3 * lv[a] + pas + 2 * a2 * ldp1[a] + bp3[0] * lp1[a][0] + bp3[1] * lp1[a][1] + lep1[a])
+            lep0 = c2 * lv[a] + a2 * ldp1[a] + bp2[0] * lp1[a][0] + bp2[1] * lp1[a][1]
+            ldp0 = c1 * (1 - a1) * lv[a] + a1 * ldp1[a] + ldpp1[a]
+            ldpp0 = -c1 * a0 * lv[a] + a0 * ldp1[a]
+            lp0 = [c1 * (1 - bp1[q]) * lv[a] + bp1[q] * lp1[a][q] + lpp1[a][q] for q in range(2)]
+            lpp0 = [-c1 * bp0[q] * lv[a] + bp0[q] * lp1[a][q] for q in range(2)]
+            E[a][:] = np.where(m, lE0, E[a])
+            st["ep"][a][:] = np.where(m, lep0, 0.0)
+            st["dp"][a][:] = np.where(m, ldp0, 0.0)
+            st["dpp"][a][:] = np.where(m, ldpp0, 0.0)
+            for q in range(2):
+                st["p"][a][q][:] = np.where(m, lp0[q], 0.0)
+                st["pp"][a][q][:] = np.where(m, lpp0[q], 0.0)
 
     # ------------------------------------------------------------------ CPML
     def _cpml_h(self, st, ex, ey, ez, hx, hy, hz, forward):

@@ -1445,6 +1445,22 @@ int oracle_get_coeffs(const oracle_state *s, double *ca, double *cb, double *da,
     return 0;
 }
 
+/* The material whose ADE coefficients the dispersive branch of a cell uses
+ * (get_tbc, yee.c:454-526), or -1 where the cell is outside that branch. */
+int oracle_get_ade_mat(const oracle_state *s, int32_t *out)
+{
+    const int xr = s->xres, yr = s->yres, zr = s->zres;
+    int i, j, k;
+    for (i = 0; i < xr; i++)
+        for (j = 0; j < yr; j++)
+            for (k = 0; k < zr; k++) {
+                int xt, yt, zt;
+                const int m = get_tbc(s, i, j, k, &xt, &yt, &zt);
+                out[IDX(s, i, j, k)] = (s->nmat > 0 && s->disp && xt * yt * zt == 0) ? m : -1;
+            }
+    return 0;
+}
+
 /* CPML profiles of one face (cpml_grade): depth entries each; returns the
  * depth, 0 for a disabled face. */
 int oracle_get_cpml(const oracle_state *s, int face, double *be, double *ce, double *bh, double *ch, double *ke, double *kh)

@@ -60,6 +60,7 @@ int oracle_get_step(const oracle_state *s);
  * ca, cb: 3*N component-major; da, db: N; flags: N (bits 0-2 tbc, 3-5 PEC
  * zeroed components, 6 dispersive cell). */
 int oracle_get_coeffs(const oracle_state *s, double *ca, double *cb, double *da, double *db, int32_t *flags);
+int oracle_get_ade_mat(const oracle_state *s, int32_t *out);
 /* Transpose of the far-field series of one step (the step index its
  * far-field call saw): out[a*N + c] += sum over the far points pts of the tap
  * coefficients that read E[a][c] times lam[(p*3 + a)*ndata + m]. */

@@ -2,7 +2,9 @@
 forward step against the C oracle (bit-exact), its transpose by the
 dot-product identity <M^n x, y> = <x, (M^T)^n y>, and its gradient of the
 far-field objective against central finite differences of the oracle's own
-objective (FP64, h = 1e-4 on eps_r)."""
+objective (FP64, h = 1e-4 on eps_r) -- also with Drude / critical-point
+materials, whose dispersive branch (yee.c:914-1108, with the CPML inside it)
+the restatement steps and transposes."""
 import numpy as np
 import pytest
 
@@ -13,10 +15,40 @@ from tests._util import random_fields
 
 
 def _dot(a, b):
-    return sum(float(np.sum(a[k][c] * b[k][c])) for k in ("E", "H") for c in range(3))
+    d = sum(float(np.sum(a[k][c] * b[k][c])) for k in ("E", "H") for c in range(3))
+    for k in ("ep", "dp", "dpp"):
+        if k in a:
+            d += sum(float(np.sum(a[k][c] * b[k][c])) for c in range(3))
+    for k in ("p", "pp"):
+        if k in a:
+            d += sum(float(np.sum(a[k][c][q] * b[k][c][q])) for c in range(3) for q in range(2))
+    return d
 
 
-@pytest.mark.parametrize("kind", ["lintab", "pec"])
+def _randomise_ade(L, st, rng, scale):
+    """Random dispersive state on the cells of the dispersive branch (elsewhere
+    it is not part of the step's state)."""
+    for k in ("ep", "dp", "dpp"):
+        for c in range(3):
+            st[k][c][:] = np.where(L.ade, rng.standard_normal(L.shape) * scale, 0.0)
+    for k in ("p", "pp"):
+        for c in range(3):
+            for q in range(2):
+                st[k][c][q][:] = np.where(L.ade, rng.standard_normal(L.shape) * scale, 0.0)
+
+
+def _copy(st):
+    out = {k: [v.copy() for v in st[k]] for k in ("E", "H")}
+    for k in ("ep", "dp", "dpp"):
+        if k in st:
+            out[k] = [v.copy() for v in st[k]]
+    for k in ("p", "pp"):
+        if k in st:
+            out[k] = [[v.copy() for v in w] for w in st[k]]
+    return out
+
+
+@pytest.mark.parametrize("kind", ["lintab", "pec", "ade", "full"])
 def test_forward_restatement_is_the_oracle_step(kind):
     s = plan.small_scene(kind)
     s.tsf = None
@@ -36,14 +68,16 @@ def test_forward_restatement_is_the_oracle_step(kind):
     assert all(np.abs(p).max() > 0 for f in st["pe"] for p in st["pe"][f])
 
 
-@pytest.mark.parametrize("kind", ["pec", "design"])
+@pytest.mark.parametrize("kind", ["pec", "design", "ade", "full", "design_drude"])
 def test_transpose_dot_product(kind):
-    if kind == "pec":
-        s = plan.small_scene("pec")
+    if kind in ("pec", "ade", "full"):
+        s = plan.small_scene(kind)
         s.tsf = None
     else:
-        s = plan.adjoint_scene(shape=(32, 32, 32), cpml_depth=6, design_shape=(4, 4, 2), glass_cells=3, nsteps=10).expanded()
+        s = plan.adjoint_scene(shape=(32, 32, 32), cpml_depth=6, design_shape=(4, 4, 2), glass_cells=3, nsteps=10,
+                               metal_cells=4 if kind == "design_drude" else 0).expanded()
     L = A.LinearStep(CpuSolver(s))
+    assert L.has_ade == (kind in ("ade", "full", "design_drude"))
     rng = np.random.default_rng(1)
     x, y = L.zero_state(), L.zero_state()
     for a in range(3):
@@ -51,8 +85,10 @@ def test_transpose_dot_product(kind):
         x["H"][a][:] = rng.standard_normal(L.shape) / 377
         y["E"][a][:] = rng.standard_normal(L.shape)
         y["H"][a][:] = rng.standard_normal(L.shape) * 377
-    x0 = {k: [v.copy() for v in x[k]] for k in ("E", "H")}
-    y0 = {k: [v.copy() for v in y[k]] for k in ("E", "H")}
+    if L.has_ade:
+        _randomise_ade(L, x, rng, 1e-11)
+        _randomise_ade(L, y, rng, 1e11)
+    x0, y0 = _copy(x), _copy(y)
     for _ in range(6):
         L.forward(x)
         L.adjoint(y)
@@ -68,6 +104,22 @@ def test_gradient_vs_finite_differences_fp64():
     J, g = A.gradient(s, obj, n)
     assert J > 0
     cells = [(0, 0, 0), (1, 2, 1), (3, 3, 0), (2, 1, 1)]
+    fd = A.objective_fd(s, obj, n, cells, 1e-4)
+    ad = np.array([g[q] for q in cells])
+    assert np.max(np.abs(ad - fd) / np.abs(fd)) < 1e-6, (ad, fd)
+
+
+def test_gradient_vs_finite_differences_fp64_drude():
+    """The same with a Drude-silver layer under the glass (inside the z0 CPML
+    and across the x and y slabs): the adjoint sweep runs through the ADE
+    branch and the CPML inside it."""
+    n = 600
+    s = plan.adjoint_scene(shape=(32, 32, 32), cpml_depth=6, design_shape=(4, 4, 2), glass_cells=3, nsteps=n,
+                           pulse_delay=2e-15, pulse_width=0.7e-15, metal_cells=8)
+    obj = plan.cone_objective(s, nth=5, nph=7)
+    J, g = A.gradient(s, obj, n)
+    assert J > 0
+    cells = [(0, 0, 0), (1, 2, 1), (3, 3, 0)]
     fd = A.objective_fd(s, obj, n, cells, 1e-4)
     ad = np.array([g[q] for q in cells])
     assert np.max(np.abs(ad - fd) / np.abs(fd)) < 1e-6, (ad, fd)
