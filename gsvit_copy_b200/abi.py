@@ -27,7 +27,7 @@ ERRORS = {
 MAT_LINEAR, MAT_LINTAB, MAT_DRUDE, MAT_CP3, MAT_CP, MAT_ADE, MAT_PLRC, MAT_PEC = 0, 1, 2, 3, 4, 5, 6, 10
 MATMODE_NONE, MATMODE_ELECTRIC, MATMODE_MAGNETIC, MATMODE_FULL = 0, 1, 2, 3
 FACE_X0, FACE_XN, FACE_Y0, FACE_YN, FACE_Z0, FACE_ZN = range(6)
-STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+STORE_F32, STORE_F16, STORE_BF16, STORE_F64 = 0, 1, 2, 3
 EX, EY, EZ, HX, HY, HZ = 0x01, 0x02, 0x04, 0x08, 0x10, 0x20
 E_ALL, H_ALL = EX | EY | EZ, HX | HY | HZ
 EH = E_ALL | H_ALL

@@ -106,6 +106,15 @@ struct fdtd_plan {
     int nbulk = 0;
     bool bulk_on = false;
     BulkMaps bmaps[2];
+    // TMA tiles of the whole grid (single plans): bulk items of the interior
+    // box and the CPML tiles around it (TILE_BULK / TILE_CPXY / TILE_CPZ)
+    bool tiles_on = false;
+    BulkItem *d_tiles[3] = {nullptr, nullptr, nullptr};
+    int ntiles[3] = {0, 0, 0};
+    BulkMaps tmaps[3][2];
+    std::vector<BulkItem> h_tiles[3];     // host copies of the tile lists (batched launches)
+    int stall = 0;                        // tests: expire every CTA's first wait after this many polls
+    double tile_bytes[3] = {0, 0, 0};     // algorithmic HBM bytes per launch of each tile kind
     int *d_err = nullptr;                 // set by a bulk CTA whose bounded wait expired
     const int *batch_err = nullptr;       // the batch's error word, for an instance of a batch
     bool failed = false;                  // an expired wait was reported: the plan only accepts destroy
@@ -175,13 +184,32 @@ DevPlan plan_for(const fdtd_plan *P, int in)
     return d;
 }
 
-// the Yee/CPML/TSF/ADE part of one step: general items + bulk items
+// one launch of the tile kernel of `kind` (TILE_*) for this step's parity
+int launch_tile_kind(fdtd_plan *P, const DevPlan &d, int in, int kind, cudaStream_t st)
+{
+    const cudaError_t e = launch_tiles(kind, d, P->tmaps[kind][in], P->d_tiles[kind], P->ntiles[kind], P->d_err,
+                                       P->hp.has_ade, P->hp.maxpoles, P->storage, P->stall, st);
+    if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("tile step launch: ") + cudaGetErrorString(e));
+    return FDTD_OK;
+}
+
+// the Yee/CPML/TSF/ADE part of one step: the TMA tiles (bulk, then the CPML
+// tiles; they touch disjoint cells and read only the input set), or, for
+// plans without them, the bulk box and the slab kernels
 int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
 {
     DevPlan d = plan_for(P, in);
     cudaError_t e;
+    if (P->tiles_on) {
+        for (int kind = 0; kind < 3; kind++) {
+            const int rc = launch_tile_kind(P, d, in, kind, st);
+            if (rc != FDTD_OK) return rc;
+        }
+        return FDTD_OK;
+    }
     if (P->bulk_on) {   // first: the slab E update reads H^{n+1/2} the bulk kernel wrote next to the slabs
-        e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
+        e = launch_tiles(TILE_BULK, d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles,
+                         P->storage, 0, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
     }
     e = launch_slab_steps(d, P->slabs, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
@@ -245,6 +273,60 @@ std::vector<BulkItem> bulk_items(const int lo[3], const int hi[3], int len, int 
 
 int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool pole_arrays);
 
+// The largest run [a, b) of indices along one axis whose cells take the plain
+// update (hp.ike/ikh of 1, outside the CPML psi ranges of boundary.c:347-519
+// and 691-884, off the edge planes).  H is special below depth - 1 and from
+// res - depth + 1 up, E below depth and from res - depth + 1 up; both at the
+// first and last index.
+void plain_run(const HostPlan &hp, int ax, int R, int *a, int *b, bool *hplain_below)
+{
+    const fdtd_cpml_face &lo = hp.cp[2 * ax], &hi = hp.cp[2 * ax + 1];
+    auto hpl = [&](int q) {
+        if (q < 0 || q >= R - 1) return false;
+        if (lo.enabled && q < lo.depth - 1) return false;
+        if (hi.enabled && q >= R - hi.depth + 1) return false;
+        return hp.ikh[ax][q] == 1.0f;
+    };
+    auto epl = [&](int q) {
+        if (q <= 0 || q >= R - 1) return false;
+        if (lo.enabled && q < lo.depth) return false;
+        if (hi.enabled && q >= R - hi.depth + 1) return false;
+        return hp.ike[ax][q] == 1.0f;
+    };
+    int ba = 0, bb = 0;
+    for (int q = 0; q < R;) {
+        if (!(hpl(q) && epl(q))) { q++; continue; }
+        int e = q;
+        while (e < R && hpl(e) && epl(e)) e++;
+        if (e - q > bb - ba) { ba = q; bb = e; }
+        q = e;
+    }
+    *a = ba;
+    *b = bb;
+    *hplain_below = ba > 0 && hpl(ba - 1);
+}
+
+// planes [a0, a1) cut into chunks of about `target` planes
+std::vector<std::pair<int, int>> plane_chunks(int a0, int a1, int target)
+{
+    std::vector<std::pair<int, int>> out;
+    if (a1 <= a0) return out;
+    const int nch = std::max(1, (a1 - a0 + target - 1) / target);
+    const int len = (a1 - a0 + nch - 1) / nch;
+    for (int i = a0; i < a1; i += len) out.push_back({i, std::min(a1, i + len)});
+    return out;
+}
+
+// (j,k) tiles of [jlo, jhi) x [klo, khi) with tj x tk own cells, over the plane chunks
+void push_tiles(std::vector<BulkItem> &v, const std::vector<std::pair<int, int>> &ch, int jlo, int jhi, int klo, int khi,
+                int tj, int tk)
+{
+    if (jlo >= jhi || klo >= khi) return;
+    for (const auto &c : ch)
+        for (int j0 = jlo; j0 < jhi; j0 += tj)
+            for (int k0 = klo; k0 < khi; k0 += tk) v.push_back({j0, k0, c.first, c.second, jhi, khi, 0, 0});
+}
+
 template <class T>
 cudaError_t upload(DevBuf &m, T **dst, const T *src, size_t count)
 {
@@ -267,6 +349,106 @@ namespace {
 
 // pole_arrays: allocate the critical-point state even for a Drude-only plan,
 // so that a batched launch may run it with the two-pole kernel variant
+// Work lists of the TMA tile kernels for a single plan.  The interior box
+// (every index plain on every axis, the bulk tile's halo row, group and plane
+// plain for H) goes to the bulk layout; the rest of the grid to the CPML
+// layouts: whole planes of the x slabs and rows of the y slabs in 15 x 60
+// tiles, the z slabs between the y slabs in 31 x 28 tiles.  The y and z
+// extents are rounded out to whole CPML tiles, so that every CPML tile is full
+// except at the grid's far edges.  Sets DevPlan::plo/phi, uploads the lists
+// and encodes the tensor maps of the three layouts.
+int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls)
+{
+    const int X = hp.xr, Y = hp.yr, Z = hp.zr;
+    const int R[3] = {X, Y, Z};
+    int a[3], b[3];
+    bool below[3];
+    for (int ax = 0; ax < 3; ax++) {
+        plain_run(hp, ax, R[ax], &a[ax], &b[ax], &below[ax]);
+        d.plo[ax] = a[ax];
+        d.phi[ax] = b[ax];
+    }
+    // bulk box: H of the plane / row below its first one must be plain too; k
+    // bounds multiples of 4 with a plain 4-cell halo group below
+    int lo[3], hi[3];
+    for (int ax = 0; ax < 3; ax++) {
+        lo[ax] = below[ax] ? a[ax] : a[ax] + 1;
+        hi[ax] = b[ax];
+    }
+    lo[2] = (lo[2] + 3) / 4 * 4;
+    while (lo[2] < hi[2] && !(lo[2] - 4 >= a[2] - (below[2] ? 1 : 0))) lo[2] += 4;
+    hi[2] = hi[2] / 4 * 4;
+    int bi0 = lo[0], bi1 = hi[0];
+    int bj0 = (lo[1] + CPXY_TJ - 1) / CPXY_TJ * CPXY_TJ, bj1 = Y - (Y - hi[1] + CPXY_TJ - 1) / CPXY_TJ * CPXY_TJ;
+    int bk0 = (lo[2] + CPZ_TK - 1) / CPZ_TK * CPZ_TK, bk1 = Z - (Z - hi[2] + CPZ_TK - 1) / CPZ_TK * CPZ_TK;
+    const bool bulk = bi0 < bi1 && bj0 < bj1 && bk0 < bk1 && hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];
+    std::vector<BulkItem> it[3];
+    // planes per item: about 10 in the bulk (neighbouring tiles then share
+    // their halo rows in L2; 512^3 rough surface, bulk kernel 2.24 ms at 96
+    // planes, 1.72 ms at 8-12, 1.79 ms at 4), whole x slabs, 16 in the y and z
+    // CPML tiles
+    if (bulk) {
+        push_tiles(it[TILE_BULK], plane_chunks(bi0, bi1, 10), bj0, bj1, bk0, bk1, BULK_TJ, BULK_TK);
+        const auto xs0 = plane_chunks(0, bi0, 1 << 30), xs1 = plane_chunks(bi1, X, 1 << 30);
+        push_tiles(it[TILE_CPXY], xs0, 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
+        push_tiles(it[TILE_CPXY], xs1, 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
+        const auto mid = plane_chunks(bi0, bi1, 16);
+        push_tiles(it[TILE_CPXY], mid, 0, bj0, 0, Z, CPXY_TJ, CPXY_TK);
+        push_tiles(it[TILE_CPXY], mid, bj1, Y, 0, Z, CPXY_TJ, CPXY_TK);
+        push_tiles(it[TILE_CPZ], mid, bj0, bj1, 0, bk0, CPZ_TJ, CPZ_TK);
+        push_tiles(it[TILE_CPZ], mid, bj0, bj1, bk1, Z, CPZ_TJ, CPZ_TK);
+    } else {
+        bi0 = bi1 = bj0 = bj1 = bk0 = bk1 = 0;
+        push_tiles(it[TILE_CPXY], plane_chunks(0, X, 16), 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
+    }
+    // algorithmic bytes per launch: fields 12 x esz + class byte per cell, the
+    // dispersive state of dispersive components, 4 psi values read and written
+    // per CPML cell (psi arrays, charged to the CPML tiles)
+    const double esz = (double)P->esz;
+    auto box_bytes = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
+        double bsum = 0;
+        if (i0 >= i1 || j0 >= j1 || k0 >= k1) return bsum;
+#pragma omp parallel for reduction(+ : bsum) schedule(static)
+        for (int i = i0; i < i1; i++)
+            for (int j = j0; j < j1; j++)
+                for (int k = k0; k < k1; k++) {
+                    const DevClass &c = hp.classes[hp.cls[((size_t)i * Y + j) * Z + k]];
+                    bsum += 12.0 * esz + 1.0;
+                    if (c.flags & CF_ADE_BRANCH)
+                        bsum += (((c.flags & CF_ADE_X) ? 1 : 0) + ((c.flags & CF_ADE_Y) ? 1 : 0) + ((c.flags & CF_ADE_Z) ? 1 : 0)) *
+                                (8.0 + esz + 16.0 * hp.maxpoles);
+                }
+        return bsum;
+    };
+    double psi = 0;
+    for (int f = 0; f < 6; f++)
+        if (hp.cp[f].enabled) {
+            const int dep = hp.cp[f].depth;
+            psi += ((f < 2) ? (double)dep * Y * Z : (f < 4) ? (double)X * dep * Z : (double)X * Y * dep) * 4 * 2.0 * esz;
+        }
+    const double all = box_bytes(0, X, 0, Y, 0, Z);
+    P->tile_bytes[TILE_BULK] = box_bytes(bi0, bi1, bj0, bj1, bk0, bk1);
+    P->tile_bytes[TILE_CPZ] = box_bytes(bi0, bi1, bj0, bj1, 0, bk0) + box_bytes(bi0, bi1, bj0, bj1, bk1, Z);
+    P->tile_bytes[TILE_CPXY] = all - P->tile_bytes[TILE_BULK] - P->tile_bytes[TILE_CPZ] + psi;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || !fn || q != cudaDriverEntryPointSuccess) return fail(FDTD_E_CUDA, "cuTensorMapEncodeTiled entry point");
+    for (int kind = 0; kind < 3; kind++) {
+        P->ntiles[kind] = (int)it[kind].size();
+        P->h_tiles[kind] = it[kind];
+        if (it[kind].empty()) continue;
+        e = upload(P->mem, &P->d_tiles[kind], it[kind].data(), it[kind].size());
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("tile work lists: ") + cudaGetErrorString(e));
+        for (int sset = 0; sset < 2; sset++)
+            if (tile_make_maps(kind, fn, d, P->fields[sset], cls, d.cpitch, P->storage, &P->tmaps[kind][sset]) != 0)
+                return fail(FDTD_E_CUDA, "tensor map encoding");
+    }
+    e = bulk_configure();
+    if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("tile kernel shared memory: ") + cudaGetErrorString(e));
+    return FDTD_OK;
+}
+
 int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool pole_arrays)
 {
     if (!out) return fail(FDTD_E_INVALID, "out is NULL");
@@ -283,7 +465,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     HostPlan &hp = P->hp;
     if (pole_arrays && hp.has_ade) hp.maxpoles = 2;
     P->storage = desc->storage;
-    P->esz = (desc->storage == FDTD_STORE_F32) ? 4 : 2;
+    P->esz = desc->storage == FDTD_STORE_F32 ? 4 : desc->storage == FDTD_STORE_F64 ? 8 : 2;
     const size_t esz = P->esz;
     P->device = device;
     cudaError_t ce = cudaSetDevice(device);
@@ -295,6 +477,12 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         return fail(e == cudaErrorMemoryAllocation ? FDTD_E_NOMEM : FDTD_E_CUDA,
                     std::string(what) + ": " + cudaGetErrorString(e));
     };
+    auto bail_rc = [&](int rc) {   // the error text is already set
+        P->mem.free_all();
+        if (P->own_stream) cudaStreamDestroy(P->own_stream);
+        delete P;
+        return rc;
+    };
 #define CA(x, what) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return bail(e_, what); } while (0)
     CA(cudaStreamCreateWithFlags(&P->own_stream, cudaStreamNonBlocking), "stream");
     P->stream = P->own_stream;
@@ -305,13 +493,25 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     d.sj = hp.zr;
     d.si = (int64_t)hp.yr * hp.zr;
     d.dx = (float)hp.dx;
+    d.dxd = hp.dx;
+    const bool r64 = P->storage == FDTD_STORE_F64;   // FP64 fields, state, tables and arithmetic
+    d.real64 = r64 ? 1 : 0;
+    const size_t rsz = r64 ? 8 : 4;                  // element size of the ADE state and the tables
+    // an FP64 table (r64) or its FP32 twin, uploaded behind a float pointer
+    auto upload_tab = [&](float **dst, const std::vector<float> &f32, const std::vector<double> &f64) {
+        if (!r64) return upload(P->mem, dst, f32.data(), f32.size());
+        double *q = nullptr;
+        cudaError_t e = upload(P->mem, &q, f64.data(), f64.size());
+        *dst = reinterpret_cast<float *>(q);
+        return e;
+    };
     // 16-bit storage scales, chosen so that every stored value of a field of
     // unit amplitude is of order one: H ~ E / Z0 (Z0 = 377 ohm) is stored
     // times 2^9; psi_H accumulates dE/dx ~ E / dx and is stored times the
     // power of two nearest dx; psi_E accumulates dH/dx and is stored times
     // that and 2^9.  Powers of two make scaling and unscaling exact.
     d.hs = 1.f; d.ihs = 1.f; d.ps = 1.f; d.ips = 1.f; d.pse = 1.f; d.ipse = 1.f;
-    if (P->storage != FDTD_STORE_F32) {
+    if (P->storage == FDTD_STORE_F16 || P->storage == FDTD_STORE_BF16) {
         const int e2 = std::max(-100, std::min(100, (int)std::lround(std::log2(hp.dx))));
         d.hs = 512.f;
         d.ihs = 1.f / 512.f;
@@ -337,29 +537,42 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         d.cpitch = pitch;
     }
     d.cls = cls;
-    DevClass *classes;
-    CA(upload(P->mem, &classes, hp.classes.data(), hp.classes.size()), "class table");
-    d.classes = classes;
+    if (r64) {
+        DevClass64 *classes;
+        CA(upload(P->mem, &classes, hp.classes64.data(), hp.classes64.size()), "class table");
+        d.classes = reinterpret_cast<const DevClass *>(classes);
+    } else {
+        DevClass *classes;
+        CA(upload(P->mem, &classes, hp.classes.data(), hp.classes.size()), "class table");
+        d.classes = classes;
+    }
     d.nclasses = (int)hp.classes.size();
     if (hp.design) {
         float *dc;
-        CA(upload(P->mem, &dc, hp.dcoef.data(), hp.dcoef.size()), "design coefficients");
+        CA(upload_tab(&dc, hp.dcoef, hp.dcoef64), "design coefficients");
         d.dcoef = dc;
         for (int q = 0; q < 6; q++) d.dbox[q] = hp.abox[q];
     }
     double bytes = (12.0 * esz + 1.0) * (double)n;   // 6 field reads + 6 writes + class byte
     if (hp.has_ade) {
-        DevAde *ade;
-        CA(upload(P->mem, &ade, hp.ades.data(), hp.ades.size()), "ADE table");
-        d.ade = ade;
+        if (r64) {
+            DevAde64 *ade;
+            CA(upload(P->mem, &ade, hp.ades64.data(), hp.ades64.size()), "ADE table");
+            d.ade = reinterpret_cast<const DevAde *>(ade);
+        } else {
+            DevAde *ade;
+            CA(upload(P->mem, &ade, hp.ades.data(), hp.ades.size()), "ADE table");
+            d.ade = ade;
+        }
         d.nade = (int)hp.ades.size();
+        const size_t nst = n * rsz / 4;   // state array in float units
         for (int a = 0; a < 3; a++) {
-            CA(P->mem.alloc(&d.q[a], n), "ADE state");
-            P->snap.push_back({d.q[a], n * 4});
+            CA(P->mem.alloc(&d.q[a], nst), "ADE state");
+            P->snap.push_back({d.q[a], n * rsz});
             for (int q = 0; q < hp.maxpoles; q++) {
-                CA(P->mem.alloc(&d.pc[a][q], n), "ADE state");
-                CA(P->mem.alloc(&d.qc[a][q], n), "ADE state");
-                P->snap.push_back({d.pc[a][q], n * 4}); P->snap.push_back({d.qc[a][q], n * 4});
+                CA(P->mem.alloc(&d.pc[a][q], nst), "ADE state");
+                CA(P->mem.alloc(&d.qc[a][q], nst), "ADE state");
+                P->snap.push_back({d.pc[a][q], n * rsz}); P->snap.push_back({d.qc[a][q], n * rsz});
             }
         }
         size_t nd = 0;   // dispersive components: Q read + written (8 B), E^{n-1} read, + 16 B per pole (p, q)
@@ -368,7 +581,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             if (k.flags & CF_ADE_BRANCH)
                 nd += ((k.flags & CF_ADE_X) ? 1 : 0) + ((k.flags & CF_ADE_Y) ? 1 : 0) + ((k.flags & CF_ADE_Z) ? 1 : 0);
         }
-        bytes += (double)nd * (8.0 + esz + 16.0 * hp.maxpoles);
+        bytes += (double)nd * (2.0 * rsz + esz + 4.0 * rsz * hp.maxpoles);
     }
     // CPML
     for (int f = 0; f < 6; f++) {
@@ -377,10 +590,10 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         if (!hp.cp[f].enabled) continue;
         const int dep = hp.cp[f].depth;
         float *be, *ce, *bh, *ch;
-        CA(upload(P->mem, &be, hp.be[f].data(), dep), "cpml");
-        CA(upload(P->mem, &ce, hp.ce[f].data(), dep), "cpml");
-        CA(upload(P->mem, &bh, hp.bh[f].data(), dep), "cpml");
-        CA(upload(P->mem, &ch, hp.ch[f].data(), dep), "cpml");
+        CA(upload_tab(&be, hp.be[f], hp.be64[f]), "cpml");
+        CA(upload_tab(&ce, hp.ce[f], hp.ce64[f]), "cpml");
+        CA(upload_tab(&bh, hp.bh[f], hp.bh64[f]), "cpml");
+        CA(upload_tab(&ch, hp.ch[f], hp.ch64[f]), "cpml");
         d.be[f] = be; d.ce[f] = ce; d.bh[f] = bh; d.ch[f] = ch;
         size_t cnt = (f < 2) ? (size_t)dep * hp.yr * hp.zr : (f < 4) ? (size_t)hp.xr * dep * hp.zr : (size_t)hp.xr * hp.yr * dep;
         for (int q = 0; q < 2; q++) {
@@ -395,8 +608,8 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     }
     for (int ax = 0; ax < 3; ax++) {
         float *a, *b;
-        CA(upload(P->mem, &a, hp.ike[ax].data(), hp.ike[ax].size()), "kappa");
-        CA(upload(P->mem, &b, hp.ikh[ax].data(), hp.ikh[ax].size()), "kappa");
+        CA(upload_tab(&a, hp.ike[ax], hp.ike64[ax]), "kappa");
+        CA(upload_tab(&b, hp.ikh[ax], hp.ikh64[ax]), "kappa");
         d.ike[ax] = a;
         d.ikh[ax] = b;
     }
@@ -418,8 +631,8 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             uint8_t *m;
             CA(upload(P->mem, &m, hp.tmap[f].data(), hp.tmap[f].size()), "tsf map");
             d.tmap[f] = m;
-            CA(P->mem.alloc(&d.tcor_h[f], hp.tmap[f].size()), "tsf corrections");
-            CA(P->mem.alloc(&d.tcor_e[f], hp.tmap[f].size()), "tsf corrections");
+            CA(P->mem.alloc(&d.tcor_h[f], hp.tmap[f].size() * rsz / 4), "tsf corrections");   // float2 / double2
+            CA(P->mem.alloc(&d.tcor_e[f], hp.tmap[f].size() * rsz / 4), "tsf corrections");
             d.tnb[f] = hp.tmap_dims[f][1];
             P->tsf_cells += (int)hp.tmap[f].size();
         }
@@ -558,10 +771,10 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             const size_t nacc = (size_t)f.nfreq * 6 * cell.size();
             CA(P->mem.alloc(&acc, nacc), "nfff accumulators");
             P->snap.push_back({acc, nacc * sizeof(double2)});
-            float *ring;   // samples not yet folded into acc: part of the state
+            float *ring;   // samples not yet folded into acc: part of the state (FP64 for r64 plans)
             const size_t nring = (size_t)NFFF_RING * 9 * cell.size();
-            CA(P->mem.alloc(&ring, nring), "nfff sample ring");
-            P->snap.push_back({ring, nring * sizeof(float)});
+            CA(P->mem.alloc(&ring, nring * rsz / 4), "nfff sample ring");
+            P->snap.push_back({ring, nring * rsz});
             P->nf.ring = ring;
             CA(P->mem.alloc(&outp, (size_t)f.npoints * f.nfreq * 3), "nfff output");
             // exp(-i omega R dt) over every retarded index R the box can produce:
@@ -657,7 +870,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         lo[2] = std::max(4, (lo[2] + 3) / 4 * 4);   // the k halo group k0-4..k0-1 stays in the grid
         hi[2] = hi[2] / 4 * 4;
         const char *nob = getenv("GSVIT_B200_NO_BULK");
-        P->bulk_on = !hp.design && ((size_t)Z * esz % 16 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
+        P->bulk_on = !hp.design && !r64 && ((size_t)Z * esz % 16 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
         std::vector<SlabBox> boxes;
         std::vector<BulkItem> blk;
         long long nblk = 0;
@@ -816,10 +1029,19 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             CA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q), "driver entry point");
             if (!fn || q != cudaDriverEntryPointSuccess) return bail(cudaErrorNotSupported, "cuTensorMapEncodeTiled");
             for (int sset = 0; sset < 2; sset++)
-                if (bulk_make_maps(fn, d, P->fields[sset], cls, d.cpitch, P->storage, &P->bmaps[sset]) != 0)
+                if (tile_make_maps(TILE_BULK, fn, d, P->fields[sset], cls, d.cpitch, P->storage, &P->bmaps[sset]) != 0)
                     return bail(cudaErrorInvalidValue, "tensor map encoding");
             // the largest layout (256 classes), so that any plan or batch may launch
             CA(bulk_configure(), "bulk kernel shared memory");
+        }
+        // TMA tiles over the whole grid (single plans; batches may use them too)
+        P->tiles_on = !hp.design && !r64 && ((size_t)Z * esz % 16 == 0) && !(nob && nob[0] == '1');
+        // test hook of the bounded-wait error path: every tile CTA of this plan
+        // also waits, at most this many polls, on an mbarrier nothing arrives on
+        if (const char *stv = getenv("GSVIT_B200_STALL_TEST")) P->stall = std::max(0, atoi(stv));
+        if (P->tiles_on) {
+            int rc = build_tiles(P, hp, d, cls);
+            if (rc != FDTD_OK) return bail_rc(rc);
         }
     }
     P->step_bytes = bytes;
@@ -870,6 +1092,12 @@ int upload_comp(fdtd_plan *P, int c, const float *src, bool sync)
         if (sync) CK(cudaStreamSynchronize(P->stream));
         return FDTD_OK;
     }
+    if (P->storage == FDTD_STORE_F64) {
+        std::vector<double> w(src, src + n);
+        CK(cudaMemcpyAsync(P->fields[P->cur][c], w.data(), n * 8, cudaMemcpyHostToDevice, P->stream));
+        CK(cudaStreamSynchronize(P->stream));
+        return FDTD_OK;
+    }
     std::vector<uint16_t> tmp(n);
     pack_storage(P->storage, c >= 3 ? P->dp.hs : 1.f, src, n, tmp.data());
     CK(cudaMemcpyAsync(P->fields[P->cur][c], tmp.data(), n * 2, cudaMemcpyHostToDevice, P->stream));
@@ -884,6 +1112,13 @@ int download_comp(fdtd_plan *P, int c, float *dst)
     const size_t n = P->hp.n;
     if (P->storage == FDTD_STORE_F32) {
         CK(cudaMemcpyAsync(dst, P->fields[P->cur][c], n * 4, cudaMemcpyDeviceToHost, P->stream));
+        return FDTD_OK;
+    }
+    if (P->storage == FDTD_STORE_F64) {
+        std::vector<double> w(n);
+        CK(cudaMemcpyAsync(w.data(), P->fields[P->cur][c], n * 8, cudaMemcpyDeviceToHost, P->stream));
+        CK(cudaStreamSynchronize(P->stream));
+        for (size_t q = 0; q < n; q++) dst[q] = (float)w[q];
         return FDTD_OK;
     }
     std::vector<uint16_t> tmp(n);
@@ -929,6 +1164,15 @@ int fdtd_set_fields(fdtd_plan *P, int mask, const double *const comps[6])
 {
     if (!P || !comps) return fail(FDTD_E_INVALID, "NULL argument");
     CK(cudaSetDevice(P->device));
+    if (P->storage == FDTD_STORE_F64) {   // no rounding: the doubles as they are
+        for (int c = 0; c < 6; c++) {
+            if (!(mask & (1 << c))) continue;
+            if (!comps[c]) return fail(FDTD_E_INVALID, "selected component pointer is NULL");
+            CK(cudaMemcpyAsync(P->fields[P->cur][c], comps[c], P->hp.n * 8, cudaMemcpyHostToDevice, P->stream));
+        }
+        CK(cudaStreamSynchronize(P->stream));
+        return FDTD_OK;
+    }
     std::vector<float> tmp(P->hp.n);
     for (int c = 0; c < 6; c++) {
         if (!(mask & (1 << c))) continue;
@@ -951,7 +1195,12 @@ int fdtd_set_design_eps(fdtd_plan *P, const double *eps_r)
     CK(cudaSetDevice(P->device));
     CK(cudaStreamSynchronize(P->stream));
     design_coefficients(&P->hp, eps_r);
-    CK(cudaMemcpy(const_cast<float *>(P->dp.dcoef), P->hp.dcoef.data(), P->hp.dcoef.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (P->storage == FDTD_STORE_F64)
+        CK(cudaMemcpy(const_cast<float *>(P->dp.dcoef), P->hp.dcoef64.data(), P->hp.dcoef64.size() * sizeof(double),
+                      cudaMemcpyHostToDevice));
+    else
+        CK(cudaMemcpy(const_cast<float *>(P->dp.dcoef), P->hp.dcoef.data(), P->hp.dcoef.size() * sizeof(float),
+                      cudaMemcpyHostToDevice));
     return FDTD_OK;
 }
 
@@ -986,6 +1235,15 @@ int fdtd_get_fields(fdtd_plan *P, int mask, double *const comps[6])
 {
     if (!P || !comps) return fail(FDTD_E_INVALID, "NULL argument");
     CK(cudaSetDevice(P->device));
+    if (P->storage == FDTD_STORE_F64) {
+        for (int c = 0; c < 6; c++) {
+            if (!(mask & (1 << c))) continue;
+            if (!comps[c]) return fail(FDTD_E_INVALID, "selected component pointer is NULL");
+            CK(cudaMemcpyAsync(comps[c], P->fields[P->cur][c], P->hp.n * 8, cudaMemcpyDeviceToHost, P->stream));
+        }
+        CK(cudaStreamSynchronize(P->stream));
+        return device_error(P);
+    }
     std::vector<float> tmp(P->hp.n);
     for (int c = 0; c < 6; c++) {
         if (!(mask & (1 << c))) continue;
@@ -1062,7 +1320,8 @@ int fdtd_step_static_scratch(fdtd_plan *P, int nsteps)
     size_t used = 0;
     if (P->tsf_cells) {
         for (int f = 0; f < 6; f++) {
-            const size_t bytes = (P->hp.tmap[f].size() * sizeof(float2) + 255) & ~(size_t)255;
+            const size_t esz2 = P->storage == FDTD_STORE_F64 ? sizeof(double2) : sizeof(float2);
+            const size_t bytes = (P->hp.tmap[f].size() * esz2 + 255) & ~(size_t)255;
             if (used + 2 * bytes > FDTD_STATIC_SCRATCH_BYTES)
                 return fail(FDTD_E_UNSUPPORTED, "the TSF face tables of this plan need more than the "
                                                 "FDTD_STATIC_SCRATCH_BYTES (32 MiB) of static scratch");
@@ -1204,13 +1463,23 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
         if (P->tsf_cells) launch_tsf_faces(P->dp, P->tsf_cells, st);
         CK(cudaEventRecord(E[1], st));
         DevPlan d = plan_for(P, in);
-        if (P->bulk_on) {
-            cudaError_t e = launch_bulk(d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
-            if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
+        if (P->tiles_on) {
+            int rc = launch_tile_kind(P, d, in, TILE_BULK, st);
+            if (rc != FDTD_OK) return rc;
+            CK(cudaEventRecord(E[2], st));
+            rc = launch_tile_kind(P, d, in, TILE_CPXY, st);
+            if (rc == FDTD_OK) rc = launch_tile_kind(P, d, in, TILE_CPZ, st);
+            if (rc != FDTD_OK) return rc;
+        } else {
+            if (P->bulk_on) {
+                cudaError_t e = launch_tiles(TILE_BULK, d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade,
+                                             P->hp.maxpoles, P->storage, 0, st);
+                if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
+            }
+            CK(cudaEventRecord(E[2], st));
+            cudaError_t e = launch_slab_steps(d, P->slabs, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
+            if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
         }
-        CK(cudaEventRecord(E[2], st));
-        cudaError_t e = launch_slab_steps(d, P->slabs, P->hp.has_ade, P->hp.maxpoles, P->storage, st);
-        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
         CK(cudaEventRecord(E[3], st));
         launch_nfff(P, in, st);
         CK(cudaEventRecord(E[4], st));
@@ -1232,15 +1501,22 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
     }
     for (auto &e : ev) cudaEventDestroy(e);
     out[0] = bulk;
-    out[1] = P->bulk_bytes;
     out[2] = slab;
-    out[3] = P->slab_bytes;
     out[4] = aux;
     out[5] = nf;
     out[6] = tot;
-    const SlabLists &L = P->slabs;   // slab H, then E over the dispersive and the plain runs
-    const int nslab = L.hblocks > 0 ? 1 + (L.eblocks > 0 ? 1 : 0) + (L.epblocks > 0 ? 1 : 0) : 0;
-    out[7] = 1 + (P->tsf_cells ? 1 : 0) + (P->bulk_on ? 1 : 0) + nslab + (P->nfff_nfreq > 0 ? 1 : 0) + (P->nfff_series ? 1 : 0);
+    int nyee;
+    if (P->tiles_on) {
+        out[1] = P->tile_bytes[TILE_BULK];
+        out[3] = P->tile_bytes[TILE_CPXY] + P->tile_bytes[TILE_CPZ];
+        nyee = (P->ntiles[TILE_BULK] > 0) + (P->ntiles[TILE_CPXY] > 0) + (P->ntiles[TILE_CPZ] > 0);
+    } else {
+        out[1] = P->bulk_bytes;
+        out[3] = P->slab_bytes;
+        const SlabLists &L = P->slabs;   // slab H, then E over the dispersive and the plain runs
+        nyee = (P->bulk_on ? 1 : 0) + (L.hblocks > 0 ? 1 + (L.eblocks > 0 ? 1 : 0) + (L.epblocks > 0 ? 1 : 0) : 0);
+    }
+    out[7] = 1 + (P->tsf_cells ? 1 : 0) + nyee + (P->nfff_nfreq > 0 ? 1 : 0) + (P->nfff_series ? 1 : 0);
     return FDTD_OK;
 }
 
@@ -1521,6 +1797,8 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
     for (int q = 1; q < nplans; q++)
         if (descs[q].storage != descs[0].storage)
             return fail(FDTD_E_UNSUPPORTED, "the instances of a batch must share one field storage type");
+    if (nplans > 0 && descs[0].storage == FDTD_STORE_F64)
+        return fail(FDTD_E_UNSUPPORTED, "FP64 storage is not available in a batch");
     fdtd_batch *B = new (std::nothrow) fdtd_batch();
     if (!B) return fail(FDTD_E_NOMEM, "host allocation failed");
     B->device = device;

@@ -1,4 +1,5 @@
-// fdtd_bulk.cuh -- TMA-staged bulk kernel (fdtd_bulk.cu).
+// fdtd_bulk.cuh -- TMA-staged tile kernels (fdtd_bulk.cu): the bulk of the grid
+// and the CPML tiles around it.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -6,30 +7,50 @@
 
 #include "fdtd_internal.h"
 
-// tensor maps of the input field set and of the class map
+// tensor maps of the input field set and of the class map (box shapes of one
+// tile layout)
 struct BulkMaps {
     CUtensorMap e[3];
     CUtensorMap h[3];
     CUtensorMap cls;
 };
 
-// one CTA: own cells [j0, min(j0+15, jhi)) x [k0, min(k0+60, khi)) of planes [ib, ie)
+// one CTA: own cells [j0, min(j0+TJ, jhi)) x [k0, min(k0+TK, khi)) of planes [ib, ie)
 struct BulkItem {
     int j0, k0, ib, ie, jhi, khi, inst, pad0;   // inst: plan of the item in a batched launch
 };
 
-// own rows and columns of a tile; the bulk box has 1 <= lo, hi <= res - 1 on
-// every axis and its k bounds (hence k0 and khi) are multiples of 4
+// Tile layouts: own rows (TJ) and own k cells (TK) of one CTA of 256 threads.
+//  bulk  15 x 60: the interior box, where every cell takes the plain update
+//        (no CPML, kappa 1, no edge rule);
+//  cpxy  15 x 60: the x slabs (whole planes) and the y slabs;
+//  cpz   31 x 28: the z slabs between the y slabs.
+// The CPML tiles run the plain update on their plain cells and the special
+// path of fdtd_cells.cuh (psi, kappa, zeroed planes, ADE-in-CPML, edges) on
+// the rest.  k0 and khi are multiples of 4 in every layout.
 #define BULK_TJ 15
 #define BULK_TK 60
+#define CPXY_TJ 15
+#define CPXY_TK 60
+#define CPZ_TJ 31
+#define CPZ_TK 28
 
-size_t bulk_smem_bytes(int nclasses, int storage);
+enum { TILE_BULK = 0, TILE_CPXY = 1, TILE_CPZ = 2 };
+
+size_t tile_smem_bytes(int kind, int nclasses, int storage);
 cudaError_t bulk_configure();
-cudaError_t launch_bulk(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade,
-                        int npoles, int storage, cudaStream_t st);
-// all items of many plans in one persistent launch of `grid` CTAs; plans and
-// maps are device tables of this step's parity, indexed by BulkItem::inst
+// `stall` > 0 (tests only): every CTA also waits, at most `stall` polls, on an
+// mbarrier nothing arrives on, so that its bounded-wait error path runs
+cudaError_t launch_tiles(int kind, const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err,
+                         bool ade, int npoles, int storage, int stall, cudaStream_t st);
+// all bulk items of many plans in one persistent launch of `grid` CTAs (bulk
+// layout); plans and maps are device tables of this step's parity, indexed by
+// BulkItem::inst
 cudaError_t launch_bulk_batch(const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems, int grid,
                               int ncls_layout, int *err, bool ade, int npoles, int storage, cudaStream_t st);
-int bulk_make_maps(void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch, int storage,
-                   BulkMaps *out);
+// the tiles of many plans, one CTA per item: plans and maps (of `kind`'s
+// layout) are device tables of this step's parity, indexed by BulkItem::inst
+cudaError_t launch_tiles_batch(int kind, const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems,
+                               int ncls_layout, int *err, bool ade, int npoles, int storage, cudaStream_t st);
+int tile_make_maps(int kind, void *encode_fn, const DevPlan &p, float *const f[6], const uint8_t *cls, int cls_pitch,
+                   int storage, BulkMaps *out);

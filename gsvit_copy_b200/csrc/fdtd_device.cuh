@@ -8,9 +8,11 @@
 
 #include "fdtd_internal.h"
 
-// ---- field storage: FP32, FP16 or BF16 elements behind the float pointers
-// of DevPlan; arithmetic is FP32 throughout.  Stor<T>::scaled tells whether
-// H and psi carry the power-of-two scales of DevPlan (16-bit storage only).
+// ---- field storage: FP32, FP16, BF16 or FP64 elements behind the float
+// pointers of DevPlan.  Arithmetic is FP32 (Stor<T>::real) for the first three
+// and FP64 for FP64 storage (the reference-precision mode).  Stor<T>::scaled
+// tells whether H and psi carry the power-of-two scales of DevPlan (16-bit
+// storage only).
 template <class T>
 struct Stor;
 
@@ -35,6 +37,7 @@ __device__ __forceinline__ uint32_t sr_seed(uint32_t step, uint32_t array)
 
 template <>
 struct Stor<float> {
+    using real = float;
     static constexpr bool scaled = false;
     static constexpr bool stochastic = false;
     __device__ static float ld(const float *p, int64_t i) { return p[i]; }
@@ -44,6 +47,7 @@ struct Stor<float> {
 };
 template <>
 struct Stor<__half> {
+    using real = float;
     static constexpr bool scaled = true;
     static constexpr bool stochastic = false;
     __device__ static float ld(const float *p, int64_t i) { return __half2float(reinterpret_cast<const __half *>(p)[i]); }
@@ -58,6 +62,7 @@ struct Stor<__nv_bfloat16> {
     // steps per period stalls), so stores round stochastically -- the 16
     // dropped bits are compared against a uniform random number, which makes
     // the stored value an unbiased estimate of the FP32 result.
+    using real = float;
     static constexpr bool scaled = true;
     static constexpr bool stochastic = true;
     __device__ static float ld(const float *p, int64_t i)
@@ -78,14 +83,92 @@ struct Stor<__nv_bfloat16> {
     __device__ static float cvt(__nv_bfloat16 v) { return __bfloat162float(v); }
 };
 
+template <>
+struct Stor<double> {
+    using real = double;
+    static constexpr bool scaled = false;
+    static constexpr bool stochastic = false;
+    __device__ static double ld(const float *p, int64_t i) { return reinterpret_cast<const double *>(p)[i]; }
+    __device__ static double ldg(const float *p, int64_t i) { return __ldg(reinterpret_cast<const double *>(p) + i); }
+    __device__ static void st(float *p, int64_t i, double v) { reinterpret_cast<double *>(p)[i] = v; }
+};
+
 // one element of a field stored as FDTD_STORE_* `storage` (small kernels
 // that read a few values per thread branch on it at run time)
-__device__ __forceinline__ float ld_any(const float *p, int64_t i, int storage)
+__device__ __forceinline__ double ld_any(const float *p, int64_t i, int storage)
 {
     if (storage == 1) return Stor<__half>::ld(p, i);
     if (storage == 2) return Stor<__nv_bfloat16>::ld(p, i);
+    if (storage == 3) return Stor<double>::ld(p, i);
     return p[i];
 }
+
+// three components of the arithmetic type R (float3 / double3)
+template <class R>
+struct V3t;
+template <>
+struct V3t<float> { using type = float3; };
+template <>
+struct V3t<double> { using type = double3; };
+template <class R>
+using V3 = typename V3t<R>::type;
+
+// ---- coefficient tables of the arithmetic type R.  R = float reads the
+// FP32 tables of DevPlan; R = double (FDTD_STORE_F64 plans) reads the FP64
+// tables the same pointers then hold.
+template <class R>
+struct Tab;
+template <>
+struct Tab<float> {
+    using Ade = DevAde;
+    using V2 = float2;
+    __device__ static float dx(const DevPlan &P) { return P.dx; }
+    __device__ static float ld(const float *p, int64_t q) { return __ldg(p + q); }
+    __device__ static float *state(float *p) { return p; }
+    // da, db of class c (scls: the class table as float4, shared or global)
+    __device__ static void hcoef(const DevPlan &, const float4 *scls, int c, float &da, float &db)
+    {
+        const float4 hc = scls[c * 4 + 2];
+        da = hc.x;
+        db = hc.y;
+    }
+    __device__ static void ecoef(const DevPlan &, const float4 *scls, int c, float ca[3], float cb[3], float cba[3],
+                                 unsigned &flags, int &ade)
+    {
+        const float4 c0 = scls[c * 4 + 0], c1 = scls[c * 4 + 1], c2 = scls[c * 4 + 2], c3 = scls[c * 4 + 3];
+        ca[0] = c0.x; ca[1] = c0.y; ca[2] = c0.z;
+        cb[0] = c1.x; cb[1] = c1.y; cb[2] = c1.z;
+        cba[0] = c3.x; cba[1] = c3.y; cba[2] = c3.z;
+        flags = __float_as_uint(c0.w);
+        ade = __float_as_int(c2.z);
+    }
+    __device__ static float tsfe(const DevPlan &, const float4 *scls, int c) { return scls[c * 4 + 1].w; }
+    __device__ static const DevAde &ade(const DevPlan &P, int a) { return P.ade[a]; }
+};
+template <>
+struct Tab<double> {
+    using Ade = DevAde64;
+    using V2 = double2;
+    __device__ static double dx(const DevPlan &P) { return P.dxd; }
+    __device__ static double ld(const float *p, int64_t q) { return __ldg(reinterpret_cast<const double *>(p) + q); }
+    __device__ static double *state(float *p) { return reinterpret_cast<double *>(p); }
+    __device__ static const DevClass64 &cls(const DevPlan &P, int c) { return reinterpret_cast<const DevClass64 *>(P.classes)[c]; }
+    __device__ static void hcoef(const DevPlan &P, const float4 *, int c, double &da, double &db)
+    {
+        da = cls(P, c).da;
+        db = cls(P, c).db;
+    }
+    __device__ static void ecoef(const DevPlan &P, const float4 *, int c, double ca[3], double cb[3], double cba[3],
+                                 unsigned &flags, int &ade)
+    {
+        const DevClass64 &k = cls(P, c);
+        for (int a = 0; a < 3; a++) { ca[a] = k.ca[a]; cb[a] = k.cb[a]; cba[a] = k.cba[a]; }
+        flags = k.flags;
+        ade = k.ade;
+    }
+    __device__ static double tsfe(const DevPlan &P, const float4 *, int c) { return cls(P, c).tsfe; }
+    __device__ static const DevAde64 &ade(const DevPlan &P, int a) { return reinterpret_cast<const DevAde64 *>(P.ade)[a]; }
+};
 
 // E (unscaled), H (times hs), psi_H (times ps) and psi_E (times pse) element
 // access.  Stores take the step number `stp` (sr_step) and the array index of
@@ -97,59 +180,69 @@ __device__ __forceinline__ uint32_t sr_step(const DevPlan &P)
     else return 0u;
 }
 template <class T>
-__device__ __forceinline__ void st_any(float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+__device__ __forceinline__ void st_any(float *p, int64_t i, typename Stor<T>::real v, uint32_t stp, uint32_t array)
 {
     if constexpr (Stor<T>::stochastic) Stor<T>::st_sr(p, i, v, sr_seed(stp, array));
     else Stor<T>::st(p, i, v);
 }
 template <class T>
-__device__ __forceinline__ float ldE(const float *p, int64_t i) { return Stor<T>::ld(p, i); }
+using real_t = typename Stor<T>::real;
 template <class T>
-__device__ __forceinline__ float ldgE(const float *p, int64_t i) { return Stor<T>::ldg(p, i); }
+__device__ __forceinline__ real_t<T> ldE(const float *p, int64_t i) { return Stor<T>::ld(p, i); }
 template <class T>
-__device__ __forceinline__ void stE(float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+__device__ __forceinline__ real_t<T> ldgE(const float *p, int64_t i) { return Stor<T>::ldg(p, i); }
+template <class T>
+__device__ __forceinline__ void stE(float *p, int64_t i, real_t<T> v, uint32_t stp, uint32_t array)
 {
     st_any<T>(p, i, v, stp, array);
 }
 template <class T>
-__device__ __forceinline__ float ldH(const DevPlan &P, const float *p, int64_t i)
+__device__ __forceinline__ real_t<T> ldH(const DevPlan &P, const float *p, int64_t i)
 {
-    return Stor<T>::scaled ? Stor<T>::ld(p, i) * P.ihs : Stor<T>::ld(p, i);
+    if constexpr (Stor<T>::scaled) return Stor<T>::ld(p, i) * P.ihs;
+    else return Stor<T>::ld(p, i);
 }
 template <class T>
-__device__ __forceinline__ float ldgH(const DevPlan &P, const float *p, int64_t i)
+__device__ __forceinline__ real_t<T> ldgH(const DevPlan &P, const float *p, int64_t i)
 {
-    return Stor<T>::scaled ? Stor<T>::ldg(p, i) * P.ihs : Stor<T>::ldg(p, i);
+    if constexpr (Stor<T>::scaled) return Stor<T>::ldg(p, i) * P.ihs;
+    else return Stor<T>::ldg(p, i);
 }
 template <class T>
-__device__ __forceinline__ void stH(const DevPlan &P, float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+__device__ __forceinline__ void stH(const DevPlan &P, float *p, int64_t i, real_t<T> v, uint32_t stp, uint32_t array)
 {
-    st_any<T>(p, i, Stor<T>::scaled ? v * P.hs : v, stp, array);
+    if constexpr (Stor<T>::scaled) st_any<T>(p, i, v * P.hs, stp, array);
+    else st_any<T>(p, i, v, stp, array);
 }
 template <class T>
-__device__ __forceinline__ float ldPsi(const DevPlan &P, const float *p, int64_t i)
+__device__ __forceinline__ real_t<T> ldPsi(const DevPlan &P, const float *p, int64_t i)
 {
-    return Stor<T>::scaled ? Stor<T>::ld(p, i) * P.ips : Stor<T>::ld(p, i);
+    if constexpr (Stor<T>::scaled) return Stor<T>::ld(p, i) * P.ips;
+    else return Stor<T>::ld(p, i);
 }
 template <class T>
-__device__ __forceinline__ float ldgPsi(const DevPlan &P, const float *p, int64_t i)
+__device__ __forceinline__ real_t<T> ldgPsi(const DevPlan &P, const float *p, int64_t i)
 {
-    return Stor<T>::scaled ? Stor<T>::ldg(p, i) * P.ips : Stor<T>::ldg(p, i);
+    if constexpr (Stor<T>::scaled) return Stor<T>::ldg(p, i) * P.ips;
+    else return Stor<T>::ldg(p, i);
 }
 template <class T>
-__device__ __forceinline__ void stPsi(const DevPlan &P, float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+__device__ __forceinline__ void stPsi(const DevPlan &P, float *p, int64_t i, real_t<T> v, uint32_t stp, uint32_t array)
 {
-    st_any<T>(p, i, Stor<T>::scaled ? v * P.ps : v, stp, array);
+    if constexpr (Stor<T>::scaled) st_any<T>(p, i, v * P.ps, stp, array);
+    else st_any<T>(p, i, v, stp, array);
 }
 template <class T>
-__device__ __forceinline__ float ldPsiE(const DevPlan &P, const float *p, int64_t i)
+__device__ __forceinline__ real_t<T> ldPsiE(const DevPlan &P, const float *p, int64_t i)
 {
-    return Stor<T>::scaled ? Stor<T>::ld(p, i) * P.ipse : Stor<T>::ld(p, i);
+    if constexpr (Stor<T>::scaled) return Stor<T>::ld(p, i) * P.ipse;
+    else return Stor<T>::ld(p, i);
 }
 template <class T>
-__device__ __forceinline__ void stPsiE(const DevPlan &P, float *p, int64_t i, float v, uint32_t stp, uint32_t array)
+__device__ __forceinline__ void stPsiE(const DevPlan &P, float *p, int64_t i, real_t<T> v, uint32_t stp, uint32_t array)
 {
-    st_any<T>(p, i, Stor<T>::scaled ? v * P.pse : v, stp, array);
+    if constexpr (Stor<T>::scaled) st_any<T>(p, i, v * P.pse, stp, array);
+    else st_any<T>(p, i, v, stp, array);
 }
 
 // a hint that moves the line holding p into L2; no register, no wait
@@ -294,40 +387,46 @@ __device__ __forceinline__ double tsf_dval(const double *data, int res, double x
 // Face order as the reference applies them: i0, in, j0, jn, k0, kn
 // (source.c:1476-1672); components (hy,hz) on i faces, (hx,hz) on j faces,
 // (hx,hy) on k faces.
-__device__ __forceinline__ void tsf_add_h(const DevPlan &P, int i, int j, int k, float &hx, float &hy, float &hz)
+template <class R>
+__device__ __forceinline__ void tsf_add_h(const DevPlan &P, int i, int j, int k, R &hx, R &hy, R &hz)
 {
+    using V2 = typename Tab<R>::V2;
+    const V2 *const *tc = reinterpret_cast<const V2 *const *>(P.tcor_h);
     const int i0 = P.t0[0], j0 = P.t0[1], k0 = P.t0[2], in = P.t1[0], jn = P.t1[1], kn = P.t1[2];
     const bool ji = j >= j0 && j <= jn, ki = k >= k0 && k <= kn, ii = i >= i0 && i <= in;
     if (ji && ki) {
-        if (i == i0 - 1) { const float2 d = P.tcor_h[0][(j - j0) * P.tnb[0] + (k - k0)]; hy += d.x; hz += d.y; }
-        if (i == in) { const float2 d = P.tcor_h[1][(j - j0) * P.tnb[1] + (k - k0)]; hy += d.x; hz += d.y; }
+        if (i == i0 - 1) { const V2 d = tc[0][(j - j0) * P.tnb[0] + (k - k0)]; hy += d.x; hz += d.y; }
+        if (i == in) { const V2 d = tc[1][(j - j0) * P.tnb[1] + (k - k0)]; hy += d.x; hz += d.y; }
     }
     if (ii && ki) {
-        if (j == j0 - 1) { const float2 d = P.tcor_h[2][(i - i0) * P.tnb[2] + (k - k0)]; hx += d.x; hz += d.y; }
-        if (j == jn) { const float2 d = P.tcor_h[3][(i - i0) * P.tnb[3] + (k - k0)]; hx += d.x; hz += d.y; }
+        if (j == j0 - 1) { const V2 d = tc[2][(i - i0) * P.tnb[2] + (k - k0)]; hx += d.x; hz += d.y; }
+        if (j == jn) { const V2 d = tc[3][(i - i0) * P.tnb[3] + (k - k0)]; hx += d.x; hz += d.y; }
     }
     if (ii && ji) {
-        if (k == k0 - 1) { const float2 d = P.tcor_h[4][(i - i0) * P.tnb[4] + (j - j0)]; hx += d.x; hy += d.y; }
-        if (k == kn) { const float2 d = P.tcor_h[5][(i - i0) * P.tnb[5] + (j - j0)]; hx += d.x; hy += d.y; }
+        if (k == k0 - 1) { const V2 d = tc[4][(i - i0) * P.tnb[4] + (j - j0)]; hx += d.x; hy += d.y; }
+        if (k == kn) { const V2 d = tc[5][(i - i0) * P.tnb[5] + (j - j0)]; hx += d.x; hy += d.y; }
     }
 }
 
 // Same for the E cell (source.c:547-771): (ey,ez) on i faces, (ex,ez) on j
 // faces, (ex,ey) on k faces.
-__device__ __forceinline__ void tsf_add_e(const DevPlan &P, int i, int j, int k, float &ex, float &ey, float &ez)
+template <class R>
+__device__ __forceinline__ void tsf_add_e(const DevPlan &P, int i, int j, int k, R &ex, R &ey, R &ez)
 {
+    using V2 = typename Tab<R>::V2;
+    const V2 *const *tc = reinterpret_cast<const V2 *const *>(P.tcor_e);
     const int i0 = P.t0[0], j0 = P.t0[1], k0 = P.t0[2], in = P.t1[0], jn = P.t1[1], kn = P.t1[2];
     const bool ji = j >= j0 && j <= jn, ki = k >= k0 && k <= kn, ii = i >= i0 && i <= in;
     if (ji && ki) {
-        if (i == i0) { const float2 d = P.tcor_e[0][(j - j0) * P.tnb[0] + (k - k0)]; ey += d.x; ez += d.y; }
-        if (i == in) { const float2 d = P.tcor_e[1][(j - j0) * P.tnb[1] + (k - k0)]; ey += d.x; ez += d.y; }
+        if (i == i0) { const V2 d = tc[0][(j - j0) * P.tnb[0] + (k - k0)]; ey += d.x; ez += d.y; }
+        if (i == in) { const V2 d = tc[1][(j - j0) * P.tnb[1] + (k - k0)]; ey += d.x; ez += d.y; }
     }
     if (ii && ki) {
-        if (j == j0) { const float2 d = P.tcor_e[2][(i - i0) * P.tnb[2] + (k - k0)]; ex += d.x; ez += d.y; }
-        if (j == jn) { const float2 d = P.tcor_e[3][(i - i0) * P.tnb[3] + (k - k0)]; ex += d.x; ez += d.y; }
+        if (j == j0) { const V2 d = tc[2][(i - i0) * P.tnb[2] + (k - k0)]; ex += d.x; ez += d.y; }
+        if (j == jn) { const V2 d = tc[3][(i - i0) * P.tnb[3] + (k - k0)]; ex += d.x; ez += d.y; }
     }
     if (ii && ji) {
-        if (k == k0) { const float2 d = P.tcor_e[4][(i - i0) * P.tnb[4] + (j - j0)]; ex += d.x; ey += d.y; }
-        if (k == kn) { const float2 d = P.tcor_e[5][(i - i0) * P.tnb[5] + (j - j0)]; ex += d.x; ey += d.y; }
+        if (k == k0) { const V2 d = tc[4][(i - i0) * P.tnb[4] + (j - j0)]; ex += d.x; ey += d.y; }
+        if (k == kn) { const V2 d = tc[5][(i - i0) * P.tnb[5] + (j - j0)]; ex += d.x; ey += d.y; }
     }
 }

@@ -45,6 +45,17 @@ struct alignas(16) DevClass {
     float pad1;
 };
 
+// The same class in FP64 (FDTD_STORE_F64 plans: DevPlan::classes then points
+// to these).
+struct alignas(16) DevClass64 {
+    double ca[3], cb[3];
+    double da, db;
+    double cba[3];
+    double tsfe;
+    uint32_t flags;
+    int32_t ade;
+};
+
 // ADE coefficients of calculate_ade_a/bp/c (plan.c:2737-2763), recast for the
 // difference form of the polarisation state: per component the kernels keep
 // Q = P_D^n - P_D^{n-1} and, per critical-point pole, p = P_cp^n and
@@ -68,10 +79,29 @@ struct DevAde {
     float bp2[2], bp3[2], bp4[2];
 };
 
+// The same set in FP64 (FDTD_STORE_F64 plans: DevPlan::ade then points to these).
+struct DevAde64 {
+    double c0dx;
+    double c2, c3;
+    double qe;
+    double ma0, a2;
+    double pe[2], qpe[2];
+    double rp[2], rq[2];
+    double bp2[2], bp3[2], bp4[2];
+};
+
 struct DevPlan {
     int xr, yr, zr;
     int64_t si, sj;                 // strides of i and j (k stride is 1)
+    // plain range per axis: a cell with every index in [plo, phi) takes the
+    // plain update (no CPML psi, kappa 1, no edge or zeroed-plane rule)
+    int plo[3], phi[3];
+    // FDTD_STORE_F64 plan: fields, psi and ADE state are doubles, and every
+    // table below (classes, ADE sets, CPML profiles, 1/kappa, TSF corrections,
+    // design coefficients) holds doubles behind its float-typed pointer
+    int real64;
     float dx;                       // cell size (cubic cells)
+    double dxd;                     // the same in FP64
     // 16-bit field storage (FDTD_STORE_F16 / _BF16): H is stored times hs,
     // psi_H times ps and psi_E times pse (powers of two, so the scaling is
     // exact); FP32 storage uses none of them.  The field and psi pointers

@@ -24,329 +24,9 @@
 #include "fdtd_device.cuh"
 #include "fdtd_kernels.cuh"
 
+#include "fdtd_cells.cuh"
+
 namespace {
-
-enum { X0 = 0, XN = 1, Y0 = 2, YN = 3, Z0 = 4, ZN = 5 };
-
-// ------------------------------------------------------------ cell updates
-
-
-#define FULLMASK 0xffffffffu
-
-// CPML psi_H update and corrections (boundary.c:347-519, face order x0 y0 z0
-// xn yn zn), TSF H corrections (source.c:1476-1672) and the outer H planes
-// zeroed by boundary_hstep (boundary.c:418-420, 455-457, 490-492), applied to
-// H after ystep_h.  `owner` cells write their psi_H.
-template <class T>
-__device__ __forceinline__ float3 h_special(const DevPlan &P, int i, int j, int k, bool owner, bool tsf, float db, float dey_i,
-                                         float dez_i, float dex_j, float dez_j, float dex_k, float dey_k, float3 hin)
-{
-    const uint32_t stp = sr_step<T>(P);
-    float hx = hin.x, hy = hin.y, hz = hin.z;
-    const int xr = P.xr, yr = P.yr, zr = P.zr;
-    const bool il = (i == xr - 1), jl = (j == yr - 1), kl = (k == zr - 1);
-    if (tsf && P.tsf_on) tsf_add_h(P, i, j, k, hx, hy, hz);
-    const bool jin = (j >= 1 && j < yr - 1), kin = (k >= 1 && k < zr - 1), iin = (i >= 1 && i < xr - 1);
-    const float dbdx = db * P.dx;
-    const float idx_ = 1.0f / P.dx;
-    if (P.cp_on[X0] && i < P.cp_d[X0] - 1 && jin && kin) {
-        const int64_t q = ((int64_t)i * yr + j) * zr + k;
-        const float bh = __ldg(P.bh[X0] + i), ch = __ldg(P.ch[X0] + i);
-        float pzx = bh * ldgPsi<T>(P, P.psih_in[X0][1], q) + ch * dey_i * idx_;
-        float pyx = bh * ldgPsi<T>(P, P.psih_in[X0][0], q) + ch * dez_i * idx_;
-        hy += dbdx * pyx;
-        hz -= dbdx * pzx;
-        if (owner) { stPsi<T>(P, P.psih_out[X0][1], q, pzx, stp, 18 + 2 * X0 + 1); stPsi<T>(P, P.psih_out[X0][0], q, pyx, stp, 18 + 2 * X0 + 0); }
-    }
-    if (P.cp_on[Y0] && j < P.cp_d[Y0] - 1 && iin && kin) {
-        const int64_t q = ((int64_t)i * P.cp_d[Y0] + j) * zr + k;
-        const float bh = __ldg(P.bh[Y0] + j), ch = __ldg(P.ch[Y0] + j);
-        float pxy = bh * ldgPsi<T>(P, P.psih_in[Y0][0], q) + ch * dez_j * idx_;
-        float pzy = bh * ldgPsi<T>(P, P.psih_in[Y0][1], q) + ch * dex_j * idx_;
-        hx -= dbdx * pxy;
-        hz += dbdx * pzy;
-        if (owner) { stPsi<T>(P, P.psih_out[Y0][0], q, pxy, stp, 18 + 2 * Y0 + 0); stPsi<T>(P, P.psih_out[Y0][1], q, pzy, stp, 18 + 2 * Y0 + 1); }
-    }
-    if (P.cp_on[Z0] && k < P.cp_d[Z0] - 1 && iin && jin) {
-        const int64_t q = ((int64_t)i * yr + j) * P.cp_d[Z0] + k;
-        const float bh = __ldg(P.bh[Z0] + k), ch = __ldg(P.ch[Z0] + k);
-        float pyz = bh * ldgPsi<T>(P, P.psih_in[Z0][1], q) + ch * dex_k * idx_;
-        float pxz = bh * ldgPsi<T>(P, P.psih_in[Z0][0], q) + ch * dey_k * idx_;
-        hy -= dbdx * pyz;
-        hx += dbdx * pxz;
-        if (owner) { stPsi<T>(P, P.psih_out[Z0][1], q, pyz, stp, 18 + 2 * Z0 + 1); stPsi<T>(P, P.psih_out[Z0][0], q, pxz, stp, 18 + 2 * Z0 + 0); }
-    }
-    if (P.cp_on[XN]) {
-        const int d = P.cp_d[XN];
-        if (i >= xr - d + 1 && i < xr - 1 && jin && kin) {
-            const int ir = i - (xr - d);
-            const int64_t q = ((int64_t)ir * yr + j) * zr + k;
-            const float bh = __ldg(P.bh[XN] + ir), ch = __ldg(P.ch[XN] + ir);
-            float pzx = bh * ldgPsi<T>(P, P.psih_in[XN][1], q) + ch * dey_i * idx_;
-            float pyx = bh * ldgPsi<T>(P, P.psih_in[XN][0], q) + ch * dez_i * idx_;
-            hy += dbdx * pyx;
-            hz -= dbdx * pzx;
-            if (owner) { stPsi<T>(P, P.psih_out[XN][1], q, pzx, stp, 18 + 2 * XN + 1); stPsi<T>(P, P.psih_out[XN][0], q, pyx, stp, 18 + 2 * XN + 0); }
-        }
-    }
-    if (P.cp_on[YN]) {
-        const int d = P.cp_d[YN];
-        if (j >= yr - d + 1 && j < yr - 1 && iin && kin) {
-            const int jr = j - (yr - d);
-            const int64_t q = ((int64_t)i * d + jr) * zr + k;
-            const float bh = __ldg(P.bh[YN] + jr), ch = __ldg(P.ch[YN] + jr);
-            float pxy = bh * ldgPsi<T>(P, P.psih_in[YN][0], q) + ch * dez_j * idx_;
-            float pzy = bh * ldgPsi<T>(P, P.psih_in[YN][1], q) + ch * dex_j * idx_;
-            hx -= dbdx * pxy;
-            hz += dbdx * pzy;
-            if (owner) { stPsi<T>(P, P.psih_out[YN][0], q, pxy, stp, 18 + 2 * YN + 0); stPsi<T>(P, P.psih_out[YN][1], q, pzy, stp, 18 + 2 * YN + 1); }
-        }
-    }
-    if (P.cp_on[ZN]) {
-        const int d = P.cp_d[ZN];
-        if (k >= zr - d + 1 && k < zr - 1 && iin && jin) {
-            const int kr = k - (zr - d);
-            const int64_t q = ((int64_t)i * yr + j) * d + kr;
-            const float bh = __ldg(P.bh[ZN] + kr), ch = __ldg(P.ch[ZN] + kr);
-            float pyz = bh * ldgPsi<T>(P, P.psih_in[ZN][1], q) + ch * dex_k * idx_;
-            float pxz = bh * ldgPsi<T>(P, P.psih_in[ZN][0], q) + ch * dey_k * idx_;
-            hy -= dbdx * pyz;
-            hx += dbdx * pxz;
-            if (owner) { stPsi<T>(P, P.psih_out[ZN][1], q, pyz, stp, 18 + 2 * ZN + 1); stPsi<T>(P, P.psih_out[ZN][0], q, pxz, stp, 18 + 2 * ZN + 0); }
-        }
-    }
-    if ((P.cp_on[XN] && il && jin && kin) || (P.cp_on[YN] && jl && iin && kin) || (P.cp_on[ZN] && kl && iin && jin))
-        hx = hy = hz = 0.f;
-    return make_float3(hx, hy, hz);
-}
-
-// H^{n+1/2}(i) at one cell from E^n and the six E differences (ystep_h,
-// yee.c:246-256, then h_special where the cell lies in a slab or on a face).
-template <class T>
-__device__ __forceinline__ void h_update(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k,
-                                         bool special, bool owner, bool tsf, float dey_i, float dez_i, float dex_j, float dez_j,
-                                         float dex_k, float dey_k, float h[3])
-{
-    const float4 hc = scls[cls * 4 + 2];     // da, db
-    const bool il = (i == P.xr - 1), jl = (j == P.yr - 1), kl = (k == P.zr - 1);
-    float ikx = 1.f, iky = 1.f, ikz = 1.f;
-    if (special) { ikx = __ldg(P.ikh[0] + i); iky = __ldg(P.ikh[1] + j); ikz = __ldg(P.ikh[2] + k); }
-    if (!(jl || kl)) h[0] = hc.x * h[0] + hc.y * (dey_k * ikz - dez_j * iky);
-    if (!(il || kl)) h[1] = hc.x * h[1] + hc.y * (dez_i * ikx - dex_k * ikz);
-    if (!(il || jl)) h[2] = hc.x * h[2] + hc.y * (dex_j * iky - dey_i * ikx);
-    if (special) {
-        const float3 o = h_special<T>(P, i, j, k, owner, tsf, hc.y, dey_i, dez_i, dex_j, dez_j, dex_k, dey_k,
-                                   make_float3(h[0], h[1], h[2]));
-        h[0] = o.x; h[1] = o.y; h[2] = o.z;
-    }
-}
-
-// E^{n+1}(i) of one cell on the general path: ADE branch with its CPML
-// (yee.c:914-1108), ordinary update (yee.c:1113-1128), PEC rule
-// (yee.c:1138-1237), boundary_estep zero planes, psi_E and corrections
-// (boundary.c:691-884) and TSF E (source.c:547-771).
-template <bool ADE, int NPOLES, class T>
-__device__ __noinline__ float3 e_special(const DevPlan &P, const float4 *scls, int cls, int i, int j, int k, bool tsf,
-                                         float3 eo3, float3 h3, float hx_jm, float hz_jm, float hx_km, float hy_km,
-                                         float hy_im, float hz_im)
-{
-    const uint32_t stp = sr_step<T>(P);
-    const float eo[3] = {eo3.x, eo3.y, eo3.z};
-    const float h[3] = {h3.x, h3.y, h3.z};
-    const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
-    const float4 c0 = scls[cls * 4 + 0], c1 = scls[cls * 4 + 1], c2 = scls[cls * 4 + 2], c3 = scls[cls * 4 + 3];
-    const unsigned fl = __float_as_uint(c0.w);
-    float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z};
-    const float cba[3] = {c3.x, c3.y, c3.z};
-    if (fl & CF_DESIGN) {   // adjoint design region: coefficients per cell
-        const int64_t q = ((int64_t)(i - P.dbox[0]) * (P.dbox[3] - P.dbox[2]) + (j - P.dbox[2])) * (P.dbox[5] - P.dbox[4]) + (k - P.dbox[4]);
-        for (int a = 0; a < 3; a++) { ca[a] = __ldg(P.dcoef + 6 * q + a); cb[a] = __ldg(P.dcoef + 6 * q + 3 + a); }
-    }
-    const int ade_set = __float_as_int(c2.z);
-    const int xr = P.xr, yr = P.yr, zr = P.zr;
-    const float ikx = __ldg(P.ike[0] + i), iky = __ldg(P.ike[1] + j), ikz = __ldg(P.ike[2] + k);
-    const float hx = h[0], hy = h[1], hz = h[2];
-    const bool gx = (j > 0 && k > 0), gy = (i > 0 && k > 0), gz = (i > 0 && j > 0);
-    const float dhz_i = i > 0 ? hz - hz_im : 0.f, dhy_i = i > 0 ? hy - hy_im : 0.f;
-    const float dhz_j = j > 0 ? hz - hz_jm : 0.f, dhx_j = j > 0 ? hx - hx_jm : 0.f;
-    const float dhx_k = k > 0 ? hx - hx_km : 0.f, dhy_k = k > 0 ? hy - hy_km : 0.f;
-    const float curlx = dhz_j * iky - dhy_k * ikz;
-    const float curly = dhx_k * ikz - dhz_i * ikx;
-    const float curlz = dhy_i * ikx - dhx_j * iky;
-    float nx = eo[0], ny = eo[1], nz = eo[2];
-    const float idx_ = 1.0f / P.dx;
-    float px0[2] = {0, 0}, pxn[2] = {0, 0}, py0[2] = {0, 0}, pyn[2] = {0, 0}, pz0[2] = {0, 0}, pzn[2] = {0, 0};
-    const bool inx0 = P.cp_on[X0] && i >= 1 && i < P.cp_d[X0];
-    const bool iny0 = P.cp_on[Y0] && j >= 1 && j < P.cp_d[Y0];
-    const bool inz0 = P.cp_on[Z0] && k >= 1 && k < P.cp_d[Z0];
-    const bool inxn = P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1;
-    const bool inyn = P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1;
-    const bool inzn = P.cp_on[ZN] && k >= zr - P.cp_d[ZN] + 1;
-    const bool zero = (P.cp_on[X0] && i == 0) || (P.cp_on[Y0] && j == 0) || (P.cp_on[Z0] && k == 0);
-    int64_t qx0 = 0, qxn = 0, qy0 = 0, qyn = 0, qz0 = 0, qzn = 0;
-    if (!zero) {
-        if (inx0) { qx0 = ((int64_t)i * yr + j) * zr + k; px0[0] = ldPsiE<T>(P, P.psie[X0][0], qx0); px0[1] = ldPsiE<T>(P, P.psie[X0][1], qx0); }
-        if (inxn) { qxn = ((int64_t)(i - (xr - P.cp_d[XN])) * yr + j) * zr + k; pxn[0] = ldPsiE<T>(P, P.psie[XN][0], qxn); pxn[1] = ldPsiE<T>(P, P.psie[XN][1], qxn); }
-        if (iny0) { qy0 = ((int64_t)i * P.cp_d[Y0] + j) * zr + k; py0[0] = ldPsiE<T>(P, P.psie[Y0][0], qy0); py0[1] = ldPsiE<T>(P, P.psie[Y0][1], qy0); }
-        if (inyn) { qyn = ((int64_t)i * P.cp_d[YN] + (j - (yr - P.cp_d[YN]))) * zr + k; pyn[0] = ldPsiE<T>(P, P.psie[YN][0], qyn); pyn[1] = ldPsiE<T>(P, P.psie[YN][1], qyn); }
-        if (inz0) { qz0 = ((int64_t)i * yr + j) * P.cp_d[Z0] + k; pz0[0] = ldPsiE<T>(P, P.psie[Z0][0], qz0); pz0[1] = ldPsiE<T>(P, P.psie[Z0][1], qz0); }
-        if (inzn) { qzn = ((int64_t)i * yr + j) * P.cp_d[ZN] + (k - (zr - P.cp_d[ZN])); pzn[0] = ldPsiE<T>(P, P.psie[ZN][0], qzn); pzn[1] = ldPsiE<T>(P, P.psie[ZN][1], qzn); }
-    }
-    if (ADE && (fl & CF_ADE_BRANCH)) {
-        const DevAde &A = P.ade[ade_set];
-        const bool comp[3] = {(fl & CF_ADE_X) != 0, (fl & CF_ADE_Y) != 0, (fl & CF_ADE_Z) != 0};
-        // difference-form state (see DevAde); E^{n-1} is the output set before this write
-        float qd[3] = {0, 0, 0}, ep[3] = {0, 0, 0}, pc[3][2], qc[3][2];
-        for (int a = 0; a < 3; a++) {
-            if (!comp[a]) continue;
-            qd[a] = P.q[a][c]; ep[a] = ldE<T>(P.fout[a], c);
-            for (int n = 0; n < NPOLES; n++) { pc[a][n] = P.pc[a][n][c]; qc[a][n] = P.qc[a][n][c]; }
-        }
-        const float curl[3] = {curlx, curly, curlz};
-        const bool gd[3] = {gx, gy, gz};
-        float ne[3] = {nx, ny, nz};
-        for (int a = 0; a < 3; a++) {
-            if (!(comp[a] && gd[a])) continue;
-            float v = A.c0dx * curl[a] + A.qe * qd[a];
-            for (int n = 0; n < NPOLES; n++) v += A.qpe[n] * qc[a][n] + A.pe[n] * pc[a][n];
-            v += A.c2 * ep[a] + A.c3 * eo[a];
-            ne[a] = v;
-        }
-        if (!zero) {   // CPML inside the ADE branch, first psi_E update
-            if (inx0 && i > 1) {   // x0 corrections are scaled by cb == 0 (yee.c:577)
-                const float be = __ldg(P.be[X0] + i), ce = __ldg(P.ce[X0] + i);
-                px0[0] = be * px0[0] + ce * dhz_i * idx_;
-                px0[1] = be * px0[1] + ce * dhy_i * idx_;
-            }
-            if (iny0 && j > 1) {
-                const float be = __ldg(P.be[Y0] + j), ce = __ldg(P.ce[Y0] + j);
-                py0[0] = be * py0[0] + ce * dhz_j * idx_;
-                py0[1] = be * py0[1] + ce * dhx_j * idx_;
-                if ((i > 0 && k > 0) && comp[0]) ne[0] += P.dx * cba[0] * py0[0];
-                if ((i > 0 && k > 0) && comp[2]) ne[2] -= P.dx * cba[2] * py0[1];
-            }
-            if (inz0 && k > 1) {
-                const float be = __ldg(P.be[Z0] + k), ce = __ldg(P.ce[Z0] + k);
-                pz0[1] = be * pz0[1] + ce * dhx_k * idx_;
-                pz0[0] = be * pz0[0] + ce * dhy_k * idx_;
-                if ((i > 0 && j > 0) && comp[1]) ne[1] += P.dx * cba[1] * pz0[1];
-                if ((i > 0 && j > 0) && comp[0]) ne[0] -= P.dx * cba[0] * pz0[0];
-            }
-            if (inxn) {
-                const int ir = i - (xr - P.cp_d[XN]);
-                const float be = __ldg(P.be[XN] + ir), ce = __ldg(P.ce[XN] + ir);
-                pxn[0] = be * pxn[0] + ce * dhz_i * idx_;
-                pxn[1] = be * pxn[1] + ce * dhy_i * idx_;
-                if ((j > 0 && k > 0) && comp[1]) ne[1] -= P.dx * cba[1] * pxn[0];
-                if ((j > 0 && k > 0) && comp[2]) ne[2] += P.dx * cba[2] * pxn[1];
-            }
-            if (inyn) {
-                const int jr = j - (yr - P.cp_d[YN]);
-                const float be = __ldg(P.be[YN] + jr), ce = __ldg(P.ce[YN] + jr);
-                pyn[0] = be * pyn[0] + ce * dhz_j * idx_;
-                pyn[1] = be * pyn[1] + ce * dhx_j * idx_;
-                if ((i > 0 && k > 0) && comp[0]) ne[0] += P.dx * cba[0] * pyn[0];
-                if ((i > 0 && k > 0) && comp[2]) ne[2] -= P.dx * cba[2] * pyn[1];
-            }
-            if (inzn) {
-                const int kr = k - (zr - P.cp_d[ZN]);
-                const float be = __ldg(P.be[ZN] + kr), ce = __ldg(P.ce[ZN] + kr);
-                pzn[1] = be * pzn[1] + ce * dhx_k * idx_;
-                pzn[0] = be * pzn[0] + ce * dhy_k * idx_;
-                if ((i > 0 && j > 0) && comp[1]) ne[1] += P.dx * cba[1] * pzn[1];
-                if ((i > 0 && j > 0) && comp[0]) ne[0] -= P.dx * cba[0] * pzn[0];
-            }
-        }
-        for (int a = 0; a < 3; a++) {   // polarisation recursions of the owned components
-            if (!comp[a]) continue;
-            const float e1 = ne[a];
-            P.q[a][c] = A.ma0 * qd[a] + A.a2 * (ep[a] + 2.f * eo[a] + e1);
-            for (int n = 0; n < NPOLES; n++) {
-                const float qn = A.rp[n] * pc[a][n] + A.rq[n] * qc[a][n] + A.bp2[n] * ep[a] + A.bp3[n] * eo[a] + A.bp4[n] * e1;
-                P.qc[a][n][c] = qn;
-                P.pc[a][n][c] = pc[a][n] + qn;
-            }
-        }
-        nx = ne[0]; ny = ne[1]; nz = ne[2];
-    }
-    if (gx && !(ADE && (fl & CF_ADE_X))) nx = ca[0] * eo[0] + cb[0] * curlx;
-    if (gy && !(ADE && (fl & CF_ADE_Y))) ny = ca[1] * eo[1] + cb[1] * curly;
-    if (gz && !(ADE && (fl & CF_ADE_Z))) nz = ca[2] * eo[2] + cb[2] * curlz;
-    if (fl & CF_PEC_X) nx = 0.f;
-    if (fl & CF_PEC_Y) ny = 0.f;
-    if (fl & CF_PEC_Z) nz = 0.f;
-    if (zero) {
-        nx = ny = nz = 0.f;
-    } else {
-        const bool tx = !(fl & CF_ADE_X), ty = !(fl & CF_ADE_Y), tz = !(fl & CF_ADE_Z);
-        const float dx = P.dx;
-        if (inx0) {
-            const float be = __ldg(P.be[X0] + i), ce = __ldg(P.ce[X0] + i);
-            px0[0] = be * px0[0] + ce * dhz_i * idx_;
-            px0[1] = be * px0[1] + ce * dhy_i * idx_;
-            if (j > 0 && k > 0) {
-                if (ty) ny -= dx * cb[1] * px0[0];
-                if (tz) nz += dx * cb[2] * px0[1];
-                stPsiE<T>(P, P.psie[X0][0], qx0, px0[0], stp, 6 + 2 * X0 + 0); stPsiE<T>(P, P.psie[X0][1], qx0, px0[1], stp, 6 + 2 * X0 + 1);
-            }
-        }
-        if (iny0) {
-            const float be = __ldg(P.be[Y0] + j), ce = __ldg(P.ce[Y0] + j);
-            py0[0] = be * py0[0] + ce * dhz_j * idx_;
-            py0[1] = be * py0[1] + ce * dhx_j * idx_;
-            if (i > 0 && k > 0) {
-                if (tx) nx += dx * cb[0] * py0[0];
-                if (tz) nz -= dx * cb[2] * py0[1];
-                stPsiE<T>(P, P.psie[Y0][0], qy0, py0[0], stp, 6 + 2 * Y0 + 0); stPsiE<T>(P, P.psie[Y0][1], qy0, py0[1], stp, 6 + 2 * Y0 + 1);
-            }
-        }
-        if (inz0) {
-            const float be = __ldg(P.be[Z0] + k), ce = __ldg(P.ce[Z0] + k);
-            pz0[1] = be * pz0[1] + ce * dhx_k * idx_;
-            pz0[0] = be * pz0[0] + ce * dhy_k * idx_;
-            if (i > 0 && j > 0) {
-                if (ty) ny += dx * cb[1] * pz0[1];
-                if (tz) nx -= dx * cb[0] * pz0[0];     // gated by ztbc in the reference (boundary.c:758-759)
-                stPsiE<T>(P, P.psie[Z0][0], qz0, pz0[0], stp, 6 + 2 * Z0 + 0); stPsiE<T>(P, P.psie[Z0][1], qz0, pz0[1], stp, 6 + 2 * Z0 + 1);
-            }
-        }
-        if (inxn) {
-            const int ir = i - (xr - P.cp_d[XN]);
-            const float be = __ldg(P.be[XN] + ir), ce = __ldg(P.ce[XN] + ir);
-            pxn[0] = be * pxn[0] + ce * dhz_i * idx_;
-            pxn[1] = be * pxn[1] + ce * dhy_i * idx_;
-            if (j > 0 && k > 0) {
-                if (ty) ny -= dx * cb[1] * pxn[0];
-                if (tz) nz += dx * cb[2] * pxn[1];
-                stPsiE<T>(P, P.psie[XN][0], qxn, pxn[0], stp, 6 + 2 * XN + 0); stPsiE<T>(P, P.psie[XN][1], qxn, pxn[1], stp, 6 + 2 * XN + 1);
-            }
-        }
-        if (inyn) {
-            const int jr = j - (yr - P.cp_d[YN]);
-            const float be = __ldg(P.be[YN] + jr), ce = __ldg(P.ce[YN] + jr);
-            pyn[0] = be * pyn[0] + ce * dhz_j * idx_;
-            pyn[1] = be * pyn[1] + ce * dhx_j * idx_;
-            if (i > 0 && k > 0) {
-                if (tx) nx += dx * cb[0] * pyn[0];
-                if (tz) nz -= dx * cb[2] * pyn[1];
-                stPsiE<T>(P, P.psie[YN][0], qyn, pyn[0], stp, 6 + 2 * YN + 0); stPsiE<T>(P, P.psie[YN][1], qyn, pyn[1], stp, 6 + 2 * YN + 1);
-            }
-        }
-        if (inzn) {
-            const int kr = k - (zr - P.cp_d[ZN]);
-            const float be = __ldg(P.be[ZN] + kr), ce = __ldg(P.ce[ZN] + kr);
-            pzn[1] = be * pzn[1] + ce * dhx_k * idx_;
-            pzn[0] = be * pzn[0] + ce * dhy_k * idx_;
-            if (i > 0 && j > 0) {
-                if (ty) ny += dx * cb[1] * pzn[1];
-                if (tx) nx -= dx * cb[0] * pzn[0];
-                stPsiE<T>(P, P.psie[ZN][0], qzn, pzn[0], stp, 6 + 2 * ZN + 0); stPsiE<T>(P, P.psie[ZN][1], qzn, pzn[1], stp, 6 + 2 * ZN + 1);
-            }
-        }
-    }
-    if (tsf && P.tsf_on) tsf_add_e(P, i, j, k, nx, ny, nz);
-    return make_float3(nx, ny, nz);
-}
 
 // ------------------------------------------------------------ slab kernels
 
@@ -391,15 +71,16 @@ __device__ __forceinline__ bool box_cell(const SlabBox *boxes, int nboxes, int &
 template <class T>
 __device__ __forceinline__ void slab_h_cell(const DevPlan &P, int i, int j, int k, bool tsf)
 {
+    using R = real_t<T>;
     const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
     const float *EX = P.fin[0], *EY = P.fin[1], *EZ = P.fin[2];
-    const float ex = ldgE<T>(EX, c), ey = ldgE<T>(EY, c), ez = ldgE<T>(EZ, c);
+    const R ex = ldgE<T>(EX, c), ey = ldgE<T>(EY, c), ez = ldgE<T>(EZ, c);
     const bool il = (i == P.xr - 1), jl = (j == P.yr - 1), kl = (k == P.zr - 1);
-    const float eyk = kl ? 0.f : ldgE<T>(EY, c + 1), exk = kl ? 0.f : ldgE<T>(EX, c + 1);
-    const float ezj = jl ? 0.f : ldgE<T>(EZ, c + P.sj), exj = jl ? 0.f : ldgE<T>(EX, c + P.sj);
-    const float ezi = il ? 0.f : ldgE<T>(EZ, c + P.si), eyi = il ? 0.f : ldgE<T>(EY, c + P.si);
-    float h[3] = {ldgH<T>(P, P.fin[3], c), ldgH<T>(P, P.fin[4], c), ldgH<T>(P, P.fin[5], c)};
+    const R eyk = kl ? R(0) : ldgE<T>(EY, c + 1), exk = kl ? R(0) : ldgE<T>(EX, c + 1);
+    const R ezj = jl ? R(0) : ldgE<T>(EZ, c + P.sj), exj = jl ? R(0) : ldgE<T>(EX, c + P.sj);
+    const R ezi = il ? R(0) : ldgE<T>(EZ, c + P.si), eyi = il ? R(0) : ldgE<T>(EY, c + P.si);
+    R h[3] = {ldgH<T>(P, P.fin[3], c), ldgH<T>(P, P.fin[4], c), ldgH<T>(P, P.fin[5], c)};
     const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
     h_update<T>(P, cl, cls_at(P, i, j, k), i, j, k, true, true, tsf, eyi - ey, ezi - ez, exj - ex, ezj - ez, exk - ex, eyk - ey, h);
     stH<T>(P, P.fout[3], c, h[0], stp, 3);
@@ -505,16 +186,17 @@ __global__ void __launch_bounds__(256, 3) slab_h_batch(const DevPlan *plans, con
 template <bool ADE, int NPOLES, class T>
 __device__ __forceinline__ void slab_e_cell(const DevPlan &P, int i, int j, int k, bool tsf)
 {
+    using R = real_t<T>;
     const uint32_t stp = sr_step<T>(P);
     const int64_t c = (int64_t)i * P.si + (int64_t)j * P.sj + k;
     const float *HX = P.fout[3], *HY = P.fout[4], *HZ = P.fout[5];   // H^{n+1/2}, written this step
-    const float3 eo = make_float3(ldgE<T>(P.fin[0], c), ldgE<T>(P.fin[1], c), ldgE<T>(P.fin[2], c));
-    const float3 h = make_float3(ldH<T>(P, HX, c), ldH<T>(P, HY, c), ldH<T>(P, HZ, c));
-    const float hx_jm = j > 0 ? ldH<T>(P, HX, c - P.sj) : 0.f, hz_jm = j > 0 ? ldH<T>(P, HZ, c - P.sj) : 0.f;
-    const float hx_km = k > 0 ? ldH<T>(P, HX, c - 1) : 0.f, hy_km = k > 0 ? ldH<T>(P, HY, c - 1) : 0.f;
-    const float hy_im = i > 0 ? ldH<T>(P, HY, c - P.si) : 0.f, hz_im = i > 0 ? ldH<T>(P, HZ, c - P.si) : 0.f;
+    const V3<R> eo{ldgE<T>(P.fin[0], c), ldgE<T>(P.fin[1], c), ldgE<T>(P.fin[2], c)};
+    const V3<R> h{ldH<T>(P, HX, c), ldH<T>(P, HY, c), ldH<T>(P, HZ, c)};
+    const R hx_jm = j > 0 ? ldH<T>(P, HX, c - P.sj) : R(0), hz_jm = j > 0 ? ldH<T>(P, HZ, c - P.sj) : R(0);
+    const R hx_km = k > 0 ? ldH<T>(P, HX, c - 1) : R(0), hy_km = k > 0 ? ldH<T>(P, HY, c - 1) : R(0);
+    const R hy_im = i > 0 ? ldH<T>(P, HY, c - P.si) : R(0), hz_im = i > 0 ? ldH<T>(P, HZ, c - P.si) : R(0);
     const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
-    const float3 en =
+    const V3<R> en =
         e_special<ADE, NPOLES, T>(P, cl, cls_at(P, i, j, k), i, j, k, tsf, eo, h, hx_jm, hz_jm, hx_km, hy_km, hy_im, hz_im);
     stE<T>(P.fout[0], c, en.x, stp, 0);
     stE<T>(P.fout[1], c, en.y, stp, 1);
@@ -544,8 +226,10 @@ __global__ void __launch_bounds__(256, 3) slab_e_batch(const DevPlan *plans, con
 // interpolation of dline.c:89-111 (FP64), projected by gex..ghz, scaled by
 // dt/(dx mu0) for H or (dt/dx)/epsilon(cell) for E, gated by TSF_SKIP, the
 // source-skip map and (k0 face) the PEC test.  Runs after aux_step.
+template <class R>
 __device__ __forceinline__ void tsf_face_cell(const DevPlan &P, int t)
 {
+    using V2 = typename Tab<R>::V2;
     const int i0 = P.t0[0], j0 = P.t0[1], k0 = P.t0[2], in = P.t1[0], jn = P.t1[1], kn = P.t1[2];
     const int ni = in - i0 + 1, nj = jn - j0 + 1, nk = kn - k0 + 1;
     const int sz[3] = {nj * nk, ni * nk, ni * nj};
@@ -556,7 +240,7 @@ __device__ __forceinline__ void tsf_face_cell(const DevPlan &P, int t)
     const int a = off / P.tnb[f], b = off % P.tnb[f];
     const uint8_t fl = P.tmap[f][off];
     const double hc = P.hcor;
-    float2 dh = make_float2(0.f, 0.f), de = make_float2(0.f, 0.f);
+    V2 dh{0, 0}, de{0, 0};
     const float4 *cls4 = reinterpret_cast<const float4 *>(P.classes);
     if (fl & 1) {
         int ei, ej, ek;   // E cell; dH / dE are the dcomp positions of the H and E corrections
@@ -579,61 +263,64 @@ __device__ __forceinline__ void tsf_face_cell(const DevPlan &P, int t)
         }
         const double ve = tsf_dval(P.aux_e, P.jres, dH);
         const double vh = tsf_dval(P.aux_h, P.jres, dE);
-        const double ce = (double)cls4[cls_at(P, ei, ej, ek) * 4 + 1].w;
+        const double ce = (double)Tab<R>::tsfe(P, cls4, cls_at(P, ei, ej, ek));
         const bool pec = (fl & 2) != 0;
         switch (f) {
         case 0:
-            if (ek < kn) dh.x = -(float)(hc * (ve * P.gez));
-            if (ej < jn) dh.y = (float)(hc * (ve * P.gey));
-            if (ej < jn) de.x = (float)(ce * (vh * P.ghz));
-            if (ek < kn) de.y = -(float)(ce * (vh * P.ghy));
+            if (ek < kn) dh.x = -(R)(hc * (ve * P.gez));
+            if (ej < jn) dh.y = (R)(hc * (ve * P.gey));
+            if (ej < jn) de.x = (R)(ce * (vh * P.ghz));
+            if (ek < kn) de.y = -(R)(ce * (vh * P.ghy));
             break;
         case 1:
-            if (ek < kn) dh.x = (float)(hc * (ve * P.gez));
-            if (ej < jn) dh.y = -(float)(hc * (ve * P.gey));
-            if (ej < jn) de.x = -(float)(ce * (vh * P.ghz));
-            if (ek < kn) de.y = (float)(ce * (vh * P.ghy));
+            if (ek < kn) dh.x = (R)(hc * (ve * P.gez));
+            if (ej < jn) dh.y = -(R)(hc * (ve * P.gey));
+            if (ej < jn) de.x = -(R)(ce * (vh * P.ghz));
+            if (ek < kn) de.y = (R)(ce * (vh * P.ghy));
             break;
         case 2:
-            if (ek < kn) dh.x = (float)(hc * (ve * P.gez));
-            if (ei < in) dh.y = -(float)(hc * (ve * P.gex));
-            if (ei < in) de.x = -(float)(ce * (vh * P.ghz));
-            if (ek < kn) de.y = (float)(ce * (vh * P.ghx));
+            if (ek < kn) dh.x = (R)(hc * (ve * P.gez));
+            if (ei < in) dh.y = -(R)(hc * (ve * P.gex));
+            if (ei < in) de.x = -(R)(ce * (vh * P.ghz));
+            if (ek < kn) de.y = (R)(ce * (vh * P.ghx));
             break;
         case 3:
-            if (ek < kn) dh.x = -(float)(hc * (ve * P.gez));
-            if (ei < in) dh.y = (float)(hc * (ve * P.gex));
-            if (ei < in) de.x = (float)(ce * (vh * P.ghz));
-            if (ek < kn) de.y = -(float)(ce * (vh * P.ghx));
+            if (ek < kn) dh.x = -(R)(hc * (ve * P.gez));
+            if (ei < in) dh.y = (R)(hc * (ve * P.gex));
+            if (ei < in) de.x = (R)(ce * (vh * P.ghz));
+            if (ek < kn) de.y = -(R)(ce * (vh * P.ghx));
             break;
         case 4:
-            if (ej < jn && !pec) dh.x = -(float)(hc * (ve * P.gey));
-            if (ei < in && !pec) dh.y = (float)(hc * (ve * P.gex));
-            if (ei < in && !pec) de.x = (float)(ce * (vh * P.ghy));
-            if (ej < jn && !pec) de.y = -(float)(ce * (vh * P.ghx));
+            if (ej < jn && !pec) dh.x = -(R)(hc * (ve * P.gey));
+            if (ei < in && !pec) dh.y = (R)(hc * (ve * P.gex));
+            if (ei < in && !pec) de.x = (R)(ce * (vh * P.ghy));
+            if (ej < jn && !pec) de.y = -(R)(ce * (vh * P.ghx));
             break;
         default:
-            if (ej < jn) dh.x = (float)(hc * (ve * P.gey));
-            if (ei < in) dh.y = -(float)(hc * (ve * P.gex));
-            if (ei < in) de.x = -(float)(ce * (vh * P.ghy));
-            if (ej < jn) de.y = (float)(ce * (vh * P.ghx));
+            if (ej < jn) dh.x = (R)(hc * (ve * P.gey));
+            if (ei < in) dh.y = -(R)(hc * (ve * P.gex));
+            if (ei < in) de.x = -(R)(ce * (vh * P.ghy));
+            if (ej < jn) de.y = (R)(ce * (vh * P.ghx));
             break;
         }
     }
-    P.tcor_h[f][off] = dh;
-    P.tcor_e[f][off] = de;
+    reinterpret_cast<V2 *>(P.tcor_h[f])[off] = dh;
+    reinterpret_cast<V2 *>(P.tcor_e[f])[off] = de;
     (void)a; (void)b;
 }
 
 __global__ void tsf_face_kernel(const __grid_constant__ DevPlan P, int total)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < total) tsf_face_cell(P, t);
+    if (t < total) {
+        if (P.real64) tsf_face_cell<double>(P, t);
+        else tsf_face_cell<float>(P, t);
+    }
 }
 
 __global__ void tsf_face_batch(const DevPlan *plans)
 {
-    tsf_face_cell(plans[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
+    tsf_face_cell<float>(plans[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------------ 1D aux grid
@@ -648,7 +335,7 @@ __device__ __forceinline__ void aux_step_body(const DevAux &A)
     if (s > 0 && s - 1 < A.nsteps_planned) {
         for (int q = tid; q < A.nprobes * 6; q += nt) {
             int p = q / 6, comp = q % 6;
-            A.probe_out[((size_t)p * A.nsteps_planned + (s - 1)) * 6 + comp] = (double)(ld_any(A.fields[comp], A.probe_cells[p], A.storage) * (comp >= 3 && A.storage ? A.ihs : 1.f));
+            A.probe_out[((size_t)p * A.nsteps_planned + (s - 1)) * 6 + comp] = ld_any(A.fields[comp], A.probe_cells[p], A.storage) * (comp >= 3 ? (double)A.ihs : 1.0);
         }
     }
     if (A.res > 0) {
@@ -685,7 +372,7 @@ __global__ void probe_capture_kernel(const DevAux A)
     if (s < 1 || s - 1 >= A.nsteps_planned) return;
     for (int q = threadIdx.x; q < A.nprobes * 6; q += blockDim.x) {
         int p = q / 6, comp = q % 6;
-        A.probe_out[((size_t)p * A.nsteps_planned + (s - 1)) * 6 + comp] = (double)(ld_any(A.fields[comp], A.probe_cells[p], A.storage) * (comp >= 3 && A.storage ? A.ihs : 1.f));
+        A.probe_out[((size_t)p * A.nsteps_planned + (s - 1)) * 6 + comp] = ld_any(A.fields[comp], A.probe_cells[p], A.storage) * (comp >= 3 ? (double)A.ihs : 1.0);
     }
 }
 
@@ -712,15 +399,18 @@ __device__ __forceinline__ void nfff_twiddles(const DevNfff &N, int first_step, 
     __syncthreads();
 }
 
-// tw: the CTA's twiddle table, or nullptr to evaluate them per cell
+// tw: the CTA's twiddle table, or nullptr to evaluate them per cell.  S: the
+// element type of the sample ring (FP32; FP64 for FP64-storage plans)
+template <class S>
 __device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_step, int nslots, bool clear, const double2 *tw)
 {
     const size_t ns = (size_t)N.ns;
+    S *ring = reinterpret_cast<S *>(N.ring);
     for (int f = 0; f < N.nfreq; f++) {
         double2 A[6];
         for (int q = 0; q < 6; q++) A[q] = N.acc[((size_t)f * 6 + q) * ns + s];
         for (int j = 0; j < nslots; j++) {
-            const float *r = N.ring + (size_t)j * 9 * ns + s;
+            const S *r = ring + (size_t)j * 9 * ns + s;
             double v[6];
             for (int a = 0; a < 3; a++) {
                 v[a] = (double)r[(3 * a) * ns];
@@ -738,12 +428,13 @@ __device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_ste
     }
     if (clear)
         for (int j = 0; j < nslots; j++)
-            for (int q = 0; q < 9; q++) N.ring[((size_t)j * 9 + q) * ns + s] = 0.f;
+            for (int q = 0; q < 9; q++) ring[((size_t)j * 9 + q) * ns + s] = 0;
 }
 
 // the step counter, the slot and the fold decision are the same for every
 // thread of a launch (one plan per CTA in a batch), so the CTA-wide twiddle
 // table and its barrier are reached by all threads
+template <class S>
 __device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
 {
     if (N.ns <= 0 || N.nfreq <= 0) return;   // a batch instance without a running DFT: zeroed, no step counter
@@ -755,19 +446,19 @@ __device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
     if (live) {
         const int64_t c = N.cell[s];
         const int64_t st = N.nstride[s];
-        float *r = N.ring + (size_t)slot * 9 * ns + s;
+        S *r = reinterpret_cast<S *>(N.ring) + (size_t)slot * 9 * ns + s;
         for (int a = 0; a < 3; a++) {
             const float *E = N.e[a];
-            r[(3 * a) * ns] = ld_any(E, c, N.storage);
-            r[(3 * a + 1) * ns] = ld_any(E, c + st, N.storage);
-            r[(3 * a + 2) * ns] = ld_any(E, c - st, N.storage);
+            r[(3 * a) * ns] = (S)ld_any(E, c, N.storage);
+            r[(3 * a + 1) * ns] = (S)ld_any(E, c + st, N.storage);
+            r[(3 * a + 2) * ns] = (S)ld_any(E, c - st, N.storage);
         }
     }
     if (slot == NFFF_RING - 1) {
         __shared__ double2 tw[NFFF_RING * NFFF_TW_MAXF];
         const bool table = N.nfreq <= NFFF_TW_MAXF;
         if (table) nfff_twiddles(N, step - (NFFF_RING - 1), NFFF_RING, tw);
-        if (live) nfff_fold(N, s, step - (NFFF_RING - 1), NFFF_RING, false, table ? tw : nullptr);
+        if (live) nfff_fold<S>(N, s, step - (NFFF_RING - 1), NFFF_RING, false, table ? tw : nullptr);
     }
 }
 
@@ -783,14 +474,21 @@ __global__ void nfff_fold_pending_kernel(const DevNfff N)
     __shared__ double2 tw[NFFF_RING * NFFF_TW_MAXF];
     const bool table = N.nfreq <= NFFF_TW_MAXF;
     if (table) nfff_twiddles(N, done - pending, pending, tw);
-    if (s < N.ns) nfff_fold(N, s, done - pending, pending, true, table ? tw : nullptr);
+    if (s < N.ns) {
+        if (N.storage == FDTD_STORE_F64) nfff_fold<double>(N, s, done - pending, pending, true, table ? tw : nullptr);
+        else nfff_fold<float>(N, s, done - pending, pending, true, table ? tw : nullptr);
+    }
 }
 
-__global__ void nfff_accumulate_kernel(const DevNfff N) { nfff_accumulate_cell(N, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void nfff_accumulate_kernel(const DevNfff N)
+{
+    if (N.storage == FDTD_STORE_F64) nfff_accumulate_cell<double>(N, blockIdx.x * blockDim.x + threadIdx.x);
+    else nfff_accumulate_cell<float>(N, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 __global__ void nfff_accumulate_batch(const DevNfff *N)
 {
-    nfff_accumulate_cell(N[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
+    nfff_accumulate_cell<float>(N[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------------ far-field integration
@@ -966,10 +664,14 @@ void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st)
 template <class T>
 cudaError_t slab_steps_t(const DevPlan &p, const SlabLists &L, bool ade, int npoles, cudaStream_t st)
 {
-    if (L.h4blocks > 0)
-        slab_h4_kernel<T><<<(unsigned)L.h4blocks, 256, 0, st>>>(p, L.h4, L.nh);
-    else
-        slab_h_kernel<T><<<(unsigned)L.hblocks, 256, 0, st>>>(p, L.h, L.nh);
+    bool h4 = false;
+    if constexpr (sizeof(T) <= 4) {   // 4-cell groups: FP32 and 16-bit storage
+        if (L.h4blocks > 0) {
+            slab_h4_kernel<T><<<(unsigned)L.h4blocks, 256, 0, st>>>(p, L.h4, L.nh);
+            h4 = true;
+        }
+    }
+    if (!h4) slab_h_kernel<T><<<(unsigned)L.hblocks, 256, 0, st>>>(p, L.h, L.nh);
     if (L.eblocks > 0) {
         if (!ade)
             slab_e_kernel<false, 0, T><<<(unsigned)L.eblocks, 256, 0, st>>>(p, L.e, L.ne);
@@ -985,6 +687,7 @@ cudaError_t slab_steps_t(const DevPlan &p, const SlabLists &L, bool ade, int npo
 cudaError_t launch_slab_steps(const DevPlan &p, const SlabLists &L, bool ade, int npoles, int storage, cudaStream_t st)
 {
     if (L.hblocks <= 0) return cudaSuccess;
+    if (storage == FDTD_STORE_F64) return slab_steps_t<double>(p, L, ade, npoles, st);
     if (storage == FDTD_STORE_F16) return slab_steps_t<__half>(p, L, ade, npoles, st);
     if (storage == FDTD_STORE_BF16) return slab_steps_t<__nv_bfloat16>(p, L, ade, npoles, st);
     return slab_steps_t<float>(p, L, ade, npoles, st);

@@ -36,7 +36,8 @@ struct DevNfff {
     const int32_t *nstride;     // +/- stride along the face normal
     const float *const *e;      // 3 E field pointers (the set written by this step)
     double2 *acc;               // [(f*6 + q)*ns + s], q = Ex,Ey,Ez, dEx,dEy,dEz
-    float *ring;                // NFFF_RING steps of raw samples [(slot*9 + 3a + r)*ns + s], r: E(c), E(c+st), E(c-st)
+    float *ring;                // NFFF_RING steps of raw samples [(slot*9 + 3a + r)*ns + s], r: E(c), E(c+st), E(c-st);
+                                // FP32 elements (FP64 for FDTD_STORE_F64 plans)
     const double *omega_dt;     // nfreq
     const int *step;            // device step counter (already advanced)
     double inv2dx;

@@ -179,17 +179,23 @@ void cpml_grade(int pos, int imax, double sigma, double kappa, double a, int m, 
     *kh = kvh;
 }
 
+// a cell's class: the FP32 coefficients, and the FP64 ones for FP64 plans
+// (zero otherwise, so that FP32 plans deduplicate on the FP32 values alone)
+struct ClassKey {
+    DevClass c;
+    DevClass64 d;
+};
 struct ClassHash {
-    size_t operator()(const DevClass &c) const
+    size_t operator()(const ClassKey &c) const
     {
         const uint32_t *w = reinterpret_cast<const uint32_t *>(&c);
         size_t h = 1469598103934665603ull;
-        for (size_t q = 0; q < sizeof(DevClass) / 4; q++) h = (h ^ w[q]) * 1099511628211ull;
+        for (size_t q = 0; q < sizeof(ClassKey) / 4; q++) h = (h ^ w[q]) * 1099511628211ull;
         return h;
     }
 };
 struct ClassEq {
-    bool operator()(const DevClass &a, const DevClass &b) const { return std::memcmp(&a, &b, sizeof(DevClass)) == 0; }
+    bool operator()(const ClassKey &a, const ClassKey &b) const { return std::memcmp(&a, &b, sizeof(ClassKey)) == 0; }
 };
 
 }  // namespace
@@ -201,9 +207,11 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
     if (!(d->dt > 0) || !(d->dx > 0)) { *err = "dt and dx must be positive"; return FDTD_E_INVALID; }
     if (d->dx != d->dy || d->dx != d->dz) { *err = "non-cubic cells are outside the implemented path"; return FDTD_E_UNSUPPORTED; }
     if (d->nmat > 0 && !d->mats) { *err = "nmat > 0 but mats is NULL"; return FDTD_E_INVALID; }
-    if (d->storage != FDTD_STORE_F32 && d->storage != FDTD_STORE_F16 && d->storage != FDTD_STORE_BF16) {
+    if (d->storage != FDTD_STORE_F32 && d->storage != FDTD_STORE_F16 && d->storage != FDTD_STORE_BF16 &&
+        d->storage != FDTD_STORE_F64) {
         *err = "unknown storage mode"; return FDTD_E_INVALID;
     }
+    hp->real64 = d->storage == FDTD_STORE_F64;
     for (int m = 1; m < d->nmat; m++) {
         int t = d->mats[m].type;
         if (t != FDTD_MAT_LINTAB && t != FDTD_MAT_ADE && t != FDTD_MAT_PEC) {
@@ -365,23 +373,36 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
         if (d->mats[m].type != FDTD_MAT_ADE) continue;
         if ((int)hp->ades.size() >= FDTD_MAX_ADE) { *err = "too many ADE materials"; return FDTD_E_UNSUPPORTED; }
         const fdtd_material &q = d->mats[m];
+        DevAde64 w;   // the difference-form set in FP64 (DevAde)
+        std::memset(&w, 0, sizeof(w));
+        w.c0dx = q.ade_c0 / dx;
+        w.c2 = q.ade_c2; w.c3 = q.ade_c3;
+        w.qe = q.ade_c1 * q.ade_a0;
+        w.ma0 = -q.ade_a0;
+        w.a2 = q.ade_a2;
+        for (int p = 0; p < 2; p++) {
+            w.pe[p] = q.ade_c1 * ((1.0 - q.ade_bp0[p]) - q.ade_bp1[p]);
+            w.qpe[p] = q.ade_c1 * q.ade_bp0[p];
+            w.rp[p] = (q.ade_bp0[p] + q.ade_bp1[p]) - 1.0;
+            w.rq[p] = -q.ade_bp0[p];
+            w.bp2[p] = q.ade_bp2[p]; w.bp3[p] = q.ade_bp3[p]; w.bp4[p] = q.ade_bp4[p];
+            if (q.ade_bp2[p] != 0 || q.ade_bp3[p] != 0 || q.ade_bp4[p] != 0) hp->maxpoles = 2;
+        }
         DevAde a;
         std::memset(&a, 0, sizeof(a));
-        a.c0dx = (float)(q.ade_c0 / dx);
-        a.c2 = (float)q.ade_c2; a.c3 = (float)q.ade_c3;
-        a.qe = (float)(q.ade_c1 * q.ade_a0);
-        a.ma0 = (float)(-q.ade_a0);
-        a.a2 = (float)q.ade_a2;
+        a.c0dx = (float)w.c0dx;
+        a.c2 = (float)w.c2; a.c3 = (float)w.c3;
+        a.qe = (float)w.qe;
+        a.ma0 = (float)w.ma0;
+        a.a2 = (float)w.a2;
         for (int p = 0; p < 2; p++) {
-            a.pe[p] = (float)(q.ade_c1 * ((1.0 - q.ade_bp0[p]) - q.ade_bp1[p]));
-            a.qpe[p] = (float)(q.ade_c1 * q.ade_bp0[p]);
-            a.rp[p] = (float)((q.ade_bp0[p] + q.ade_bp1[p]) - 1.0);
-            a.rq[p] = (float)(-q.ade_bp0[p]);
-            a.bp2[p] = (float)q.ade_bp2[p]; a.bp3[p] = (float)q.ade_bp3[p]; a.bp4[p] = (float)q.ade_bp4[p];
-            if (q.ade_bp2[p] != 0 || q.ade_bp3[p] != 0 || q.ade_bp4[p] != 0) hp->maxpoles = 2;
+            a.pe[p] = (float)w.pe[p]; a.qpe[p] = (float)w.qpe[p];
+            a.rp[p] = (float)w.rp[p]; a.rq[p] = (float)w.rq[p];
+            a.bp2[p] = (float)w.bp2[p]; a.bp3[p] = (float)w.bp3[p]; a.bp4[p] = (float)w.bp4[p];
         }
         ade_slot[m] = (int)hp->ades.size();
         hp->ades.push_back(a);
+        hp->ades64.push_back(w);
     }
 
     // per-cell classes, deduplicated; thread-local tables merged afterwards
@@ -389,8 +410,9 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
 #ifdef _OPENMP
     nthr = omp_get_max_threads();
 #endif
-    std::vector<std::vector<DevClass>> local(nthr);
-    std::vector<std::unordered_map<DevClass, int, ClassHash, ClassEq>> lmap(nthr);
+    std::vector<std::vector<ClassKey>> local(nthr);
+    std::vector<std::unordered_map<ClassKey, int, ClassHash, ClassEq>> lmap(nthr);
+    const bool r64 = hp->real64;
     std::vector<int> plane_owner(xr, 0);
     std::vector<uint16_t> lid(n);
     std::string perr;
@@ -404,13 +426,17 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
         plane_owner[i] = tid;
         for (int j = 0; j < yr; j++)
             for (int k = 0; k < zr; k++) {
-                DevClass c;
-                std::memset(&c, 0, sizeof(c));
+                ClassKey key;
+                std::memset(&key, 0, sizeof(key));
+                DevClass &c = key.c;
+                DevClass64 &w = key.d;   // stays zero for FP32 plans
                 int xt, yt, zt;
                 int m = get_tbc(g, i, j, k, &xt, &yt, &zt);
                 double ca[3], cb[3];
                 get_cabs(g, hp->bnds, i, j, k, dt, dx, ca, cb);
                 for (int a = 0; a < 3; a++) { c.ca[a] = (float)ca[a]; c.cb[a] = (float)cb[a]; }
+                if (r64)
+                    for (int a = 0; a < 3; a++) { w.ca[a] = ca[a]; w.cb[a] = cb[a]; }
                 if (disp && xt * yt * zt == 0) {
                     c.flags |= CF_ADE_BRANCH;
                     if (!xt) c.flags |= CF_ADE_X;
@@ -420,6 +446,7 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
                     const fdtd_material &q = d->mats[m];
                     double cba = (dt / q.epsilon / dx) / (1 + q.sigma * dt / 2 / q.epsilon);
                     c.cba[0] = c.cba[1] = c.cba[2] = (float)cba;
+                    if (r64) w.cba[0] = w.cba[1] = w.cba[2] = cba;
                 }
                 // H coefficients (ystep_h, yee.c:213-243)
                 int mi = g.mat(i, j, k);
@@ -439,11 +466,13 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
                 c.da = (float)da;
                 c.db = (float)db;
                 c.tsfe = (float)(ecor / g.eps(i, j, k));
+                if (r64) { w.da = da; w.db = db; w.tsfe = ecor / g.eps(i, j, k); }
                 const bool affected = hp->design && i >= hp->abox[0] && i < hp->abox[1] && j >= hp->abox[2] &&
                                       j < hp->abox[3] && k >= hp->abox[4] && k < hp->abox[5];
                 if (affected) {   // E coefficients per cell (design_coefficients); no TSF face here
-                    for (int a = 0; a < 3; a++) { c.ca[a] = 0.f; c.cb[a] = 0.f; }
+                    for (int a = 0; a < 3; a++) { c.ca[a] = 0.f; c.cb[a] = 0.f; w.ca[a] = 0; w.cb[a] = 0; }
                     c.tsfe = 0.f;
+                    w.tsfe = 0;
                     c.flags |= CF_DESIGN;
                 }
                 // PEC rule, yee.c:1138-1237 (no SF source on this path)
@@ -463,19 +492,20 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
                         if (tyz == P && t0 != P) c.flags |= CF_PEC_X;
                     }
                 }
+                if (r64) { w.flags = c.flags; w.ade = c.ade; }
                 auto &mp = lmap[tid];
-                auto it = mp.find(c);
+                auto it = mp.find(key);
                 int id;
                 if (it == mp.end()) {
                     id = (int)local[tid].size();
-                    local[tid].push_back(c);
-                    mp.emplace(c, id);
+                    local[tid].push_back(key);
+                    mp.emplace(key, id);
                 } else
                     id = it->second;
                 lid[g.idx(i, j, k)] = (uint16_t)std::min(id, 65535);
             }
     }
-    std::unordered_map<DevClass, int, ClassHash, ClassEq> gmap;
+    std::unordered_map<ClassKey, int, ClassHash, ClassEq> gmap;
     std::vector<std::vector<int>> remap(nthr);
     for (int t = 0; t < nthr; t++) {
         for (auto &c : local[t]) {
@@ -483,7 +513,8 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
             int id;
             if (it == gmap.end()) {
                 id = (int)hp->classes.size();
-                hp->classes.push_back(c);
+                hp->classes.push_back(c.c);
+                if (r64) hp->classes64.push_back(c.d);
                 gmap.emplace(c, id);
             } else
                 id = it->second;
@@ -510,11 +541,13 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
         bool low = (f % 2 == 0);
         hp->be[f].resize(dep); hp->ce[f].resize(dep); hp->bh[f].resize(dep); hp->ch[f].resize(dep);
         hp->ke[f].resize(dep); hp->kh[f].resize(dep);
+        hp->be64[f].resize(dep); hp->ce64[f].resize(dep); hp->bh64[f].resize(dep); hp->ch64[f].resize(dep);
         for (int q = 0; q < dep; q++) {
             double be, ce, bh, ch, ke, kh;
             cpml_grade(low ? q : dep - q, dep, d->cpml[f].sigma, d->cpml[f].kappa, d->cpml[f].a, d->cpml[f].m, dt, low,
                        &be, &ce, &bh, &ch, &ke, &kh);
             hp->be[f][q] = (float)be; hp->ce[f][q] = (float)ce; hp->bh[f][q] = (float)bh; hp->ch[f][q] = (float)ch;
+            hp->be64[f][q] = be; hp->ce64[f][q] = ce; hp->bh64[f][q] = bh; hp->ch64[f][q] = ch;
             hp->ke[f][q] = ke; hp->kh[f][q] = kh;
         }
     }
@@ -522,6 +555,8 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
         int res = ax == 0 ? xr : ax == 1 ? yr : zr;
         hp->ike[ax].assign(res, 1.0f);
         hp->ikh[ax].assign(res, 1.0f);
+        hp->ike64[ax].assign(res, 1.0);
+        hp->ikh64[ax].assign(res, 1.0);
         for (int q = 0; q < res; q++) {
             double ke = 1, kh = 1;
             int f0 = 2 * ax, fn = 2 * ax + 1;
@@ -535,6 +570,8 @@ int build_host_plan(const fdtd_desc *d, HostPlan *hp, std::string *err)
             }
             hp->ike[ax][q] = (float)(1.0 / ke);
             hp->ikh[ax][q] = (float)(1.0 / kh);
+            hp->ike64[ax][q] = 1.0 / ke;
+            hp->ikh64[ax][q] = 1.0 / kh;
         }
     }
     // probes
@@ -587,6 +624,7 @@ void design_coefficients(HostPlan *hp, const double *eps_r)
             for (int k = dbx[4]; k < dbx[5]; k++, q++) hp->ctx_eps[cidx(i, j, k)] = eps_r[q] * EPS0;
     const size_t na = (size_t)(a[1] - a[0]) * (a[3] - a[2]) * (a[5] - a[4]);
     hp->dcoef.assign(6 * na, 0.f);
+    hp->dcoef64.assign(6 * na, 0.0);
     const double dt = hp->dt, dx = hp->dx;
     q = 0;
     for (int i = a[0]; i < a[1]; i++)
@@ -608,8 +646,10 @@ void design_coefficients(HostPlan *hp, const double *eps_r)
                 }
                 const double E[3] = {ex, ey, ez}, S[3] = {sx, sy, sz};
                 for (int c = 0; c < 3; c++) {
-                    hp->dcoef[6 * q + c] = (float)((1 - S[c] * dt / 2 / E[c]) / (1 + S[c] * dt / 2 / E[c]));
-                    hp->dcoef[6 * q + 3 + c] = (float)((dt / E[c] / dx) / (1 + S[c] * dt / 2 / E[c]));
+                    hp->dcoef64[6 * q + c] = (1 - S[c] * dt / 2 / E[c]) / (1 + S[c] * dt / 2 / E[c]);
+                    hp->dcoef64[6 * q + 3 + c] = (dt / E[c] / dx) / (1 + S[c] * dt / 2 / E[c]);
+                    hp->dcoef[6 * q + c] = (float)hp->dcoef64[6 * q + c];
+                    hp->dcoef[6 * q + 3 + c] = (float)hp->dcoef64[6 * q + 3 + c];
                 }
             }
 }

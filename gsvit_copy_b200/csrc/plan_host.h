@@ -15,6 +15,14 @@ struct HostPlan {
     std::vector<uint8_t> cls;            // per-cell class index
     std::vector<DevClass> classes;
     std::vector<DevAde> ades;
+    // FDTD_STORE_F64 plans: the same tables in FP64 (classes then deduplicated
+    // on the FP64 coefficients, so classes64[c] rounds to classes[c])
+    bool real64 = false;
+    std::vector<DevClass64> classes64;
+    std::vector<DevAde64> ades64;
+    std::vector<double> be64[6], ce64[6], bh64[6], ch64[6];
+    std::vector<double> ike64[3], ikh64[3];
+    std::vector<double> dcoef64;
     bool has_ade = false;
     int maxpoles = 0;
     std::vector<int8_t> bnds, sskip;     // derived maps (plan.c:5387-5416, 5298-5326)

@@ -85,6 +85,13 @@ extern "C" {
 #define FDTD_STORE_F32   0
 #define FDTD_STORE_F16   1
 #define FDTD_STORE_BF16  2
+/* Reference precision: fields, psi slabs and the Drude/critical-point state
+ * stored in FP64 and every update computed in FP64 from FP64 coefficient
+ * tables, one thread per cell on the general kernels (the arithmetic of
+ * GSvit's CPU path, yee.c:145-1247, boundary.c, source.c).  Meant for
+ * pinning the FP32 and 16-bit runs at sizes the CPU oracle cannot reach; no
+ * batches, no adjoint.  No counterpart in the reference's GPU path. */
+#define FDTD_STORE_F64   3
 
 /* field component bit mask (copy-in / copy-out), cf. SvGpuSync pool.h:49-54 */
 #define FDTD_EX 0x01
