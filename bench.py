@@ -64,11 +64,18 @@ def parse():
     ap.add_argument("--res", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extensions", action="store_true",
+                    help="skip the extensions block (FP16 / BF16 storage and the batched instances)")
+    ap.add_argument("--ext-steps", type=int, default=20, help="timed steps of each extensions measurement")
     ap.add_argument("--adj-steps", type=int, default=4000, help="adjoint workload: forward steps")
     ap.add_argument("--fd-cells", type=int, default=16, help="adjoint workload: cells checked by finite differences")
-    ap.add_argument("--fd-h", type=float, default=0.1, help="adjoint workload: finite-difference step on eps_r")
-    ap.add_argument("--workload", choices=["rough512", "batched", "adjoint"], default="rough512",
-                    help="batched: 48 uneven rough-surface instances in one batch against the same run one by one")
+    ap.add_argument("--fd-h", type=float, default=1e-3, help="adjoint workload: finite-difference step on eps_r")
+    ap.add_argument("--fd-storage", choices=["f64", "f32"], default="f64",
+                    help="adjoint workload: field storage of the finite-difference runs")
+    ap.add_argument("--prec-steps", type=int, default=4000, help="precision workload: steps of every run")
+    ap.add_argument("--workload", choices=["rough512", "batched", "adjoint", "precision"], default="rough512",
+                    help="batched: 48 uneven rough-surface instances in one batch against the same run one by one; "
+                         "precision: FP32 / FP16 / BF16 storage against the FP64 reference-precision run")
     return ap.parse_args()
 
 
@@ -233,17 +240,51 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(res):
-    """DRAM bytes per launch of the bulk kernel from the committed ncu launch list of this workload."""
+def ncu_traffic(res, kernel="bulk_kernel"):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary of this workload."""
     path = os.path.join(HERE, "profiles", f"launches_rough{res}.txt")
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("bulk_kernel dram_bytes_per_launch:"):
+                if line.startswith(f"{kernel} dram_bytes_per_launch:"):
                     return float(line.split(":", 1)[1].split()[0])
     except OSError:
         pass
     return None
+
+
+KERNEL_NAMES = {
+    "bulk": "tile_kernel, bulk layout (TMA-staged fused H+E step of the interior box)",
+    "cpml": "tile_kernel, CPML layouts (TMA-staged fused H+E step with psi, kappa and ADE-in-CPML)",
+}
+
+
+def kernel_rooflines(prof, nprof, step_bytes, step_ms, peak, peak_kind, res):
+    """Per-kernel figures of one step from fdtd_step_profile (CUDA events
+    around each launch group): device ms, algorithmic bytes, achieved GB/s and
+    the fraction of the HBM peak; the roofline block is the kernel with the
+    largest share of the step."""
+    total = prof["total_ms"] / nprof
+    ks = {}
+    for key, ms_key, b_key in (("bulk", "bulk_ms", "bulk_bytes"), ("cpml", "slab_ms", "slab_bytes")):
+        ms = prof[ms_key] / nprof
+        b = prof[b_key]
+        gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else None
+        ks[key] = {"kernel": KERNEL_NAMES[key], "ms_per_launch": ms, "algorithmic_bytes": b, "achieved_gbs": gbs,
+                   "frac": gbs / peak if gbs else None, "step_share": ms / total if total else None}
+    ks["aux_tsf"] = {"kernel": "1D aux grid + TSF face tables", "ms_per_step": prof["aux_ms"] / nprof,
+                     "step_share": prof["aux_ms"] / nprof / total if total else None}
+    ks["nfff"] = {"kernel": "NFFF surface samples + running-DFT fold", "ms_per_step": prof["nfff_ms"] / nprof,
+                  "step_share": prof["nfff_ms"] / nprof / total if total else None}
+    top = max(("bulk", "cpml"), key=lambda k: ks[k]["ms_per_launch"])
+    t = ks[top]
+    roofline = {"kernel": t["kernel"], "bound": "hbm", "achieved": t["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                "frac": t["frac"], "peak_source": peak_kind,
+                "traffic": ncu_traffic(res, "bulk_kernel" if top == "bulk" else "cpml_tiles"),
+                "algorithmic_bytes": t["algorithmic_bytes"], "ms_per_launch": t["ms_per_launch"],
+                "step_share": t["step_share"]}
+    step_gbs = step_bytes / (step_ms * 1e-3) / 1e9
+    return roofline, ks, {"achieved": step_gbs, "frac": step_gbs / peak, "bytes": step_bytes, "ms": step_ms}
 
 
 # ----------------------------------------------------------------- CPU sample
@@ -331,21 +372,13 @@ def run_b200(a):
     # per-kernel profile of a few more steps (CUDA events around each launch)
     prof = g.step_profile(8)
     nprof = 8
-    bulk_s = prof["bulk_ms"] / nprof * 1e-3
     peak, peak_kind = hbm_peak()
-    achieved = prof["bulk_bytes"] / bulk_s / 1e9 if bulk_s > 0 else None
-    roofline = {"kernel": "bulk_kernel (TMA-tiled fused H+E step of the interior box)", "bound": "hbm",
-                "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
-                "traffic": ncu_traffic(a.res), "algorithmic_bytes": prof["bulk_bytes"],
-                "ms_per_launch": prof["bulk_ms"] / nprof,
-                "step_share": prof["bulk_ms"] / prof["total_ms"] if prof["total_ms"] else None}
+    step_bytes = g.step_bytes()
+    roofline, kernels, step_roof = kernel_rooflines(prof, nprof, step_bytes, ms / K, peak, peak_kind, a.res)
     # far-field integration of the accumulated running DFTs (once per run)
     t0 = time.perf_counter()
     spec = g.nfff_spectrum()
     ff_ms = (time.perf_counter() - t0) * 1e3
-    step_bytes = g.step_bytes()
-    step_gbs = step_bytes / (ms / K * 1e-3) / 1e9
     # the step kernels of K steps, then the probe capture that closes fdtd_step
     gpu_launches = int(prof["launches_per_step"]) * K + (1 if scene.probes is not None and len(scene.probes) else 0)
 
@@ -374,6 +407,10 @@ def run_b200(a):
     g.close()
     barrier()
 
+    ext = None
+    if rank == 0 and world == 1 and not a.no_extensions:
+        ext = extensions(a, local)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         v, thr, kind, n = cpu_sample_run(budget_s=a.cpu_seconds)
@@ -387,15 +424,89 @@ def run_b200(a):
             "dtype": "f32", "data": "synthetic (seeded Gaussian-correlated height map)",
             "config": config_block(a.res, scene), "clocks": clocks, "e2e": e2e,
             "gpu_launches": gpu_launches, "roofline": roofline,
-            "step_gbs_algorithmic": step_gbs, "step_bytes_algorithmic": step_bytes,
-            "kernel_ms_per_step": {k: prof[k] / nprof for k in ("bulk_ms", "slab_ms", "aux_ms", "nfff_ms", "total_ms")},
+            "step_roofline": step_roof, "step_roofline_frac": step_roof["frac"],
+            "kernels": kernels,
             "farfield_finalize_ms": ff_ms,
             "farfield_points": int(spec.shape[0]),
+            "extensions": ext,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     ranks.close()
     return 0
+
+
+def timed_steps(g, K, W, stream):
+    """Device time (ms) of K steps of solver g on `stream` after W warm-up steps."""
+    import torch
+    g.set_stream(stream.cuda_stream)
+    g.step(W)
+    g.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    g.step(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    g.sync()
+    return e0.elapsed_time(e1)
+
+
+def storage_measure(res, storage, K, W, device):
+    """Gcell-updates/s of the rough-surface workload with 16-bit field storage."""
+    import torch
+    from gsvit_copy_b200.solver import Solver
+    scene = workload_scene(res, max(4000, K + W + 64))
+    scene.storage = storage
+    stream = torch.cuda.Stream()
+    g = Solver(scene, device=device)
+    ms = timed_steps(g, K, W, stream)
+    g.close()
+    return scene.ncells * K / (ms * 1e-3) / 1e9, ms / K
+
+
+def batched_measure(K, W, nscenes=48, tune_steps=2):
+    """The batched instances (plan.batch_scenes) stepped as one batch from CUDA
+    graphs after the tuner picked the bulk work list; device-synchronised host
+    clock around K steps."""
+    import torch
+    from gsvit_copy_b200 import plan
+    from gsvit_copy_b200.solver import Batch
+    scenes = plan.batch_scenes(nscenes, nsteps=max(2000, K + W + 64))
+    cells = sum(sc.ncells for sc in scenes)
+    batch = Batch(scenes)
+    tune = batch.tune(trial_steps=tune_steps)
+    cfg = batch.config()
+    batch.step_graph(W + (W % 2), chunk=16)
+    batch.sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.step_graph(K, chunk=16)
+    batch.sync()
+    dt = time.perf_counter() - t0
+    batch.close()
+    return cells, cells * K / dt / 1e9, dt / K * 1e3, cfg, tune
+
+
+def extensions(a, device):
+    """Figures of the library's extensions beyond GSvit's FP32 path, on this
+    box, each a separate short run after the headline (not part of `value`):
+    the same workload with FP16 and BF16 field storage, and 48 uneven
+    instances stepped as one batch."""
+    from gsvit_copy_b200 import abi
+    K, W = a.ext_steps, 3
+    out = {}
+    for name, st in (("fp16_storage", abi.STORE_F16), ("bf16_storage", abi.STORE_BF16)):
+        v, msps = storage_measure(a.res, st, K, W, device)
+        out[name] = {"value": v, "unit": UNIT, "ms_per_step": msps, "steps": K, "warmup": W,
+                     "workload": f"rough Drude-silver surface {a.res}^3 (as the headline), {name[:4].upper()} "
+                                 "fields / psi / E^n-1 in HBM, FP32 arithmetic"}
+    cells, v, msps, cfg, tune = batched_measure(K, W)
+    out["batched_48"] = {"value": v, "unit": UNIT, "ms_per_step": msps, "steps": K, "cells": cells,
+                         "workload": "48 rough-surface instances, x,y in {64,96,128,192}, z in {64,96,128}, "
+                                     "Drude or Lorentz, 8-cell CPML, one batch",
+                         "bulk_work_list": cfg, "timing": "host clock around synchronised device work"}
+    return out
 
 
 def run_batched(a):
@@ -485,6 +596,18 @@ def run_adjoint(a):
     adj_s = time.perf_counter() - t0
     fd = None
     if a.fd_cells > 0:
+        # central differences of J; with --fd-storage f64 through a plan of the
+        # same scene with FP64 fields and arithmetic, so that h = 1e-3 is not
+        # drowned by FP32 rounding
+        from gsvit_copy_b200 import abi
+        if a.fd_storage == "f64":
+            s_fd = plan.adjoint_scene(nsteps=n)
+            s_fd.storage = abi.STORE_F64
+            g.close()
+            g = Solver(s_fd)
+        init = g.snapshot()
+        g.step(n)
+        J_fd = g.objective_value(obj)
         rng = np.random.default_rng(16)
         cells = [tuple(int(rng.integers(0, m)) for m in grad.shape) for _ in range(a.fd_cells)]
         eps0 = s.design["eps"].copy()
@@ -502,8 +625,10 @@ def run_adjoint(a):
         g.set_design_eps(eps0)
         fdv = np.array(vals)
         adv = np.array([grad[q] for q in cells])
-        fd = {"cells": len(cells), "h": a.fd_h, "max_err_over_max_grad": float(np.abs(adv - fdv).max() / np.abs(grad).max()),
-              "max_rel_err": float((np.abs(adv - fdv) / np.abs(adv)).max())}
+        fd = {"cells": len(cells), "h": a.fd_h, "storage": a.fd_storage, "J_fd_plan": J_fd,
+              "max_err_over_max_grad": float(np.abs(adv - fdv).max() / np.abs(grad).max()),
+              "max_rel_err": float((np.abs(adv - fdv) / np.abs(adv)).max()),
+              "adjoint": adv.tolist(), "finite_differences": fdv.tolist()}
     line = {
         "metric": METRIC, "value": s.ncells * n / fwd_s / 1e9, "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": 1,
         "ms_per_step": fwd_s / n * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -520,8 +645,77 @@ def run_adjoint(a):
     return 0
 
 
+def _rel(a, b, chunk=1 << 24):
+    """Relative L2 distance |a - b| / |b| of two large arrays, in chunks (no full-size temporaries)."""
+    import numpy as np
+    a, b = a.reshape(-1), b.reshape(-1)
+    num = den = 0.0
+    for q in range(0, b.size, chunk):
+        x = a[q:q + chunk].astype(np.float64)
+        y = b[q:q + chunk].astype(np.float64)
+        num += float(np.dot(x - y, x - y))
+        den += float(np.dot(y, y))
+    return (num / den) ** 0.5 if den > 0 else num ** 0.5
+
+
+def run_precision(a):
+    """The FP64 pin of the headline workload at full size: the 512^3 rough
+    Drude-silver surface stepped --prec-steps steps with FP64 field storage and
+    arithmetic (FDTD_STORE_F64: the reference's own precision), then with FP32,
+    FP16 and BF16 storage; E, the probe series and the far-field spectrum of
+    each against the FP64 run (relative L2), and each run's device time."""
+    import numpy as np
+    import torch
+    from gsvit_copy_b200 import abi
+    from gsvit_copy_b200.solver import Solver
+    n = a.prec_steps
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    runs = {}
+    ref = None
+    for name, st in (("f64", abi.STORE_F64), ("f32", abi.STORE_F32), ("f16", abi.STORE_F16), ("bf16", abi.STORE_BF16)):
+        scene = workload_scene(a.res, n)
+        scene.storage = st
+        cfg = config_block(a.res, scene)
+        g = Solver(scene, device=0)
+        g.set_stream(stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        g.step(n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        g.sync()
+        ms = e0.elapsed_time(e1)
+        E = g.fields(abi.E_ALL, dtype=np.float32 if st != abi.STORE_F64 else np.float64)[:3]
+        out = {"gcells": scene.ncells * n / (ms * 1e-3) / 1e9, "ms_per_step": ms / n,
+               "probes": g.probes(), "spectrum": g.nfff_spectrum(), "E": E}
+        g.close()
+        if ref is None:
+            ref = out
+            runs[name] = {"value": out["gcells"], "ms_per_step": out["ms_per_step"]}
+            continue
+        runs[name] = {"value": out["gcells"], "ms_per_step": out["ms_per_step"],
+                      "rel_l2_E": [_rel(x, y) for x, y in zip(out["E"], ref["E"])],
+                      "rel_l2_probes": _rel(out["probes"], ref["probes"]),
+                      "rel_l2_farfield": _rel(out["spectrum"], ref["spectrum"])}
+        del out
+    line = {
+        "metric": METRIC, "value": runs["f32"]["value"], "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": 0,
+        "ms_per_step": runs["f32"]["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Gaussian-correlated height map)",
+        "config": dict(cfg, workload_kind="precision pin against FP64"),
+        "precision": runs,
+        "tolerance_note": "rel L2 of E, probe series and far-field spectrum after the full run, against the FP64 run",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if a.workload == "precision":
+        return run_precision(a)
     if a.workload == "batched":
         return run_batched(a)
     if a.workload == "adjoint":

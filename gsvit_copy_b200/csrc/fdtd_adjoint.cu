@@ -4,8 +4,9 @@
 // (slab kernels; the bulk kernel computes the same expressions) is linear in
 // (E, H, psi_E, psi_H): the H half step (ystep_h yee.c:146-265, CPML H
 // boundary.c:347-519, zero planes boundary.c:418-492) and the E half step
-// (ystep_e yee.c:530-1247 without the dispersive branch, PEC rule, zero planes
-// and CPML E boundary.c:691-884).  The TSF corrections are sources that do
+// (ystep_e yee.c:530-1247 with the dispersive branch in the difference form of
+// DevAde and the CPML inside it, yee.c:914-1108, PEC rule, zero planes and CPML
+// E boundary.c:691-884).  The TSF corrections are sources that do
 // not depend on the fields.  The adjoint applies the transposed half steps in
 // reverse order, each in two gathers over the cells, so that no two threads
 // write one value:
@@ -32,8 +33,31 @@ __device__ __forceinline__ void cell_ijk(const DevPlan &P, int64_t c, int &i, in
     i = (int)(t / P.yr);
 }
 
-// ---- E half step: A -- adjoint of E^n, psi_E and the H differences
+// ---- E half step: A -- adjoint of E^n, psi_E and the H differences, and,
+// in cells of the dispersive branch, of the ADE state (E^{n-1}, Q, p, q)
 // dd: 0 dhz_j, 1 dhy_k, 2 dhx_k, 3 dhz_i, 4 dhy_i, 5 dhx_j (backward differences)
+//
+// Forward, per cell (e_special): the ADE value ne of the dispersive components
+// (c0dx curl + qe Q + sum(qpe q + pe p) + c2 E^{n-1} + c3 E^n where the curl
+// exists, E^n elsewhere), the CPML inside the branch (a first psi_E update,
+// psi1 = be psi0 + ce D/dx, and ne +/-= dx cba psi1), the state recursions
+// from ne, the ordinary update of the other components, the PEC rule, then
+// (off the zeroed planes) the second psi_E update psi2 = be psi1 + ce D/dx
+// with corrections of the non-dispersive components, stored where the two
+// other indices are > 0.  Reversed here in the opposite order.
+struct FaceT {             // one psi_E array of one face at this cell
+    bool in, store, first; // cell in the slab; psi2 stored; first update (dispersive branch)
+    int64_t q;             // psi index
+    float be, ce;
+    int dix;               // the difference it reads (dd index)
+    int bnd_c;             // the E component of the boundary correction, its sign, its gate component
+    float bnd_s;
+    int bnd_t;
+    int ade_c;             // the E component of the correction in the branch (-1: none), its sign
+    float ade_s;
+};
+
+template <bool ADE>
 __global__ void adj_e_a(const __grid_constant__ DevPlan P, const DevAdj A, int64_t n)
 {
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
@@ -42,91 +66,177 @@ __global__ void adj_e_a(const __grid_constant__ DevPlan P, const DevAdj A, int64
         const int xr = P.xr, yr = P.yr, zr = P.zr;
         const int cls = cls_at(P, i, j, k);
         const float4 *cl = reinterpret_cast<const float4 *>(P.classes);
-        const float4 c0 = cl[cls * 4 + 0], c1 = cl[cls * 4 + 1];
+        const float4 c0 = cl[cls * 4 + 0], c1 = cl[cls * 4 + 1], c2 = cl[cls * 4 + 2], c3 = cl[cls * 4 + 3];
         const unsigned fl = __float_as_uint(c0.w);
         float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z};
+        const float cba[3] = {c3.x, c3.y, c3.z};
         if (fl & CF_DESIGN) {
             const int64_t q = ((int64_t)(i - P.dbox[0]) * (P.dbox[3] - P.dbox[2]) + (j - P.dbox[2])) * (P.dbox[5] - P.dbox[4]) + (k - P.dbox[4]);
             for (int a = 0; a < 3; a++) { ca[a] = P.dcoef[6 * q + a]; cb[a] = P.dcoef[6 * q + 3 + a]; }
         }
+        const bool ade = ADE && (fl & CF_ADE_BRANCH);
+        const bool comp[3] = {ade && (fl & CF_ADE_X), ade && (fl & CF_ADE_Y), ade && (fl & CF_ADE_Z)};
+        const bool gd[3] = {j > 0 && k > 0, i > 0 && k > 0, i > 0 && j > 0};
         float e[3] = {A.eb[0][c], A.eb[1][c], A.eb[2][c]};
         float d[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const float dx = P.dx, idx_ = 1.0f / P.dx;
         const bool zero = (P.cp_on[X0] && i == 0) || (P.cp_on[Y0] && j == 0) || (P.cp_on[Z0] && k == 0);
-        if (zero) {
-            e[0] = e[1] = e[2] = 0.f;
-        } else {
-            const float dx = P.dx, idx_ = 1.0f / P.dx;
+        // the psi_E arrays this cell touches (faces x0 xn y0 yn z0 zn, two each)
+        FaceT F[6][2];
+        {
             const bool inx0 = P.cp_on[X0] && i >= 1 && i < P.cp_d[X0];
             const bool iny0 = P.cp_on[Y0] && j >= 1 && j < P.cp_d[Y0];
             const bool inz0 = P.cp_on[Z0] && k >= 1 && k < P.cp_d[Z0];
             const bool inxn = P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1;
             const bool inyn = P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1;
             const bool inzn = P.cp_on[ZN] && k >= zr - P.cp_d[ZN] + 1;
-            // x faces: psi[0] <- dhz_i, psi[1] <- dhy_i; ny -= dx cb1 psi[0], nz += dx cb2 psi[1]
-            auto xface = [&](int f, int pos, int64_t q) {
-                const float be = P.be[f][pos], ce = P.ce[f][pos];
-                const float t0 = A.pe[f][0][q] - dx * cb[1] * e[1], t1 = A.pe[f][1][q] + dx * cb[2] * e[2];
-                A.pe[f][0][q] = be * t0;
-                A.pe[f][1][q] = be * t1;
-                d[3] += ce * idx_ * t0;
-                d[4] += ce * idx_ * t1;
-            };
-            // y faces: psi[0] <- dhz_j, psi[1] <- dhx_j; nx += dx cb0 psi[0], nz -= dx cb2 psi[1]
-            auto yface = [&](int f, int pos, int64_t q) {
-                const float be = P.be[f][pos], ce = P.ce[f][pos];
-                const float t0 = A.pe[f][0][q] + dx * cb[0] * e[0], t1 = A.pe[f][1][q] - dx * cb[2] * e[2];
-                A.pe[f][0][q] = be * t0;
-                A.pe[f][1][q] = be * t1;
-                d[0] += ce * idx_ * t0;
-                d[5] += ce * idx_ * t1;
-            };
-            // z faces: psi[1] <- dhx_k, psi[0] <- dhy_k; ny += dx cb1 psi[1], nx -= dx cb0 psi[0]
-            auto zface = [&](int f, int pos, int64_t q) {
-                const float be = P.be[f][pos], ce = P.ce[f][pos];
-                const float t1 = A.pe[f][1][q] + dx * cb[1] * e[1], t0 = A.pe[f][0][q] - dx * cb[0] * e[0];
-                A.pe[f][1][q] = be * t1;
-                A.pe[f][0][q] = be * t0;
-                d[2] += ce * idx_ * t1;
-                d[1] += ce * idx_ * t0;
-            };
-            if (inx0 && j > 0 && k > 0) xface(X0, i, ((int64_t)i * yr + j) * zr + k);
-            if (iny0 && i > 0 && k > 0) yface(Y0, j, ((int64_t)i * P.cp_d[Y0] + j) * zr + k);
-            if (inz0 && i > 0 && j > 0) zface(Z0, k, ((int64_t)i * yr + j) * P.cp_d[Z0] + k);
-            if (inxn && j > 0 && k > 0) {
-                const int ir = i - (xr - P.cp_d[XN]);
-                xface(XN, ir, ((int64_t)ir * yr + j) * zr + k);
+            const bool in[6] = {inx0, inxn, iny0, inyn, inz0, inzn};
+            const int pos[6] = {i, i - (xr - P.cp_d[XN]), j, j - (yr - P.cp_d[YN]), k, k - (zr - P.cp_d[ZN])};
+            const bool first[6] = {inx0 && i > 1, inxn, iny0 && j > 1, inyn, inz0 && k > 1, inzn};
+            for (int f = 0; f < 6; f++) {
+                const int ax = f / 2;
+                int64_t q = 0;
+                if (in[f]) {
+                    if (f == X0) q = ((int64_t)i * yr + j) * zr + k;
+                    else if (f == XN) q = ((int64_t)pos[f] * yr + j) * zr + k;
+                    else if (f == Y0) q = ((int64_t)i * P.cp_d[Y0] + j) * zr + k;
+                    else if (f == YN) q = ((int64_t)i * P.cp_d[YN] + pos[f]) * zr + k;
+                    else if (f == Z0) q = ((int64_t)i * yr + j) * P.cp_d[Z0] + k;
+                    else q = ((int64_t)i * yr + j) * P.cp_d[ZN] + pos[f];
+                }
+                const float be = in[f] ? P.be[f][pos[f]] : 0.f, ce = in[f] ? P.ce[f][pos[f]] : 0.f;
+                for (int r = 0; r < 2; r++) {
+                    FaceT &t = F[f][r];
+                    t.in = in[f] && !zero;
+                    t.store = t.in && gd[ax];
+                    t.first = t.in && ade && first[f];
+                    t.q = q;
+                    t.be = be;
+                    t.ce = ce;
+                    t.ade_c = -1;
+                    t.ade_s = 0.f;
+                }
+                if (ax == 0) {        // psi[0] <- dhz_i: ny -= dx cb1 psi; psi[1] <- dhy_i: nz += dx cb2 psi
+                    F[f][0].dix = 3; F[f][0].bnd_c = 1; F[f][0].bnd_s = -1.f; F[f][0].bnd_t = 1;
+                    F[f][1].dix = 4; F[f][1].bnd_c = 2; F[f][1].bnd_s = +1.f; F[f][1].bnd_t = 2;
+                    if (f == XN) {    // x0 corrections in the branch are scaled by cb == 0 (yee.c:577)
+                        F[f][0].ade_c = 1; F[f][0].ade_s = -1.f;
+                        F[f][1].ade_c = 2; F[f][1].ade_s = +1.f;
+                    }
+                } else if (ax == 1) { // psi[0] <- dhz_j: nx += dx cb0 psi; psi[1] <- dhx_j: nz -= dx cb2 psi
+                    F[f][0].dix = 0; F[f][0].bnd_c = 0; F[f][0].bnd_s = +1.f; F[f][0].bnd_t = 0;
+                    F[f][1].dix = 5; F[f][1].bnd_c = 2; F[f][1].bnd_s = -1.f; F[f][1].bnd_t = 2;
+                    F[f][0].ade_c = 0; F[f][0].ade_s = +1.f;
+                    F[f][1].ade_c = 2; F[f][1].ade_s = -1.f;
+                } else {              // psi[1] <- dhx_k: ny += dx cb1 psi; psi[0] <- dhy_k: nx -= dx cb0 psi
+                    F[f][1].dix = 2; F[f][1].bnd_c = 1; F[f][1].bnd_s = +1.f; F[f][1].bnd_t = 1;
+                    F[f][0].dix = 1; F[f][0].bnd_c = 0; F[f][0].bnd_s = -1.f;
+                    F[f][0].bnd_t = f == Z0 ? 2 : 0;   // the z0 ex correction is gated by ztbc (boundary.c:758-759)
+                    F[f][1].ade_c = 1; F[f][1].ade_s = +1.f;
+                    F[f][0].ade_c = 0; F[f][0].ade_s = -1.f;
+                }
             }
-            if (inyn && i > 0 && k > 0) {
-                const int jr = j - (yr - P.cp_d[YN]);
-                yface(YN, jr, ((int64_t)i * P.cp_d[YN] + jr) * zr + k);
+        }
+        // second psi_E update and the boundary corrections, reversed
+        float lp[6][2], ident[6][2];
+        for (int f = 0; f < 6; f++)
+            for (int r = 0; r < 2; r++) {
+                const FaceT &t = F[f][r];
+                lp[f][r] = 0.f;
+                ident[f][r] = 0.f;
+                if (!t.in) continue;
+                const float lam = A.pe[f][r][t.q];
+                if (t.store) {
+                    const float l2 = lam + (comp[t.bnd_t] ? 0.f : t.bnd_s * dx * cb[t.bnd_c] * e[t.bnd_c]);
+                    lp[f][r] = t.be * l2;
+                    d[t.dix] += t.ce * idx_ * l2;
+                } else {
+                    ident[f][r] = lam;   // psi stored unchanged
+                }
             }
-            if (inzn && i > 0 && j > 0) {
-                const int kr = k - (zr - P.cp_d[ZN]);
-                zface(ZN, kr, ((int64_t)i * yr + j) * P.cp_d[ZN] + kr);
-            }
+        if (zero) {
+            e[0] = e[1] = e[2] = 0.f;
+        } else {
             if (fl & CF_PEC_X) e[0] = 0.f;
             if (fl & CF_PEC_Y) e[1] = 0.f;
             if (fl & CF_PEC_Z) e[2] = 0.f;
-            const float ikx = P.ike[0][i], iky = P.ike[1][j], ikz = P.ike[2][k];
-            if (j > 0 && k > 0) {   // curlx = dhz_j iky - dhy_k ikz
-                const float t = cb[0] * e[0];
-                d[0] += t * iky;
-                d[1] -= t * ikz;
-                e[0] = ca[0] * e[0];
+        }
+        // adjoint of the ADE value of the dispersive components: u = its own
+        // adjoint plus what the state recursions read from it
+        float u[3] = {0.f, 0.f, 0.f};
+        if (ADE && ade) {
+            const DevAde &Ad = P.ade[__float_as_int(c2.z)];
+            for (int a = 0; a < 3; a++) {
+                if (!comp[a]) continue;
+                float v = e[a] + Ad.a2 * A.q[a][c];
+                for (int m = 0; m < 2; m++)
+                    if (A.pc[a][m]) v += Ad.bp4[m] * (A.qc[a][m][c] + A.pc[a][m][c]);
+                u[a] = v;
             }
-            if (i > 0 && k > 0) {   // curly = dhx_k ikz - dhz_i ikx
-                const float t = cb[1] * e[1];
-                d[2] += t * ikz;
-                d[3] -= t * ikx;
-                e[1] = ca[1] * e[1];
+            // the corrections of the CPML inside the branch
+            for (int f = 0; f < 6; f++)
+                for (int r = 0; r < 2; r++) {
+                    const FaceT &t = F[f][r];
+                    if (t.first && t.ade_c >= 0 && comp[t.ade_c] && gd[f / 2])
+                        lp[f][r] += t.ade_s * dx * cba[t.ade_c] * u[t.ade_c];
+                }
+        }
+        // first psi_E update (dispersive branch) and the psi adjoints
+        for (int f = 0; f < 6; f++)
+            for (int r = 0; r < 2; r++) {
+                const FaceT &t = F[f][r];
+                if (!t.in) continue;
+                float l0 = ident[f][r];
+                if (t.first) {
+                    l0 += t.be * lp[f][r];
+                    d[t.dix] += t.ce * idx_ * lp[f][r];
+                } else {
+                    l0 += lp[f][r];
+                }
+                A.pe[f][r][t.q] = l0;
             }
-            if (i > 0 && j > 0) {   // curlz = dhy_i ikx - dhx_j iky
-                const float t = cb[2] * e[2];
-                d[4] += t * ikx;
-                d[5] -= t * iky;
-                e[2] = ca[2] * e[2];
+        const float ikx = P.ike[0][i], iky = P.ike[1][j], ikz = P.ike[2][k];
+        // curl x = dhz_j iky - dhy_k ikz, curl y = dhx_k ikz - dhz_i ikx, curl z = dhy_i ikx - dhx_j iky
+        float w[3] = {0.f, 0.f, 0.f};
+        if (!zero) {
+            for (int a = 0; a < 3; a++) {
+                if (!gd[a] || comp[a]) continue;   // ordinary update
+                w[a] = cb[a] * e[a];
+                e[a] = ca[a] * e[a];
             }
         }
+        if (ADE && ade) {
+            const DevAde &Ad = P.ade[__float_as_int(c2.z)];
+            for (int a = 0; a < 3; a++) {
+                if (!comp[a]) continue;
+                const float ua = u[a], lq1 = A.q[a][c];
+                float lqt[2] = {0.f, 0.f}, lp1[2] = {0.f, 0.f};
+                for (int m = 0; m < 2; m++)
+                    if (A.pc[a][m]) { lp1[m] = A.pc[a][m][c]; lqt[m] = A.qc[a][m][c] + lp1[m]; }
+                const float lv = gd[a] ? ua : 0.f;
+                float le0 = (gd[a] ? Ad.c3 * ua : ua) + 2.f * Ad.a2 * lq1 + A.ep[a][c];
+                float lep = Ad.c2 * lv + Ad.a2 * lq1;
+                for (int m = 0; m < 2; m++) {
+                    le0 += Ad.bp3[m] * lqt[m];
+                    lep += Ad.bp2[m] * lqt[m];
+                }
+                w[a] = Ad.c0dx * lv;
+                e[a] = le0;
+                A.ep[a][c] = lep;
+                A.q[a][c] = Ad.qe * lv + Ad.ma0 * lq1;
+                for (int m = 0; m < 2; m++)
+                    if (A.pc[a][m]) {
+                        A.qc[a][m][c] = Ad.qpe[m] * lv + Ad.rq[m] * lqt[m];
+                        A.pc[a][m][c] = Ad.pe[m] * lv + Ad.rp[m] * lqt[m] + lp1[m];
+                    }
+            }
+        }
+        d[0] += w[0] * iky;
+        d[1] -= w[0] * ikz;
+        d[2] += w[1] * ikz;
+        d[3] -= w[1] * ikx;
+        d[4] += w[2] * ikx;
+        d[5] -= w[2] * iky;
         for (int a = 0; a < 3; a++) A.eb[a][c] = e[a];
         for (int q = 0; q < 6; q++) A.dd[q][c] = d[q];
     }
@@ -366,7 +476,8 @@ int grid_for(int64_t n)
 void launch_adjoint_e(const DevPlan &p, const DevAdj &a, cudaStream_t st)
 {
     const int64_t n = (int64_t)p.xr * p.yr * p.zr;
-    adj_e_a<<<grid_for(n), 256, 0, st>>>(p, a, n);
+    if (p.nade > 0) adj_e_a<true><<<grid_for(n), 256, 0, st>>>(p, a, n);
+    else adj_e_a<false><<<grid_for(n), 256, 0, st>>>(p, a, n);
     adj_e_b<<<grid_for(n), 256, 0, st>>>(p, a, n);
 }
 

@@ -12,6 +12,11 @@ struct DevAdj {
     float *dd[6];              // adjoints of the six field differences of a half step
     float *pe[6][2];           // adjoints of psi_E (DevPlan::psie layout)
     float *ph[6][2];           // adjoints of psi_H (DevPlan::psih_in layout)
+    // plans with dispersive cells: adjoints of the ADE state (the difference
+    // form of DevAde), of E^{n-1} as the next step reads it, of Q, and of the
+    // critical-point p and q (NULL without poles)
+    float *ep[3], *q[3];
+    float *pc[3][2], *qc[3][2];
 };
 
 // far-field objective: per surface cell and component the complex weights

@@ -1694,6 +1694,14 @@ struct fdtd_batch {
     int *d_err = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_steps = 0;
+    // Each instance runs the path it runs alone: the TMA tiles over its whole
+    // grid (fdtd_plan::tiles_on; their lists concatenated per kernel variant
+    // and tile kind, one CTA per item) or the bulk box and slab kernels (the
+    // lists above hold only these instances).
+    int ntiled = 0;
+    BulkItem *d_titems[3][3] = {};   // [variant group][tile kind]
+    int ntitems[3][3] = {};
+    BulkMaps *d_tmaps[3][2] = {};    // [tile kind][parity], indexed by instance
 };
 
 namespace {
@@ -1719,7 +1727,7 @@ cudaError_t batch_set_items(fdtd_batch *B, int len, bool persistent)
         std::vector<BulkItem> all;
         for (size_t q = 0; q < B->plans.size(); q++) {
             fdtd_plan *P = B->plans[q];
-            if (!P->bulk_on || B->group[q] != g) continue;
+            if (!P->bulk_on || P->tiles_on || B->group[q] != g) continue;
             const int lo[3] = {P->region[0], P->region[2], P->region[4]}, hi[3] = {P->region[1], P->region[3], P->region[5]};
             const auto it = bulk_items(lo, hi, len > 0 ? len : P->bulk_len, (int)q);
             all.insert(all.end(), it.begin(), it.end());
@@ -1750,7 +1758,15 @@ int batch_launch_step(fdtd_batch *B, cudaStream_t st)
     const int in = B->cur, n = (int)B->plans.size();
     launch_aux_step_batch(B->d_aux[in], n, st);
     if (B->max_tsf) launch_tsf_faces_batch(B->d_plans[in], n, B->max_tsf, st);
-    for (int g = 0; g < 3; g++) {
+    for (int g = 0; g < 3; g++)   // instances with TMA tiles
+        for (int kind = 0; kind < 3; kind++) {
+            if (!B->ntitems[g][kind]) continue;
+            cudaError_t e = launch_tiles_batch(kind, B->d_plans[in], B->d_tmaps[kind][in], B->d_titems[g][kind],
+                                               B->ntitems[g][kind], B->ncls, B->d_err, g > 0, g == 2 ? 2 : 0, B->storage, st);
+            if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched tile launch: ") + cudaGetErrorString(e));
+        }
+    for (int g = 0; g < 3; g++) {   // the others: bulk box and slab kernels
+        if (!B->nitems[g] && !B->nboxes[g] && !B->neboxes[g]) continue;
         const bool ade = g > 0;
         const int npoles = g == 2 ? 2 : 0;
         cudaError_t e = launch_bulk_batch(B->d_plans[in], B->d_maps[in], B->d_items[g], B->nitems[g], B->bulk_grid[g], B->ncls,
@@ -1761,7 +1777,7 @@ int batch_launch_step(fdtd_batch *B, cudaStream_t st)
                                     B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
     }
-    {   // E of every instance's plain runs (after all H half steps)
+    if (B->nepboxes) {   // E of every instance's plain runs (after all H half steps)
         cudaError_t e = launch_slab_e_plain_batch(B->d_plans[in], B->d_epboxes, B->nepboxes, B->nepblocks, B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
     }
@@ -1852,7 +1868,7 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
     for (int g = 0; g < 3; g++) {
         std::vector<SlabBox> boxes;
         for (int q = 0; q < nplans; q++) {
-            if (B->group[q] != g) continue;
+            if (B->group[q] != g || B->plans[q]->tiles_on) continue;
             for (SlabBox b : B->plans[q]->h_boxes) {
                 b.first_block = B->nslab_blocks[g];
                 b.inst = q;
@@ -1866,7 +1882,7 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
         // E runs with a dispersive cell, numbered for this variant's launch
         std::vector<SlabBox> ebx;
         for (int q = 0; q < nplans; q++) {
-            if (B->group[q] != g) continue;
+            if (B->group[q] != g || B->plans[q]->tiles_on) continue;
             for (SlabBox b : B->plans[q]->h_eboxes) {
                 b.first_block = B->neblocks[g];
                 b.inst = q;
@@ -1889,19 +1905,45 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
     }
     {   // E runs without a dispersive cell, every instance in one launch
         std::vector<SlabBox> pbx;
-        for (int q = 0; q < nplans; q++)
+        for (int q = 0; q < nplans; q++) {
+            if (B->plans[q]->tiles_on) continue;
             for (SlabBox b : B->plans[q]->h_epboxes) {
                 b.first_block = B->nepblocks;
                 b.inst = q;
                 pbx.push_back(b);
                 B->nepblocks += ((long long)(b.i1 - b.i0) * (b.j1 - b.j0) * (b.k1 - b.k0) + 255) / 256;
             }
+        }
         if (B->nepblocks > 0x7fffffffLL) { fail(FDTD_E_UNSUPPORTED, "too many slab cells for one launch"); return bail(FDTD_E_UNSUPPORTED); }
         if (!pbx.empty()) BA(upload(B->mem, &B->d_epboxes, pbx.data(), pbx.size()), "batch slab boxes");
         B->nepboxes = (int)pbx.size();
     }
     BA(B->mem.alloc(&B->d_err, 1), "error word");
     for (auto *P : B->plans) P->batch_err = B->d_err;   // the instances' readbacks check the batch's word too
+    for (auto *P : B->plans) B->ntiled += P->tiles_on ? 1 : 0;
+    if (B->ntiled) {
+        for (int kind = 0; kind < 3; kind++) {
+            for (int in = 0; in < 2; in++) {
+                std::vector<BulkMaps> tm(nplans);
+                std::memset(tm.data(), 0, sizeof(BulkMaps) * nplans);
+                for (int q = 0; q < nplans; q++)
+                    if (B->plans[q]->ntiles[kind]) tm[q] = B->plans[q]->tmaps[kind][in];
+                BA(upload(B->mem, &B->d_tmaps[kind][in], tm.data(), tm.size()), "batch tile maps");
+            }
+            for (int g = 0; g < 3; g++) {
+                std::vector<BulkItem> all;
+                for (int q = 0; q < nplans; q++) {
+                    if (B->group[q] != g || !B->plans[q]->tiles_on) continue;
+                    for (BulkItem it : B->plans[q]->h_tiles[kind]) {
+                        it.inst = q;
+                        all.push_back(it);
+                    }
+                }
+                if (!all.empty()) BA(upload(B->mem, &B->d_titems[g][kind], all.data(), all.size()), "batch tile lists");
+                B->ntitems[g][kind] = (int)all.size();
+            }
+        }
+    }
     BA(batch_set_items(B, 0, true), "batch work list");
     BA(cudaDeviceSynchronize(), "batch set-up");
 #undef BA
@@ -2113,6 +2155,15 @@ cudaError_t adj_alloc(fdtd_plan *P, AdjBufs &B)
             if ((e = B.mem.alloc(&B.a.ph[f][q], cnt)) != cudaSuccess) return e;
         }
     }
+    if (hp.has_ade)
+        for (int c = 0; c < 3; c++) {
+            if ((e = B.mem.alloc(&B.a.ep[c], n)) != cudaSuccess) return e;
+            if ((e = B.mem.alloc(&B.a.q[c], n)) != cudaSuccess) return e;
+            for (int m = 0; m < hp.maxpoles; m++) {
+                if ((e = B.mem.alloc(&B.a.pc[c][m], n)) != cudaSuccess) return e;
+                if ((e = B.mem.alloc(&B.a.qc[c][m], n)) != cudaSuccess) return e;
+            }
+        }
     return cudaSuccess;
 }
 
@@ -2208,7 +2259,6 @@ int objective_from_spectrum(fdtd_plan *P, const fdtd_objective *obj, double *J)
 
 int check_adjoint_plan(const fdtd_plan *P)
 {
-    if (P->hp.has_ade) return fail(FDTD_E_UNSUPPORTED, "the adjoint covers non-dispersive materials only");
     if (P->storage != FDTD_STORE_F32) return fail(FDTD_E_UNSUPPORTED, "the adjoint needs FP32 field storage");
     return FDTD_OK;
 }

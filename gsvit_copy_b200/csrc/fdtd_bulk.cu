@@ -30,16 +30,18 @@
 // for the components its staged class word marks.
 //
 // In a CPML tile (CP = true) a 4-cell group whose cells are not all plain
-// (DevPlan::plo/phi) takes the special path of fdtd_cells.cuh cell by cell:
-// h_update with psi_H (written by the owner only; halo copies read it) and
-// e_special with psi_E, kappa, ADE-in-CPML, PEC and TSF.  Plain groups of a
-// CPML tile take the same plain update as the bulk.
+// (DevPlan::plo/phi) takes the special path of fdtd_cpgroup.cuh: h_update
+// with psi_H (written by the owner only; halo copies read it) and e_special
+// with psi_E, kappa, ADE-in-CPML, PEC and TSF, for the four cells at once
+// with 4-vector psi and state traffic.  Plain groups of a CPML tile take the
+// same plain update as the bulk.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "fdtd_bulk.cuh"
 #include "../../include/gsvit_b200.h"
 #include "fdtd_cells.cuh"
+#include "fdtd_cpgroup.cuh"
 #include "fdtd_device.cuh"
 
 namespace {
@@ -357,16 +359,20 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                 }
             } else if (CP) {
                 // ystep_h with kappa and the edge rules, then psi_H, TSF and the
-                // zeroed planes (h_update / h_special); psi_H is written by the owner
+                // zeroed planes (fdtd_cpgroup.cuh); psi_H is written by the owner
+                float dyi[4], dzi[4], dxj[4], dzj[4], dxk[4], dyk[4];
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    float h[3] = {hx[c], hy[c], hz[c]};
-                    if (Stor<T>::scaled) { h[0] *= P.ihs; h[1] *= P.ihs; h[2] *= P.ihs; }
+                    if (Stor<T>::scaled) { hx[c] *= P.ihs; hy[c] *= P.ihs; hz[c] *= P.ihs; }
                     const float eyk = c < 3 ? ey[c + 1] : eyk4, exk = c < 3 ? ex[c + 1] : exk4;
-                    h_update<T>(P, scls, (cw >> (8 * c)) & 0xff, i, j, kq + c, true, act, tsf_plane, eyi[c] - ey[c],
-                                ezi[c] - ez[c], exj[c] - ex[c], ezj[c] - ez[c], exk - ex[c], eyk - ey[c], h);
-                    hx[c] = h[0]; hy[c] = h[1]; hz[c] = h[2];
+                    dyi[c] = eyi[c] - ey[c];
+                    dzi[c] = ezi[c] - ez[c];
+                    dxj[c] = exj[c] - ex[c];
+                    dzj[c] = ezj[c] - ez[c];
+                    dxk[c] = exk - ex[c];
+                    dyk[c] = eyk - ey[c];
                 }
+                cp_h_group<T>(P, scls, cw, i, j, kq, act, tsf_plane, dyi, dzi, dxj, dzj, dxk, dyk, hx, hy, hz);
             }
             if (act) {
                 const float q = Stor<T>::scaled ? P.hs : 1.f;
@@ -396,16 +402,10 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
             const float *eo[3] = {ex, ey, ez};
             float ne[3][4];
             if (CP && special) {
-                // the general E path cell by cell (e_special: ADE with its CPML,
-                // ordinary update with kappa, PEC, zeroed planes, psi_E, TSF E)
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const float3 en = e_special<ADE, NPOLES, T>(
-                        P, scls, (cw >> (8 * c)) & 0xff, i, j, kq + c, tsf_plane, make_float3(ex[c], ey[c], ez[c]),
-                        make_float3(hx[c], hy[c], hz[c]), hxj[c], hzj[c], c ? hx[c - 1] : hxk0, c ? hy[c - 1] : hyk0,
-                        hyim[c], hzim[c]);
-                    ne[0][c] = en.x; ne[1][c] = en.y; ne[2][c] = en.z;
-                }
+                // the general E path (e_special: ADE with its CPML, ordinary
+                // update with kappa, PEC, zeroed planes, psi_E, TSF E) by group
+                cp_e_group<ADE, NPOLES, T>(P, scls, sade, cw, i, j, kq, c0i, tsf_plane, ex, ey, ez, hx, hy, hz, hxj, hzj,
+                                           hxk0, hyk0, hyim, hzim, ne);
             } else {
                 float cu[3][4];   // curl H of the four cells
 #pragma unroll

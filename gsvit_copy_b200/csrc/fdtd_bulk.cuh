@@ -25,9 +25,9 @@ struct BulkItem {
 //        (no CPML, kappa 1, no edge rule);
 //  cpxy  15 x 60: the x slabs (whole planes) and the y slabs;
 //  cpz   31 x 28: the z slabs between the y slabs.
-// The CPML tiles run the plain update on their plain cells and the special
-// path of fdtd_cells.cuh (psi, kappa, zeroed planes, ADE-in-CPML, edges) on
-// the rest.  k0 and khi are multiples of 4 in every layout.
+// The CPML tiles run the plain update on their plain 4-cell groups and the
+// special path of fdtd_cpgroup.cuh (psi, kappa, zeroed planes, ADE-in-CPML,
+// edges) on the rest.  k0 and khi are multiples of 4 in every layout.
 #define BULK_TJ 15
 #define BULK_TK 60
 #define CPXY_TJ 15

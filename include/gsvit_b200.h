@@ -337,9 +337,11 @@ int fdtd_get_nclasses(const fdtd_plan *plan, int *nclasses);
  * No counterpart in the reference (GSvit steps one domain per process).  Many
  * independent plans -- instances of uneven size, material and source -- are
  * stepped in lockstep: each kernel of a step is one launch over all of them,
- * with per-instance parameter tables on the device and a persistent bulk
- * kernel that walks the concatenated work list (one launch per kernel
- * variant in use: no ADE, Drude, critical-point poles).  Results are
+ * with per-instance parameter tables on the device (one launch per kernel
+ * variant in use: no ADE, Drude, critical-point poles).  Each instance runs
+ * the kernels it runs alone: the TMA tiles over its whole grid, one CTA per
+ * tile of every such instance, or else a persistent bulk kernel that walks
+ * the concatenated bulk work list, and the slab kernels.  Results are
  * bit-identical to the same plans stepped one by one. */
 typedef struct fdtd_batch fdtd_batch;
 
@@ -357,13 +359,14 @@ int fdtd_batch_step(fdtd_batch *batch, int nsteps);
 int fdtd_batch_step_graph(fdtd_batch *batch, int nsteps, int chunk);
 /* Wait for the batch; reports an expired bounded wait as FDTD_E_TIMEOUT. */
 int fdtd_batch_sync(fdtd_batch *batch);
-/* Autotuner: times trial_steps steps for each candidate work list (planes per
- * bulk item 8 / 16 / 32 / 64 / whole, persistent grid or one CTA per item),
- * keeps the fastest and restores every instance's state.  report (if not
- * NULL) receives up to report_len/3 rows {planes (0 = whole), persistent,
- * ms per step}; *ncand the number of rows. */
+/* Autotuner: times trial_steps steps for each candidate work list of the
+ * bulk kernel (planes per bulk item 8 / 16 / 32 / 64 / whole, persistent grid
+ * or one CTA per item; it steps the instances without TMA tiles), keeps the
+ * fastest and restores every instance's state.  report (if not NULL)
+ * receives up to report_len/3 rows {planes (0 = whole), persistent, ms per
+ * step}; *ncand the number of rows. */
 int fdtd_batch_tune(fdtd_batch *batch, int trial_steps, double *report, int report_len, int *ncand);
-/* The work list in use: planes per item (0 = whole), persistent launch,
+/* The bulk work list in use: planes per item (0 = whole), persistent launch,
  * grid size and number of items. */
 int fdtd_batch_config(const fdtd_batch *batch, int *planes_per_item, int *persistent, int *grid, int *items);
 
@@ -406,8 +409,9 @@ int fdtd_objective_value(fdtd_plan *plan, const fdtd_objective *obj, double *J);
  * J, then the discrete adjoint of those steps backwards, recomputing each
  * segment of the forward run from its checkpoint (the lossy CPML makes the
  * step irreversible).  grad[c] = dJ/d eps_r of every design cell (dbox
- * order, k fastest).  Needs a design region, FP32 storage, no dispersive
- * material and the running-DFT far field.  On return the plan holds the
+ * order, k fastest).  Needs a design region, FP32 storage and the
+ * running-DFT far field; Drude / critical-point materials outside the design
+ * region are transposed with their polarisation state.  On return the plan holds the
  * forward state after nsteps.  Device memory: (nsteps/checkpoint + 1) copies
  * of the stepping state (fdtd_snapshot_size) plus checkpoint x 12 bytes per
  * cell of the design box. */

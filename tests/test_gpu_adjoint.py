@@ -24,9 +24,9 @@ pytestmark = pytest.mark.gpu
 NSTEPS = 600
 
 
-def small_design_scene(nsteps=NSTEPS, seed=5):
+def small_design_scene(nsteps=NSTEPS, seed=5, metal_cells=0):
     return plan.adjoint_scene(shape=(32, 32, 32), cpml_depth=6, design_shape=(4, 4, 2), glass_cells=3, nsteps=nsteps,
-                              pulse_delay=2e-15, pulse_width=0.7e-15, seed=seed)
+                              pulse_delay=2e-15, pulse_width=0.7e-15, seed=seed, metal_cells=metal_cells)
 
 
 def test_design_forward_vs_oracle():
@@ -45,13 +45,16 @@ def test_design_forward_vs_oracle():
     assert abs(g.objective_value(obj) / A.objective_value(o, obj) - 1) < 1e-5
 
 
-@pytest.mark.parametrize("which", ["pec", "design"])
+@pytest.mark.parametrize("which", ["pec", "design", "ade", "full", "design_drude"])
 def test_transposed_step_vs_fp64(which):
-    if which == "pec":
-        s = plan.small_scene("pec")
+    """8 transposed steps from random (E, H) adjoints; the polarisation,
+    E^{n-1} and psi adjoints start at zero on both sides ("ade" and "full"
+    run the Drude / critical-point branch and the CPML inside it)."""
+    if which in ("pec", "ade", "full"):
+        s = plan.small_scene(which)
         s.tsf = None
     else:
-        s = small_design_scene(nsteps=10)
+        s = small_design_scene(nsteps=10, metal_cells=8 if which == "design_drude" else 0)
     g = Solver(s)
     L = A.LinearStep(CpuSolver(s.expanded()))
     rng = np.random.default_rng(4)
@@ -69,8 +72,11 @@ def test_transposed_step_vs_fp64(which):
     assert max(errs) < 1e-5, errs
 
 
-def test_gradient_vs_fp64_adjoint():
-    s = small_design_scene()
+@pytest.mark.parametrize("metal", [0, 8])
+def test_gradient_vs_fp64_adjoint(metal):
+    """metal = 8: a Drude-silver layer across the bottom of the grid, inside
+    the z0 CPML, so that the backward pass runs the transposed ADE branch."""
+    s = small_design_scene(metal_cells=metal)
     obj = plan.cone_objective(s, nth=5, nph=7)
     g = Solver(s)
     J, grad = g.adjoint_gradient(obj, NSTEPS, checkpoint=128)
