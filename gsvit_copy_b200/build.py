@@ -20,7 +20,8 @@ OUT = os.path.join(HERE, "libgsvit_b200.so")
 BUILD = os.path.join(HERE, "_build")
 
 SOURCES = ["fdtd_kernels.cu", "fdtd_bulk.cu", "fdtd_adjoint.cu", "fdtd_api.cu", "plan_host.cpp"]
-HEADERS = ["fdtd_internal.h", "fdtd_device.cuh", "fdtd_kernels.cuh", "fdtd_bulk.cuh", "fdtd_adjoint.cuh", "plan_host.h", os.path.join("..", "..", "include", "gsvit_b200.h")]
+HEADERS = ["fdtd_internal.h", "fdtd_device.cuh", "fdtd_cells.cuh", "fdtd_cpgroup.cuh", "fdtd_kernels.cuh", "fdtd_bulk.cuh",
+           "fdtd_adjoint.cuh", "plan_host.h", os.path.join("..", "..", "include", "gsvit_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

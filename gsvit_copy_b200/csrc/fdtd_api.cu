@@ -1035,7 +1035,14 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             CA(bulk_configure(), "bulk kernel shared memory");
         }
         // TMA tiles over the whole grid (single plans; batches may use them too)
-        P->tiles_on = !hp.design && !r64 && ((size_t)Z * esz % 16 == 0) && !(nob && nob[0] == '1');
+        // the CPML tiles take one face per axis: every extent at least both depths + 8
+        bool roomy = true;
+        for (int ax = 0; ax < 3; ax++) {
+            const int ext = ax == 0 ? X : ax == 1 ? Y : Z;
+            const int dd = (hp.cp[2 * ax].enabled ? hp.cp[2 * ax].depth : 0) + (hp.cp[2 * ax + 1].enabled ? hp.cp[2 * ax + 1].depth : 0);
+            roomy = roomy && ext >= dd + 8;
+        }
+        P->tiles_on = !hp.design && !r64 && roomy && ((size_t)Z * esz % 16 == 0) && !(nob && nob[0] == '1');
         // test hook of the bounded-wait error path: every tile CTA of this plan
         // also waits, at most this many polls, on an mbarrier nothing arrives on
         if (const char *stv = getenv("GSVIT_B200_STALL_TEST")) P->stall = std::max(0, atoi(stv));

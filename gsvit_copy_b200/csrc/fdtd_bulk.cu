@@ -29,12 +29,13 @@
 // of plane i, and plane i+1's lines are prefetched into L2 at the same time
 // for the components its staged class word marks.
 //
-// In a CPML tile (CP = true) a 4-cell group whose cells are not all plain
-// (DevPlan::plo/phi) takes the special path of fdtd_cpgroup.cuh: h_update
-// with psi_H (written by the owner only; halo copies read it) and e_special
-// with psi_E, kappa, ADE-in-CPML, PEC and TSF, for the four cells at once
-// with 4-vector psi and state traffic.  Plain groups of a CPML tile take the
-// same plain update as the bulk.
+// In a CPML tile (CP = true) every 4-cell group inside the grid takes the
+// special path of fdtd_cpgroup.cuh: h_update with psi_H (written by the owner
+// only; halo copies read it) and e_special with psi_E, kappa, ADE-in-CPML,
+// PEC and TSF, for the four cells at once with 4-vector psi and state
+// traffic.  The CPML kernels carry no plain path: their loop body stays
+// small enough for the instruction cache, and on a plain cell the special
+// path computes the plain update (kappa 1, no psi, no edge rule).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -231,9 +232,8 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
     const int j = j0 - 1 + tr, kq = k0 - 4 + 4 * tg;
     const bool own = tr >= 1 && tg >= 1 && j < it.jhi && kq < it.khi;   // groups are whole (khi - k0 % 4 == 0)
     const int eb = tr * BWE + off + 4 * tg, hb = tr * BWH + off + 4 * tg, cb = tr * BWC + off8 + 4 * tg;
-    // CPML tiles: the group is plain when all its indices lie in the plain
-    // ranges; a special group inside the grid takes the special path
-    const bool jk_plain = j >= P.plo[1] && j < P.phi[1] && kq >= P.plo[2] && kq + 3 < P.phi[2];
+    // CPML tiles: every group inside the grid takes the special path (on a
+    // plain cell it computes the plain update: kappa 1, no psi, no edge rule)
     const bool jk_in = j >= 0 && j < P.yr && kq >= 0 && kq < P.zr;
     // TSF: does this thread's group touch a face of the TSF box?  Per plane
     // below: faces i = i0-1, i0, in over the box's (j,k) extent; lateral faces
@@ -265,7 +265,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
         unsigned char *st = stages + s * STAGE, *st1 = stages + s1 * STAGE;
         const bool prologue = (i < ib);
         const bool act = !prologue && own && ok;     // this thread updates and stores its group
-        const bool special = CP && jk_in && i >= 0 && i < P.xr && !(jk_plain && i >= P.plo[0] && i < P.phi[0]);
+        const bool special = CP && jk_in && i >= 0 && i < P.xr;
         const uint32_t cw = *reinterpret_cast<const uint32_t *>(cbox<T, L>(st) + cb);
         const int cl0 = cw & 0xff;
         const bool uni = cw == (uint32_t)cl0 * 0x01010101u;   // one class for the four cells
@@ -277,20 +277,22 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
         float aq[3][4], aep[3][4];
         uint32_t adem = 0;   // components with at least one dispersive cell in the group
         if (ADE) {
-            if (act && !special) {
+            if constexpr (!CP) {
+                if (act) {
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const int cl = (cw >> (8 * c)) & 0xff;
-                    const uint32_t fl = __float_as_uint(scls[cl * 4].w);
-                    if (fl & CF_ADE_BRANCH) adem |= fl & (CF_ADE_X | CF_ADE_Y | CF_ADE_Z);
-                    if (uni) break;
+                    for (int c = 0; c < 4; c++) {
+                        const int cl = (cw >> (8 * c)) & 0xff;
+                        const uint32_t fl = __float_as_uint(scls[cl * 4].w);
+                        if (fl & CF_ADE_BRANCH) adem |= fl & (CF_ADE_X | CF_ADE_Y | CF_ADE_Z);
+                        if (uni) break;
+                    }
                 }
-            }
 #pragma unroll
-            for (int a = 0; a < 3; a++) {
-                if (adem & (1u << a)) {
-                    ldq4a(aq[a], P.q[a] + c0i);
-                    ldg4a<T>(aep[a], P.fout[a], c0i);
+                for (int a = 0; a < 3; a++) {
+                    if (adem & (1u << a)) {
+                        ldq4a(aq[a], P.q[a] + c0i);
+                        ldg4a<T>(aep[a], P.fout[a], c0i);
+                    }
                 }
             }
             // the next plane's dispersive state into L2 (its class word is
@@ -316,6 +318,11 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                 }
             }
         }
+        // CPML tiles: the next plane's psi lines into L2, one request per
+        // 128-byte line of a row (the row's first own group and every group
+        // on a line boundary)
+        if (CP && ok && jk_in && i + 1 < ie && i + 1 < P.xr && i + 1 >= 0 && ((kq & 31) == 0 || tg == 1))
+            cp_prefetch_psi<T>(P, i + 1, j, kq);
         // ---- H phase: four cells per thread
         {
             const T *EX = ebox<T, L>(st, 0), *EY = ebox<T, L>(st, 1), *EZ = ebox<T, L>(st, 2);
@@ -331,7 +338,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
             lds4a<T>(hx, hbox<T, L>(st, 0) + hb);
             lds4a<T>(hy, hbox<T, L>(st, 1) + hb);
             lds4a<T>(hz, hbox<T, L>(st, 2) + hb);
-            if (!special) {
+            if constexpr (!CP) {
                 float da[4], db[4];
                 {
                     const float4 hc = scls[cl0 * 4 + 2];
@@ -357,7 +364,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
 #pragma unroll
                     for (int c = 0; c < 4; c++) tsf_add_h(P, i, j, kq + c, hx[c], hy[c], hz[c]);
                 }
-            } else if (CP) {
+            } else if (special) {
                 // ystep_h with kappa and the edge rules, then psi_H, TSF and the
                 // zeroed planes (fdtd_cpgroup.cuh); psi_H is written by the owner
                 float dyi[4], dzi[4], dxj[4], dzj[4], dxk[4], dyk[4];
@@ -401,9 +408,10 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
             const float hxj[4] = {hxj4.x, hxj4.y, hxj4.z, hxj4.w}, hzj[4] = {hzj4.x, hzj4.y, hzj4.z, hzj4.w};
             const float *eo[3] = {ex, ey, ez};
             float ne[3][4];
-            if (CP && special) {
+            if constexpr (CP) {
                 // the general E path (e_special: ADE with its CPML, ordinary
                 // update with kappa, PEC, zeroed planes, psi_E, TSF E) by group
+                // (an own group lies inside the grid)
                 cp_e_group<ADE, NPOLES, T>(P, scls, sade, cw, i, j, kq, c0i, tsf_plane, ex, ey, ez, hx, hy, hz, hxj, hzj,
                                            hxk0, hyk0, hyim, hzim, ne);
             } else {

@@ -8,12 +8,14 @@
 // stored before the next face's; the dispersive state of a component is one
 // vector per array.  A face of e_special does its first psi update (ADE
 // branch, corrections of the components the ADE owns) and its second
-// (corrections of the others) together: the two touch disjoint components,
-// each in the reference's face order x0 y0 z0 xn yn zn, so the sums are
-// those of e_special -- except the z0 correction of Ex, which the reference
-// gates by the z component: a cell whose ADE owns Ex but not Ez takes it
-// after its polarisation recursion and PEC rule, as e_special does.  FP32
-// arithmetic (tiles run FP32, FP16 and BF16 storage; no design region).
+// (corrections of the others) together: the two touch disjoint components.
+// The z0 correction of Ex, which the reference gates by the z component, is
+// the exception: a cell whose ADE owns Ex but not Ez takes it after its
+// polarisation recursion and PEC rule, as e_special does.  Faces go x, y, z,
+// one per axis (tiles need every grid extent >= both depths + 8); the
+// reference's order x0 y0 z0 xn yn zn differs from it only for a corner
+// group on faces of both sides, by rounding.  FP32 arithmetic (tiles run
+// FP32, FP16 and BF16 storage; no design region).
 //
 // psi vectors: a face of x or y covers the group whole (its psi rows run over
 // all k); a z face is read and written as one vector when its depth is a
@@ -61,6 +63,29 @@ __device__ __forceinline__ void psi_st4(float *p, int64_t q, bool vec, const boo
         for (int c = 0; c < 4; c++)
             if (m[c]) st_any<T>(p, q + c, Stor<T>::scaled ? v[c] * scale : v[c], stp, array);
     }
+}
+
+// The psi lines of the faces that hold group (i, j, kq) into L2: psi_E and
+// this step's input psi_H, both of which plane i reads.  Issued a plane ahead,
+// so that the special path's loads hit L2 rather than DRAM.
+template <class T>
+__device__ __forceinline__ void cp_prefetch_psi(const DevPlan &P, int i, int j, int kq)
+{
+    const int xr = P.xr, yr = P.yr, zr = P.zr;
+    auto pf = [&](int f, int64_t q) {
+        const int64_t b = q * (int64_t)sizeof(T);
+        prefetch_l2(reinterpret_cast<const char *>(P.psie[f][0]) + b);
+        prefetch_l2(reinterpret_cast<const char *>(P.psie[f][1]) + b);
+        prefetch_l2(reinterpret_cast<const char *>(P.psih_in[f][0]) + b);
+        prefetch_l2(reinterpret_cast<const char *>(P.psih_in[f][1]) + b);
+    };
+    if (P.cp_on[X0] && i < P.cp_d[X0]) pf(X0, ((int64_t)i * yr + j) * zr + kq);
+    if (P.cp_on[XN] && i >= xr - P.cp_d[XN]) pf(XN, ((int64_t)(i - (xr - P.cp_d[XN])) * yr + j) * zr + kq);
+    if (P.cp_on[Y0] && j < P.cp_d[Y0]) pf(Y0, ((int64_t)i * P.cp_d[Y0] + j) * zr + kq);
+    if (P.cp_on[YN] && j >= yr - P.cp_d[YN]) pf(YN, ((int64_t)i * P.cp_d[YN] + (j - (yr - P.cp_d[YN]))) * zr + kq);
+    if (P.cp_on[Z0] && kq < P.cp_d[Z0]) pf(Z0, ((int64_t)i * yr + j) * P.cp_d[Z0] + kq);
+    if (P.cp_on[ZN] && kq + 3 >= zr - P.cp_d[ZN])
+        pf(ZN, ((int64_t)i * yr + j) * P.cp_d[ZN] + max(kq - (zr - P.cp_d[ZN]), 0));
 }
 
 // H^{n+1/2} of a special group: h_update (special = true) then h_special,
@@ -167,25 +192,28 @@ __device__ __forceinline__ void cp_h_group(const DevPlan &P, const float4 *scls,
             psi_st4<T>(P.psih_out[f][0], q, all, m, ps, p0, stp, 18 + 2 * f + 0);
         }
     };
-    bool mz0[4], mzn[4], az0 = false, azn = false;
+    // one face per axis (tiles need every grid extent >= both depths + 8):
+    // x, then y, then z -- boundary_hstep's order x0 y0 z0 xn yn zn except
+    // for a corner group on faces of both sides, where the sums differ by
+    // rounding only
+    bool mz[4], az0 = false, azn = false;
     {
         const int d0 = P.cp_d[Z0], dn = P.cp_d[ZN];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const int k = kq + c;
-            mz0[c] = P.cp_on[Z0] && k < d0 - 1 && iin && jin;
-            mzn[c] = P.cp_on[ZN] && k >= zr - dn + 1 && k < zr - 1 && iin && jin;
-            az0 = az0 || mz0[c];
-            azn = azn || mzn[c];
+            const bool a0 = P.cp_on[Z0] && k < d0 - 1 && iin && jin;
+            const bool an = P.cp_on[ZN] && k >= zr - dn + 1 && k < zr - 1 && iin && jin;
+            mz[c] = a0 || an;
+            az0 = az0 || a0;
+            azn = azn || an;
         }
     }
-    // face order x0 y0 z0 xn yn zn (boundary_hstep)
     if (P.cp_on[X0] && i < P.cp_d[X0] - 1 && jin) xface(X0, i);
+    else if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1 && i < xr - 1 && jin) xface(XN, i - (xr - P.cp_d[XN]));
     if (P.cp_on[Y0] && j < P.cp_d[Y0] - 1 && iin) yface(Y0, j);
-    if (az0) zface(Z0, 0, mz0);
-    if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1 && i < xr - 1 && jin) xface(XN, i - (xr - P.cp_d[XN]));
-    if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1 && j < yr - 1 && iin) yface(YN, j - (yr - P.cp_d[YN]));
-    if (azn) zface(ZN, zr - P.cp_d[ZN], mzn);
+    else if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1 && j < yr - 1 && iin) yface(YN, j - (yr - P.cp_d[YN]));
+    if (az0 || azn) zface(az0 ? Z0 : ZN, az0 ? 0 : zr - P.cp_d[ZN], mz);
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const bool kl = kq + c == zr - 1;
@@ -394,25 +422,26 @@ __device__ __forceinline__ void cp_e_group(const DevPlan &P, const float4 *scls,
         psi_st4<T>(P.psie[f][0], q, vec, m, pse, p0, stp, 6 + 2 * f + 0);
         psi_st4<T>(P.psie[f][1], q, vec, m, pse, p1, stp, 6 + 2 * f + 1);
     };
-    bool iz0[4], izn[4], az0 = false, azn = false;
+    // one face per axis, x then y then z (as in cp_h_group)
+    bool iz[4], az0 = false, azn = false;
     {
         const int d0 = P.cp_d[Z0], dn = P.cp_d[ZN];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const int k = kq + c;
             zdx[c] = 0.f;
-            iz0[c] = P.cp_on[Z0] && k >= 1 && k < d0;
-            izn[c] = P.cp_on[ZN] && k >= zr - dn + 1;
-            az0 = az0 || iz0[c];
-            azn = azn || izn[c];
+            const bool a0 = P.cp_on[Z0] && k >= 1 && k < d0;
+            const bool an = P.cp_on[ZN] && k >= zr - dn + 1;
+            iz[c] = a0 || an;
+            az0 = az0 || a0;
+            azn = azn || an;
         }
     }
     if (P.cp_on[X0] && i >= 1 && i < P.cp_d[X0]) xface(X0, i, i > 1);
+    else if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1) xface(XN, i - (xr - P.cp_d[XN]), true);
     if (P.cp_on[Y0] && j >= 1 && j < P.cp_d[Y0]) yface(Y0, j, j > 1);
-    if (az0) zface(Z0, 0, iz0);
-    if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1) xface(XN, i - (xr - P.cp_d[XN]), true);
-    if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1) yface(YN, j - (yr - P.cp_d[YN]), true);
-    if (azn) zface(ZN, zr - P.cp_d[ZN], izn);
+    else if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1) yface(YN, j - (yr - P.cp_d[YN]), true);
+    if (az0 || azn) zface(az0 ? Z0 : ZN, az0 ? 0 : zr - P.cp_d[ZN], iz);
     // polarisation recursions of the owned components, their PEC rule
     if (ADE && adem) {
 #pragma unroll

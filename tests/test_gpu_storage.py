@@ -21,8 +21,9 @@ pytestmark = pytest.mark.gpu
 FIELD_TOL = {abi.STORE_F16: 5e-3, abi.STORE_BF16: 4e-2}
 FAR_TOL = {abi.STORE_F16: 1e-3, abi.STORE_BF16: 1e-2}
 STORES = [pytest.param(abi.STORE_F16, id="f16"), pytest.param(abi.STORE_BF16, id="bf16")]
-# k rows of 48 cells are 96 bytes at 16 bits: the TMA bulk kernel takes the interior
-SHAPE = (40, 36, 48)
+# k rows of 64 cells are 128 bytes at 16 bits: the TMA tiles run, and the
+# interior box is large enough for the bulk layout
+SHAPE = (40, 48, 64)
 
 
 def _scene(kind, storage, nsteps=40):
