@@ -266,7 +266,7 @@ std::vector<BulkItem> bulk_items(const int lo[3], const int hi[3], int len, int 
     for (int ib = lo[0]; ib < hi[0]; ib += len)
         for (int j0 = lo[1]; j0 < hi[1]; j0 += BULK_TJ)
             for (int k0 = lo[2]; k0 < hi[2]; k0 += BULK_TK)
-                blk.push_back({j0, k0, ib, std::min(hi[0], ib + len), hi[1], hi[2], inst, 0});
+                blk.push_back({j0, k0, ib, std::min(hi[0], ib + len), lo[1], hi[1], lo[2], hi[2], inst, 0});
     return blk;
 }
 
@@ -317,14 +317,19 @@ std::vector<std::pair<int, int>> plane_chunks(int a0, int a1, int target)
     return out;
 }
 
-// (j,k) tiles of [jlo, jhi) x [klo, khi) with tj x tk own cells, over the plane chunks
+// (j,k) tiles of [jlo, jhi) x [klo, khi) with tj x tk own cells, over the
+// plane chunks.  jend / kend: the tiles end at jhi / khi, so that the first
+// one may start below jlo / klo (its rows or groups there supply halo values
+// only); otherwise they start at jlo / klo and the last one ends past jhi / khi.
 void push_tiles(std::vector<BulkItem> &v, const std::vector<std::pair<int, int>> &ch, int jlo, int jhi, int klo, int khi,
-                int tj, int tk)
+                int tj, int tk, bool jend = false, bool kend = false)
 {
     if (jlo >= jhi || klo >= khi) return;
+    const int js = jend ? jhi - (jhi - jlo + tj - 1) / tj * tj : jlo;
+    const int ks = kend ? khi - (khi - klo + tk - 1) / tk * tk : klo;
     for (const auto &c : ch)
-        for (int j0 = jlo; j0 < jhi; j0 += tj)
-            for (int k0 = klo; k0 < khi; k0 += tk) v.push_back({j0, k0, c.first, c.second, jhi, khi, 0, 0});
+        for (int j0 = js; j0 < jhi; j0 += tj)
+            for (int k0 = ks; k0 < khi; k0 += tk) v.push_back({j0, k0, c.first, c.second, jlo, jhi, klo, khi, 0, 0});
 }
 
 template <class T>
@@ -351,12 +356,13 @@ namespace {
 // so that a batched launch may run it with the two-pole kernel variant
 // Work lists of the TMA tile kernels for a single plan.  The interior box
 // (every index plain on every axis, the bulk tile's halo row, group and plane
-// plain for H) goes to the bulk layout; the rest of the grid to the CPML
-// layouts: whole planes of the x slabs and rows of the y slabs in 15 x 60
-// tiles, the z slabs between the y slabs in 31 x 28 tiles.  The y and z
-// extents are rounded out to whole CPML tiles, so that every CPML tile is full
-// except at the grid's far edges.  Sets DevPlan::plo/phi, uploads the lists
-// and encodes the tensor maps of the three layouts.
+// plain for H) goes to the bulk layout, its last tiles partial; the rest of
+// the grid to the CPML layouts: whole planes of the x slabs and rows of the y
+// slabs in 15 x 60 tiles, the z slabs between the y slabs in 31 x 28 tiles.
+// The CPML tiles below the box end at its first row / k cell, so that the
+// part of them past the grid's low edge is the idle one.  Sets
+// DevPlan::plo/phi, uploads the lists and encodes the tensor maps of the
+// three layouts.
 int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls)
 {
     const int X = hp.xr, Y = hp.yr, Z = hp.zr;
@@ -378,10 +384,8 @@ int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls
     lo[2] = (lo[2] + 3) / 4 * 4;
     while (lo[2] < hi[2] && !(lo[2] - 4 >= a[2] - (below[2] ? 1 : 0))) lo[2] += 4;
     hi[2] = hi[2] / 4 * 4;
-    int bi0 = lo[0], bi1 = hi[0];
-    int bj0 = (lo[1] + CPXY_TJ - 1) / CPXY_TJ * CPXY_TJ, bj1 = Y - (Y - hi[1] + CPXY_TJ - 1) / CPXY_TJ * CPXY_TJ;
-    int bk0 = (lo[2] + CPZ_TK - 1) / CPZ_TK * CPZ_TK, bk1 = Z - (Z - hi[2] + CPZ_TK - 1) / CPZ_TK * CPZ_TK;
-    const bool bulk = bi0 < bi1 && bj0 < bj1 && bk0 < bk1 && hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];
+    int bi0 = lo[0], bi1 = hi[0], bj0 = lo[1], bj1 = hi[1], bk0 = lo[2], bk1 = hi[2];
+    const bool bulk = bi0 < bi1 && bj0 < bj1 && bk0 < bk1;
     std::vector<BulkItem> it[3];
     // planes per item: about 10 in the bulk (neighbouring tiles then share
     // their halo rows in L2; 512^3 rough surface, bulk kernel 2.24 ms at 96
@@ -393,9 +397,9 @@ int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls
         push_tiles(it[TILE_CPXY], xs0, 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
         push_tiles(it[TILE_CPXY], xs1, 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
         const auto mid = plane_chunks(bi0, bi1, 16);
-        push_tiles(it[TILE_CPXY], mid, 0, bj0, 0, Z, CPXY_TJ, CPXY_TK);
+        push_tiles(it[TILE_CPXY], mid, 0, bj0, 0, Z, CPXY_TJ, CPXY_TK, true, false);
         push_tiles(it[TILE_CPXY], mid, bj1, Y, 0, Z, CPXY_TJ, CPXY_TK);
-        push_tiles(it[TILE_CPZ], mid, bj0, bj1, 0, bk0, CPZ_TJ, CPZ_TK);
+        push_tiles(it[TILE_CPZ], mid, bj0, bj1, 0, bk0, CPZ_TJ, CPZ_TK, false, true);
         push_tiles(it[TILE_CPZ], mid, bj0, bj1, bk1, Z, CPZ_TJ, CPZ_TK);
     } else {
         bi0 = bi1 = bj0 = bj1 = bk0 = bk1 = 0;

@@ -230,7 +230,8 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
 
     // this thread's cells: row j = j0 - 1 + tr, k = kq .. kq + 3
     const int j = j0 - 1 + tr, kq = k0 - 4 + 4 * tg;
-    const bool own = tr >= 1 && tg >= 1 && j < it.jhi && kq < it.khi;   // groups are whole (khi - k0 % 4 == 0)
+    // groups are whole (klo, khi and k0 are multiples of 4)
+    const bool own = tr >= 1 && tg >= 1 && j >= it.jlo && j < it.jhi && kq >= it.klo && kq < it.khi;
     const int eb = tr * BWE + off + 4 * tg, hb = tr * BWH + off + 4 * tg, cb = tr * BWC + off8 + 4 * tg;
     // CPML tiles: every group inside the grid takes the special path (on a
     // plain cell it computes the plain update: kappa 1, no psi, no edge rule)

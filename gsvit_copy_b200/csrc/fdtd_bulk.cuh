@@ -15,9 +15,11 @@ struct BulkMaps {
     CUtensorMap cls;
 };
 
-// one CTA: own cells [j0, min(j0+TJ, jhi)) x [k0, min(k0+TK, khi)) of planes [ib, ie)
+// one CTA: own cells [max(j0, jlo), min(j0+TJ, jhi)) x [max(k0, klo), min(k0+TK, khi))
+// of planes [ib, ie); a tile may start below its region (j0 < jlo, k0 < klo,
+// even below 0): those rows and groups only supply halo values
 struct BulkItem {
-    int j0, k0, ib, ie, jhi, khi, inst, pad0;   // inst: plan of the item in a batched launch
+    int j0, k0, ib, ie, jlo, jhi, klo, khi, inst, pad0;   // inst: plan of the item in a batched launch
 };
 
 // Tile layouts: own rows (TJ) and own k cells (TK) of one CTA of 256 threads.
