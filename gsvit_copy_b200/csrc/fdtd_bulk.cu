@@ -274,26 +274,24 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
         const int64_t c0i = (int64_t)i * si + (int64_t)j * sj + kq;   // global index of this group's first cell
         // dispersive state of this group, requested before the H phase so that
         // the loads overlap it (Drude: Q and E^{n-1}; the pole state follows in
-        // the E phase); the special path loads its own
+        // the E phase)
         float aq[3][4], aep[3][4];
         uint32_t adem = 0;   // components with at least one dispersive cell in the group
         if (ADE) {
-            if constexpr (!CP) {
-                if (act) {
+            if (act) {
 #pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        const int cl = (cw >> (8 * c)) & 0xff;
-                        const uint32_t fl = __float_as_uint(scls[cl * 4].w);
-                        if (fl & CF_ADE_BRANCH) adem |= fl & (CF_ADE_X | CF_ADE_Y | CF_ADE_Z);
-                        if (uni) break;
-                    }
+                for (int c = 0; c < 4; c++) {
+                    const int cl = (cw >> (8 * c)) & 0xff;
+                    const uint32_t fl = __float_as_uint(scls[cl * 4].w);
+                    if (fl & CF_ADE_BRANCH) adem |= fl & (CF_ADE_X | CF_ADE_Y | CF_ADE_Z);
+                    if (uni) break;
                 }
+            }
 #pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    if (adem & (1u << a)) {
-                        ldq4a(aq[a], P.q[a] + c0i);
-                        ldg4a<T>(aep[a], P.fout[a], c0i);
-                    }
+            for (int a = 0; a < 3; a++) {
+                if (adem & (1u << a)) {
+                    ldq4a(aq[a], P.q[a] + c0i);
+                    ldg4a<T>(aep[a], P.fout[a], c0i);
                 }
             }
             // the next plane's dispersive state into L2 (its class word is
@@ -414,7 +412,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                 // update with kappa, PEC, zeroed planes, psi_E, TSF E) by group
                 // (an own group lies inside the grid)
                 cp_e_group<ADE, NPOLES, T>(P, scls, sade, cw, i, j, kq, c0i, tsf_plane, ex, ey, ez, hx, hy, hz, hxj, hzj,
-                                           hxk0, hyk0, hyim, hzim, ne);
+                                           hxk0, hyk0, hyim, hzim, adem, aq, aep, ne);
             } else {
                 float cu[3][4];   // curl H of the four cells
 #pragma unroll

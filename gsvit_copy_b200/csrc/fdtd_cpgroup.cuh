@@ -106,12 +106,15 @@ __device__ __forceinline__ void cp_h_group(const DevPlan &P, const float4 *scls,
     const float dx = P.dx, idx_ = 1.0f / dx;
     float dbdx[4];
     bool kin[4];
+    // 1/kappa of the four cells (kq % 4 == 0, the table is 256-byte aligned)
+    const float4 ikz4 = __ldg(reinterpret_cast<const float4 *>(P.ikh[2] + kq));
+    const float ikzs[4] = {ikz4.x, ikz4.y, ikz4.z, ikz4.w};
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const int k = kq + c;
         const float4 hc = scls[((cw >> (8 * c)) & 0xff) * 4 + 2];
         const float da = hc.x, db = hc.y;
-        const float ikz = __ldg(P.ikh[2] + k);
+        const float ikz = ikzs[c];
         const bool kl = k == zr - 1;
         kin[c] = k >= 1 && k < zr - 1;
         if (!(jl || kl)) hx[c] = da * hx[c] + db * (dey_k[c] * ikz - dez_j[c] * iky);
@@ -172,13 +175,15 @@ __device__ __forceinline__ void cp_h_group(const DevPlan &P, const float4 *scls,
         const int d = P.cp_d[f];
         const bool vec = (d & 3) == 0;
         const int64_t q = ((int64_t)i * yr + j) * d + (kq - base);
-        float p0[4], p1[4];
+        float p0[4], p1[4], bhs[4], chs[4];
         psi_ld4<T, true>(P.psih_in[f][1], q, vec, m, ips, p1);
         psi_ld4<T, true>(P.psih_in[f][0], q, vec, m, ips, p0);
+        psi_ld4<float, true>(P.bh[f], kq - base, vec, m, 1.f, bhs);   // profiles of the four cells
+        psi_ld4<float, true>(P.ch[f], kq - base, vec, m, 1.f, chs);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             if (!m[c]) continue;
-            const float bh = __ldg(P.bh[f] + (kq + c - base)), ch = __ldg(P.ch[f] + (kq + c - base));
+            const float bh = bhs[c], ch = chs[c];
             const float pyz = bh * p1[c] + ch * dex_k[c] * idx_;
             const float pxz = bh * p0[c] + ch * dey_k[c] * idx_;
             hy[c] -= dbdx[c] * pyz;
@@ -225,13 +230,16 @@ __device__ __forceinline__ void cp_h_group(const DevPlan &P, const float4 *scls,
 // E^{n+1} of a special group: e_special for the four cells.  e*: E^n; h*:
 // H^{n+1/2} of the cells, hxj/hzj of row j-1, hxk0/hyk0 of cell kq-1,
 // hyim/hzim of plane i-1.  Writes psi_E and the dispersive state; returns
-// the new E in ne (before the store).
+// the new E in ne (before the store).  adem, aq, aep: the components owned by
+// the ADE in some cell of the group and their Q and E^{n-1}, which the caller
+// requested before the H phase (the loads then overlap it).
 template <bool ADE, int NPOLES, class T>
 __device__ __forceinline__ void cp_e_group(const DevPlan &P, const float4 *scls, const DevAde *sade, uint32_t cw, int i, int j,
                                            int kq, int64_t c0i, bool tsf, const float (&ex)[4], const float (&ey)[4],
                                            const float (&ez)[4], const float (&hx)[4], const float (&hy)[4],
                                            const float (&hz)[4], const float (&hxj)[4], const float (&hzj)[4], float hxk0,
-                                           float hyk0, const float (&hyim)[4], const float (&hzim)[4], float (&ne)[3][4])
+                                           float hyk0, const float (&hyim)[4], const float (&hzim)[4], uint32_t adem,
+                                           float (&aq)[3][4], const float (&aep)[3][4], float (&ne)[3][4])
 {
     const int xr = P.xr, yr = P.yr, zr = P.zr;
     const uint32_t stp = sr_step<T>(P);
@@ -248,21 +256,14 @@ __device__ __forceinline__ void cp_e_group(const DevPlan &P, const float4 *scls,
     auto cls_of = [&](int c) { return (int)((cw >> (8 * c)) & 0xff); };
 
     bool zero[4];
-    uint32_t adem = 0;   // components owned by the ADE in at least one cell
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-        zero[c] = (P.cp_on[X0] && i == 0) || (P.cp_on[Y0] && j == 0) || (P.cp_on[Z0] && kq + c == 0);
-        const unsigned fl = __float_as_uint(scls[cls_of(c) * 4].w);
-        if (ADE && (fl & CF_ADE_BRANCH)) adem |= fl & (CF_ADE_X | CF_ADE_Y | CF_ADE_Z);
-    }
-    // dispersive state of the owned components (difference form, DevAde)
-    float aq[3][4], aep[3][4], pq[3][2][4], qq[3][2][4];
-    if (ADE) {
+    for (int c = 0; c < 4; c++) zero[c] = (P.cp_on[X0] && i == 0) || (P.cp_on[Y0] && j == 0) || (P.cp_on[Z0] && kq + c == 0);
+    // pole state of the owned components (difference form, DevAde)
+    float pq[3][2][4], qq[3][2][4];
+    if (ADE && NPOLES > 0) {
 #pragma unroll
         for (int a = 0; a < 3; a++) {
             if (!(adem & (1u << a))) continue;
-            ldq4a(aq[a], P.q[a] + c0i);
-            ldg4a<T>(aep[a], P.fout[a], c0i);
 #pragma unroll
             for (int n = 0; n < NPOLES; n++) {
                 ldq4a(pq[a][n], P.pc[a][n] + c0i);
@@ -272,13 +273,15 @@ __device__ __forceinline__ void cp_e_group(const DevPlan &P, const float4 *scls,
     }
     // ADE values before the CPML corrections, ordinary update and PEC of the
     // other components
+    const float4 ikz4 = __ldg(reinterpret_cast<const float4 *>(P.ike[2] + kq));
+    const float ikzs[4] = {ikz4.x, ikz4.y, ikz4.z, ikz4.w};
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const int k = kq + c;
         const int cl = cls_of(c);
         const float4 c0 = scls[cl * 4 + 0], c1 = scls[cl * 4 + 1];
         const unsigned fl = __float_as_uint(c0.w);
-        const float ikz = __ldg(P.ike[2] + k);
+        const float ikz = ikzs[c];
         const float curl[3] = {d_zj(c) * iky - d_yk(c) * ikz, d_xk(c) * ikz - d_zi(c) * ikx, d_yi(c) * ikx - d_xj(c) * iky};
         const bool gd[3] = {j > 0 && k > 0, i > 0 && k > 0, i > 0 && j > 0};
         const float eo[3] = {ex[c], ey[c], ez[c]};
@@ -390,16 +393,18 @@ __device__ __forceinline__ void cp_e_group(const DevPlan &P, const float4 *scls,
 #pragma unroll
         for (int c = 0; c < 4; c++) { m[c] = in[c] && !zero[c] && i > 0 && j > 0; any = any || m[c]; }
         if (!any) return;
-        float p0[4], p1[4];
+        float p0[4], p1[4], bes[4], ces[4];
         psi_ld4<T, false>(P.psie[f][1], q, vec, m, ipse, p1);
         psi_ld4<T, false>(P.psie[f][0], q, vec, m, ipse, p0);
+        psi_ld4<float, true>(P.be[f], kq - base, vec, m, 1.f, bes);   // profiles of the four cells
+        psi_ld4<float, true>(P.ce[f], kq - base, vec, m, 1.f, ces);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             if (!m[c]) continue;
             const int k = kq + c;
             const int cl = cls_of(c);
             const unsigned fl = __float_as_uint(scls[cl * 4].w);
-            const float be = __ldg(P.be[f] + (k - base)), ce = __ldg(P.ce[f] + (k - base));
+            const float be = bes[c], ce = ces[c];
             const float dxk = d_xk(c), dyk = d_yk(c);
             if (ADE && (fl & CF_ADE_BRANCH) && (f == ZN || k > 1)) {
                 p1[c] = be * p1[c] + ce * dxk * idx_;
