@@ -511,58 +511,81 @@ def extensions(a, device):
 
 def run_batched(a):
     """48 independent rough-surface instances (x, y in {64, 96, 128, 192}, z in
-    {64, 96, 128}, Drude or Lorentz, 8-cell CPML) stepped as one batch after the
-    autotuner picked its work list, against the same instances stepped one by
-    one with the plain solver (each from a CUDA graph).  Gcell-updates/s over
-    all instances, device-timed; the fields are set to the same seeded state
-    in both runs."""
+    {64, 96, 128}, Drude or Lorentz, 8-cell CPML) stepped as one batch per GPU
+    after the autotuner picked its work list, against the same instances
+    stepped one by one with the plain solver (each from a CUDA graph).  With N
+    ranks (torchrun, one GPU each) the instances are split whole across the
+    ranks (plan.shard_instances: no exchange, weak in the instance count per
+    GPU), each rank steps its own batch, and the batch arm is timed on the
+    device (events on the batch's stream) as the max over ranks.  value =
+    the cell updates of all instances over that time."""
     import torch
     from gsvit_copy_b200 import plan
     from gsvit_copy_b200.solver import Batch, Solver
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    ranks = Replicas("nccl", torch.device("cuda", local))
     K, W = a.steps, a.warmup
-    scenes = plan.batch_scenes(48, nsteps=max(2000, K + W + 64))
-    cells = sum(sc.ncells for sc in scenes)
-    torch.cuda.set_device(0)
-    ev = lambda: torch.cuda.Event(enable_timing=True)
-    batch = Batch(scenes)
+    scenes_all = plan.batch_scenes(48, nsteps=max(2000, K + W + 64))
+    cells_all = [sc.ncells for sc in scenes_all]
+    mine = plan.shard_instances(cells_all, world)[rank]
+    scenes = [scenes_all[q] for q in mine]
+    cells = sum(cells_all)
+    batch = Batch(scenes, device=local)
     tune = batch.tune(trial_steps=3)
     cfg = batch.config()
+    ext = torch.cuda.ExternalStream(batch.stream_handle())
     batch.step_graph(W + (W % 2), chunk=16)
     batch.sync()
     torch.cuda.synchronize()
-    with ClockSampler(bus_id_of(0)) as clk:
-        t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ranks.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(bus_id_of(local)) as clk:
+        e0.record(ext)
         batch.step_graph(K, chunk=16)
-        batch.sync()
-        batch_s = time.perf_counter() - t0
+        e1.record(ext)
+        torch.cuda.synchronize()
+    batch.sync()
+    ranks.barrier()
+    batch_ms = ranks.max(e0.elapsed_time(e1))
     clocks = clk.summary()
     batch.close()
-    # one by one: each instance its own plan and graph, the same step count
-    single_s = 0.0
+    # one by one: each instance of this rank its own plan and graph, the same step count
+    single_ms = 0.0
+    stream = torch.cuda.Stream()
     for sc in scenes:
-        g = Solver(sc)
+        g = Solver(sc, device=local)
+        g.set_stream(stream.cuda_stream)
         g.step_graph(W + (W % 2), chunk=16)
         g.sync()
-        t0 = time.perf_counter()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
         g.step_graph(K, chunk=16)
+        f1.record(stream)
+        torch.cuda.synchronize()
         g.sync()
-        single_s += time.perf_counter() - t0
+        single_ms += f0.elapsed_time(f1)
         g.close()
-    value = cells * K / batch_s / 1e9
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
-        "ms_per_step": batch_s / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded height maps, sizes, materials, angles)",
-        "config": {"workload": "48 rough-surface instances, x,y in {64,96,128,192}, z in {64,96,128}, Drude or Lorentz, "
-                               "8-cell CPML, TSF 0-60 deg, NFFF 3 wavelengths 10x19", "cells": cells,
-                   "batch_work_list": cfg, "tuner": [{"planes_per_item": t[0], "persistent": t[1], "ms_per_step": t[2]}
-                                                    for t in tune]},
-        "one_by_one": {"value": cells * K / single_s / 1e9, "unit": UNIT, "ms_per_step": single_s / K * 1e3},
-        "speedup_vs_one_by_one": single_s / batch_s,
-        "timing": "host clock around synchronised device work, both arms",
-        "clocks": clocks,
-    }
-    print(json.dumps(line), flush=True)
+    single_ms = ranks.max(single_ms)
+    value = cells * K / (batch_ms * 1e-3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": batch_ms / K, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded height maps, sizes, materials, angles)",
+            "config": {"workload": "48 rough-surface instances, x,y in {64,96,128,192}, z in {64,96,128}, Drude or Lorentz, "
+                                   "8-cell CPML, TSF 0-60 deg, NFFF 3 wavelengths 10x19", "cells": cells,
+                       "parallelism": f"instances split whole over {world} GPU(s), no exchange",
+                       "instances_rank0": len(mine), "batch_work_list_rank0": cfg,
+                       "tuner_rank0": [{"planes_per_item": t[0], "persistent": t[1], "ms_per_step": t[2]} for t in tune]},
+            "one_by_one": {"value": cells * K / (single_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": single_ms / K},
+            "speedup_vs_one_by_one": single_ms / batch_ms,
+            "timing": "CUDA events on the batch's stream (and the solver stream one by one), max over ranks",
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ranks.close()
     return 0
 
 
@@ -600,14 +623,16 @@ def run_adjoint(a):
         # same scene with FP64 fields and arithmetic, so that h = 1e-3 is not
         # drowned by FP32 rounding
         from gsvit_copy_b200 import abi
+        obj_fd = obj
         if a.fd_storage == "f64":
             s_fd = plan.adjoint_scene(nsteps=n)
+            obj_fd = plan.cone_objective(s_fd)   # the same far points, appended to this scene's NFFF
             s_fd.storage = abi.STORE_F64
             g.close()
             g = Solver(s_fd)
         init = g.snapshot()
         g.step(n)
-        J_fd = g.objective_value(obj)
+        J_fd = g.objective_value(obj_fd)
         rng = np.random.default_rng(16)
         cells = [tuple(int(rng.integers(0, m)) for m in grad.shape) for _ in range(a.fd_cells)]
         eps0 = s.design["eps"].copy()
@@ -620,7 +645,7 @@ def run_adjoint(a):
                 g.restore(init)
                 g.set_design_eps(e)
                 g.step(n)
-                jj.append(g.objective_value(obj))
+                jj.append(g.objective_value(obj_fd))
             vals.append((jj[0] - jj[1]) / (2 * a.fd_h))
         g.set_design_eps(eps0)
         fdv = np.array(vals)

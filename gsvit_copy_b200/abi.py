@@ -166,6 +166,7 @@ def load_library():
         "fdtd_batch_sync": ([P], C.c_int),
         "fdtd_batch_tune": ([P, C.c_int, _dp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "fdtd_batch_config": ([P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "fdtd_batch_get_stream": ([P, C.POINTER(P)], C.c_int),
         "fdtd_set_design_eps": ([P, _dp], C.c_int),
         "fdtd_objective_value": ([P, C.POINTER(Objective), _dp], C.c_int),
         "fdtd_adjoint_gradient": ([P, C.POINTER(Objective), C.c_int, C.c_int, _dp, _dp], C.c_int),
@@ -187,7 +188,7 @@ HEADER_SYMBOLS = [
     "fdtd_snapshot_size", "fdtd_snapshot_save", "fdtd_snapshot_restore",
     "fdtd_last_error", "fdtd_step_bytes",
     "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_size", "fdtd_batch_plan", "fdtd_batch_step",
-    "fdtd_batch_step_graph", "fdtd_batch_sync", "fdtd_batch_tune", "fdtd_batch_config",
+    "fdtd_batch_step_graph", "fdtd_batch_sync", "fdtd_batch_tune", "fdtd_batch_config", "fdtd_batch_get_stream",
     "fdtd_set_design_eps", "fdtd_objective_value", "fdtd_adjoint_gradient", "fdtd_adjoint_transpose",
 ]
 

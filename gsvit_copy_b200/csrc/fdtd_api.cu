@@ -107,14 +107,14 @@ struct fdtd_plan {
     bool bulk_on = false;
     BulkMaps bmaps[2];
     // TMA tiles of the whole grid (single plans): bulk items of the interior
-    // box and the CPML tiles around it (TILE_BULK / TILE_CPXY / TILE_CPZ)
+    // box and the CPML tiles around it (TILE_BULK / TILE_CPX / TILE_CPY / TILE_CPZ)
     bool tiles_on = false;
-    BulkItem *d_tiles[3] = {nullptr, nullptr, nullptr};
-    int ntiles[3] = {0, 0, 0};
-    BulkMaps tmaps[3][2];
-    std::vector<BulkItem> h_tiles[3];     // host copies of the tile lists (batched launches)
+    BulkItem *d_tiles[NTILE] = {};
+    int ntiles[NTILE] = {};
+    BulkMaps tmaps[NTILE][2];
+    std::vector<BulkItem> h_tiles[NTILE];   // host copies of the tile lists (batched launches)
     int stall = 0;                        // tests: expire every CTA's first wait after this many polls
-    double tile_bytes[3] = {0, 0, 0};     // algorithmic HBM bytes per launch of each tile kind
+    double tile_bytes[NTILE] = {};         // algorithmic HBM bytes per launch of each tile kind
     int *d_err = nullptr;                 // set by a bulk CTA whose bounded wait expired
     const int *batch_err = nullptr;       // the batch's error word, for an instance of a batch
     bool failed = false;                  // an expired wait was reported: the plan only accepts destroy
@@ -201,7 +201,7 @@ int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
     DevPlan d = plan_for(P, in);
     cudaError_t e;
     if (P->tiles_on) {
-        for (int kind = 0; kind < 3; kind++) {
+        for (int kind = 0; kind < NTILE; kind++) {
             const int rc = launch_tile_kind(P, d, in, kind, st);
             if (rc != FDTD_OK) return rc;
         }
@@ -386,7 +386,15 @@ int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls
     hi[2] = hi[2] / 4 * 4;
     int bi0 = lo[0], bi1 = hi[0], bj0 = lo[1], bj1 = hi[1], bk0 = lo[2], bk1 = hi[2];
     const bool bulk = bi0 < bi1 && bj0 < bj1 && bk0 < bk1;
-    std::vector<BulkItem> it[3];
+    // design cells (per-cell E coefficients) are handled by the bulk layout
+    // only: a plan whose design cells reach outside the interior box keeps the
+    // slab kernels
+    if (hp.design && !(bulk && hp.abox[0] >= bi0 && hp.abox[1] <= bi1 && hp.abox[2] >= bj0 && hp.abox[3] <= bj1 &&
+                       hp.abox[4] >= bk0 && hp.abox[5] <= bk1)) {
+        P->tiles_on = false;
+        return FDTD_OK;
+    }
+    std::vector<BulkItem> it[NTILE];
     // planes per item: about 10 in the bulk (neighbouring tiles then share
     // their halo rows in L2; 512^3 rough surface, bulk kernel 2.24 ms at 96
     // planes, 1.72 ms at 8-12, 1.79 ms at 4), whole x slabs, 16 in the y and z
@@ -394,16 +402,16 @@ int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls
     if (bulk) {
         push_tiles(it[TILE_BULK], plane_chunks(bi0, bi1, 10), bj0, bj1, bk0, bk1, BULK_TJ, BULK_TK);
         const auto xs0 = plane_chunks(0, bi0, 1 << 30), xs1 = plane_chunks(bi1, X, 1 << 30);
-        push_tiles(it[TILE_CPXY], xs0, 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
-        push_tiles(it[TILE_CPXY], xs1, 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
+        push_tiles(it[TILE_CPX], xs0, 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
+        push_tiles(it[TILE_CPX], xs1, 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
         const auto mid = plane_chunks(bi0, bi1, 16);
-        push_tiles(it[TILE_CPXY], mid, 0, bj0, 0, Z, CPXY_TJ, CPXY_TK, true, false);
-        push_tiles(it[TILE_CPXY], mid, bj1, Y, 0, Z, CPXY_TJ, CPXY_TK);
+        push_tiles(it[TILE_CPY], mid, 0, bj0, 0, Z, CPXY_TJ, CPXY_TK, true, false);
+        push_tiles(it[TILE_CPY], mid, bj1, Y, 0, Z, CPXY_TJ, CPXY_TK);
         push_tiles(it[TILE_CPZ], mid, bj0, bj1, 0, bk0, CPZ_TJ, CPZ_TK, false, true);
         push_tiles(it[TILE_CPZ], mid, bj0, bj1, bk1, Z, CPZ_TJ, CPZ_TK);
     } else {
         bi0 = bi1 = bj0 = bj1 = bk0 = bk1 = 0;
-        push_tiles(it[TILE_CPXY], plane_chunks(0, X, 16), 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
+        push_tiles(it[TILE_CPX], plane_chunks(0, X, 16), 0, Y, 0, Z, CPXY_TJ, CPXY_TK);
     }
     // algorithmic bytes per launch: fields 12 x esz + class byte per cell, the
     // dispersive state of dispersive components, 4 psi values read and written
@@ -424,21 +432,31 @@ int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls
                 }
         return bsum;
     };
-    double psi = 0;
-    for (int f = 0; f < 6; f++)
-        if (hp.cp[f].enabled) {
-            const int dep = hp.cp[f].depth;
-            psi += ((f < 2) ? (double)dep * Y * Z : (f < 4) ? (double)X * dep * Z : (double)X * Y * dep) * 4 * 2.0 * esz;
-        }
     const double all = box_bytes(0, X, 0, Y, 0, Z);
     P->tile_bytes[TILE_BULK] = box_bytes(bi0, bi1, bj0, bj1, bk0, bk1);
     P->tile_bytes[TILE_CPZ] = box_bytes(bi0, bi1, bj0, bj1, 0, bk0) + box_bytes(bi0, bi1, bj0, bj1, bk1, Z);
-    P->tile_bytes[TILE_CPXY] = all - P->tile_bytes[TILE_BULK] - P->tile_bytes[TILE_CPZ] + psi;
+    P->tile_bytes[TILE_CPY] = box_bytes(bi0, bi1, 0, bj0, 0, Z) + box_bytes(bi0, bi1, bj1, Y, 0, Z);
+    P->tile_bytes[TILE_CPX] = all - P->tile_bytes[TILE_BULK] - P->tile_bytes[TILE_CPZ] - P->tile_bytes[TILE_CPY];
+    // psi values: charged to the CPML kinds by the cells of each slab they hold
+    for (int f = 0; f < 6; f++)
+        if (hp.cp[f].enabled) {
+            const int dep = hp.cp[f].depth;
+            const double per = 4 * 2.0 * esz;
+            if (f < 2) P->tile_bytes[TILE_CPX] += (double)dep * Y * Z * per;
+            else if (f < 4) {   // y slabs: the x-slab planes belong to CPX
+                P->tile_bytes[TILE_CPX] += (double)(X - (bi1 - bi0)) * dep * Z * per;
+                P->tile_bytes[TILE_CPY] += (double)(bi1 - bi0) * dep * Z * per;
+            } else {   // z slabs: CPX planes, CPY rows, CPZ the rest
+                P->tile_bytes[TILE_CPX] += (double)(X - (bi1 - bi0)) * Y * dep * per;
+                P->tile_bytes[TILE_CPY] += (double)(bi1 - bi0) * (Y - (bj1 - bj0)) * dep * per;
+                P->tile_bytes[TILE_CPZ] += (double)(bi1 - bi0) * (bj1 - bj0) * dep * per;
+            }
+        }
     void *fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
     if (e != cudaSuccess || !fn || q != cudaDriverEntryPointSuccess) return fail(FDTD_E_CUDA, "cuTensorMapEncodeTiled entry point");
-    for (int kind = 0; kind < 3; kind++) {
+    for (int kind = 0; kind < NTILE; kind++) {
         P->ntiles[kind] = (int)it[kind].size();
         P->h_tiles[kind] = it[kind];
         if (it[kind].empty()) continue;
@@ -1041,12 +1059,24 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         // TMA tiles over the whole grid (single plans; batches may use them too)
         // the CPML tiles take one face per axis: every extent at least both depths + 8
         bool roomy = true;
+        int dmin = 1 << 30;
         for (int ax = 0; ax < 3; ax++) {
             const int ext = ax == 0 ? X : ax == 1 ? Y : Z;
             const int dd = (hp.cp[2 * ax].enabled ? hp.cp[2 * ax].depth : 0) + (hp.cp[2 * ax + 1].enabled ? hp.cp[2 * ax + 1].depth : 0);
             roomy = roomy && ext >= dd + 8;
+            for (int f = 2 * ax; f < 2 * ax + 2; f++)
+                if (hp.cp[f].enabled) dmin = std::min(dmin, hp.cp[f].depth);
         }
-        P->tiles_on = !hp.design && !r64 && roomy && ((size_t)Z * esz % 16 == 0) && !(nob && nob[0] == '1');
+        const bool can_tile = !r64 && roomy && ((size_t)Z * esz % 16 == 0) && !(nob && nob[0] == '1');
+        // Default: tiles for CPML of depth >= 16.  Thinner slabs fill the CPML
+        // tiles poorly (a z slab of depth 8 uses 12 of a z tile's 28 k cells)
+        // and the slab kernels are faster there (the 48-instance batch with
+        // 8-cell CPML: 8.4 Gcell/s tiled against 13.8 on the slab kernels; the
+        // 512^3 rough surface with 16-cell CPML: 3.03 against 3.05 ms).
+        // GSVIT_B200_TILES=1 / 0 at plan creation forces them on / off.
+        const char *tv = getenv("GSVIT_B200_TILES");
+        const bool want = tv ? tv[0] == '1' : dmin >= 16;
+        P->tiles_on = can_tile && want;
         // test hook of the bounded-wait error path: every tile CTA of this plan
         // also waits, at most this many polls, on an mbarrier nothing arrives on
         if (const char *stv = getenv("GSVIT_B200_STALL_TEST")) P->stall = std::max(0, atoi(stv));
@@ -1478,8 +1508,7 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
             int rc = launch_tile_kind(P, d, in, TILE_BULK, st);
             if (rc != FDTD_OK) return rc;
             CK(cudaEventRecord(E[2], st));
-            rc = launch_tile_kind(P, d, in, TILE_CPXY, st);
-            if (rc == FDTD_OK) rc = launch_tile_kind(P, d, in, TILE_CPZ, st);
+            for (int kind = TILE_CPX; kind < NTILE && rc == FDTD_OK; kind++) rc = launch_tile_kind(P, d, in, kind, st);
             if (rc != FDTD_OK) return rc;
         } else {
             if (P->bulk_on) {
@@ -1519,8 +1548,9 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
     int nyee;
     if (P->tiles_on) {
         out[1] = P->tile_bytes[TILE_BULK];
-        out[3] = P->tile_bytes[TILE_CPXY] + P->tile_bytes[TILE_CPZ];
-        nyee = (P->ntiles[TILE_BULK] > 0) + (P->ntiles[TILE_CPXY] > 0) + (P->ntiles[TILE_CPZ] > 0);
+        out[3] = P->tile_bytes[TILE_CPX] + P->tile_bytes[TILE_CPY] + P->tile_bytes[TILE_CPZ];
+        nyee = 0;
+        for (int kind = 0; kind < NTILE; kind++) nyee += P->ntiles[kind] > 0;
     } else {
         out[1] = P->bulk_bytes;
         out[3] = P->slab_bytes;
@@ -1710,9 +1740,9 @@ struct fdtd_batch {
     // and tile kind, one CTA per item) or the bulk box and slab kernels (the
     // lists above hold only these instances).
     int ntiled = 0;
-    BulkItem *d_titems[3][3] = {};   // [variant group][tile kind]
-    int ntitems[3][3] = {};
-    BulkMaps *d_tmaps[3][2] = {};    // [tile kind][parity], indexed by instance
+    BulkItem *d_titems[3][NTILE] = {};   // [variant group][tile kind]
+    int ntitems[3][NTILE] = {};
+    BulkMaps *d_tmaps[NTILE][2] = {};    // [tile kind][parity], indexed by instance
 };
 
 namespace {
@@ -1770,7 +1800,7 @@ int batch_launch_step(fdtd_batch *B, cudaStream_t st)
     launch_aux_step_batch(B->d_aux[in], n, st);
     if (B->max_tsf) launch_tsf_faces_batch(B->d_plans[in], n, B->max_tsf, st);
     for (int g = 0; g < 3; g++)   // instances with TMA tiles
-        for (int kind = 0; kind < 3; kind++) {
+        for (int kind = 0; kind < NTILE; kind++) {
             if (!B->ntitems[g][kind]) continue;
             cudaError_t e = launch_tiles_batch(kind, B->d_plans[in], B->d_tmaps[kind][in], B->d_titems[g][kind],
                                                B->ntitems[g][kind], B->ncls, B->d_err, g > 0, g == 2 ? 2 : 0, B->storage, st);
@@ -1933,7 +1963,7 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
     for (auto *P : B->plans) P->batch_err = B->d_err;   // the instances' readbacks check the batch's word too
     for (auto *P : B->plans) B->ntiled += P->tiles_on ? 1 : 0;
     if (B->ntiled) {
-        for (int kind = 0; kind < 3; kind++) {
+        for (int kind = 0; kind < NTILE; kind++) {
             for (int in = 0; in < 2; in++) {
                 std::vector<BulkMaps> tm(nplans);
                 std::memset(tm.data(), 0, sizeof(BulkMaps) * nplans);
@@ -1965,6 +1995,13 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
 int fdtd_batch_destroy(fdtd_batch *B)
 {
     batch_free(B);
+    return FDTD_OK;
+}
+
+int fdtd_batch_get_stream(const fdtd_batch *B, void **stream)
+{
+    if (!B || !stream) return fail(FDTD_E_INVALID, "NULL argument");
+    *stream = (void *)B->stream;
     return FDTD_OK;
 }
 

@@ -191,11 +191,12 @@ __device__ __forceinline__ void bulk_init_bars(const BulkSmem &m)
 // ((gplane + p - p0) / S) & 1, gplane counting the planes this CTA has
 // streamed in earlier items, so that a persistent CTA keeps its mbarriers.
 // Returns false when a bounded wait gave up (after draining its copies).
-template <bool ADE, int NPOLES, class T, class L, bool CP>
+template <bool ADE, int NPOLES, class T, class L, int CPF>
 __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, const BulkItem &it, const BulkSmem &m,
                                           uint32_t &gplane, int *err, int stall)
 {
     constexpr int TGRP = L::TGRP, TROWS = L::TROWS, NTH = L::NTH;
+    constexpr bool CP = CPF != 0;   // a CPML layout; CPF: the faces its tiles can meet (CPF_X | CPF_Y | CPF_Z)
     unsigned char *stages = m.stages;
     const float4 *scls = m.scls;
     float4 *xch = m.xch;
@@ -269,7 +270,9 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
         const bool special = CP && jk_in && i >= 0 && i < P.xr;
         const uint32_t cw = *reinterpret_cast<const uint32_t *>(cbox<T, L>(st) + cb);
         const int cl0 = cw & 0xff;
-        const bool uni = cw == (uint32_t)cl0 * 0x01010101u;   // one class for the four cells
+        // one class for the four cells (and no design cell: those take per-cell
+        // coefficients on the cell-by-cell path)
+        const bool uni = cw == (uint32_t)cl0 * 0x01010101u && !(P.dcoef && (__float_as_uint(scls[cl0 * 4].w) & CF_DESIGN));
         const bool tsf_plane = (tifc && (i == ti0 - 1 || i == ti0 || i == tin)) || (tlat && i >= ti0 && i <= tin);
         const int64_t c0i = (int64_t)i * si + (int64_t)j * sj + kq;   // global index of this group's first cell
         // dispersive state of this group, requested before the H phase so that
@@ -378,7 +381,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                     dxk[c] = exk - ex[c];
                     dyk[c] = eyk - ey[c];
                 }
-                cp_h_group<T>(P, scls, cw, i, j, kq, act, tsf_plane, dyi, dzi, dxj, dzj, dxk, dyk, hx, hy, hz);
+                cp_h_group<CPF, T>(P, scls, cw, i, j, kq, act, tsf_plane, dyi, dzi, dxj, dzj, dxk, dyk, hx, hy, hz);
             }
             if (act) {
                 const float q = Stor<T>::scaled ? P.hs : 1.f;
@@ -411,7 +414,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                 // the general E path (e_special: ADE with its CPML, ordinary
                 // update with kappa, PEC, zeroed planes, psi_E, TSF E) by group
                 // (an own group lies inside the grid)
-                cp_e_group<ADE, NPOLES, T>(P, scls, sade, cw, i, j, kq, c0i, tsf_plane, ex, ey, ez, hx, hy, hz, hxj, hzj,
+                cp_e_group<CPF, ADE, NPOLES, T>(P, scls, sade, cw, i, j, kq, c0i, tsf_plane, ex, ey, ez, hx, hy, hz, hxj, hzj,
                                            hxk0, hyk0, hyim, hzim, adem, aq, aep, ne);
             } else {
                 float cu[3][4];   // curl H of the four cells
@@ -477,13 +480,19 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
 #pragma unroll
                             for (int c = 0; c < 4; c++) ne[a][c] = 0.f;
                 } else {
-                    // material boundary inside the group: cell by cell
+                    // material boundary inside the group, or a design cell: cell by cell
 #pragma unroll
                     for (int c = 0; c < 4; c++) {
                         const int cl = (cw >> (8 * c)) & 0xff;
                         const float4 c0 = scls[cl * 4 + 0], c1 = scls[cl * 4 + 1];
                         const unsigned fl = __float_as_uint(c0.w);
-                        const float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z};
+                        float ca[3] = {c0.x, c0.y, c0.z}, cb[3] = {c1.x, c1.y, c1.z};
+                        if (fl & CF_DESIGN) {   // adjoint design region: coefficients per cell (DevPlan::dcoef)
+                            const int64_t q = ((int64_t)(i - P.dbox[0]) * (P.dbox[3] - P.dbox[2]) + (j - P.dbox[2])) *
+                                                  (P.dbox[5] - P.dbox[4]) + (kq + c - P.dbox[4]);
+#pragma unroll
+                            for (int a = 0; a < 3; a++) { ca[a] = __ldg(P.dcoef + 6 * q + a); cb[a] = __ldg(P.dcoef + 6 * q + 3 + a); }
+                        }
 #pragma unroll
                         for (int a = 0; a < 3; a++) ne[a][c] = ca[a] * eo[a][c] + cb[a] * cu[a][c];
                         if (ADE && (fl & CF_ADE_BRANCH)) {
@@ -552,7 +561,7 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
     return true;
 }
 
-template <bool ADE, int NPOLES, class T, class L, bool CP>
+template <bool ADE, int NPOLES, class T, class L, int CPF>
 __global__ void __launch_bounds__(L::NTH, 2) tile_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ BulkMaps M,
                                                          const BulkItem *items, int *err, int stall)
 {
@@ -565,12 +574,12 @@ __global__ void __launch_bounds__(L::NTH, 2) tile_kernel(const __grid_constant__
     __syncthreads();
     uint32_t gplane = 0;
     const BulkItem it = items[blockIdx.x];
-    bulk_item<ADE, NPOLES, T, L, CP>(P, M, it, m, gplane, err, stall);
+    bulk_item<ADE, NPOLES, T, L, CPF>(P, M, it, m, gplane, err, stall);
 }
 
 // The tiles of many plans, one CTA per item: each item names its plan (it.inst)
 // in the per-plan tables of this step's parity.
-template <bool ADE, int NPOLES, class T, class L, bool CP>
+template <bool ADE, int NPOLES, class T, class L, int CPF>
 __global__ void __launch_bounds__(L::NTH, 2) tile_kernel_batch(const DevPlan *plans, const BulkMaps *maps,
                                                                const BulkItem *items, int ncls_layout, int *err)
 {
@@ -583,7 +592,7 @@ __global__ void __launch_bounds__(L::NTH, 2) tile_kernel_batch(const DevPlan *pl
     bulk_init_bars(m);
     __syncthreads();
     uint32_t gplane = 0;
-    bulk_item<ADE, NPOLES, T, L, CP>(P, maps[it.inst], it, m, gplane, err, 0);
+    bulk_item<ADE, NPOLES, T, L, CPF>(P, maps[it.inst], it, m, gplane, err, 0);
 }
 
 // Many plans in one persistent launch (bulk layout): CTA b takes items b,
@@ -607,7 +616,7 @@ __global__ void __launch_bounds__(LBulk::NTH, 2) bulk_kernel_batch(const DevPlan
             cur = it.inst;
         }
         __syncthreads();
-        if (!bulk_item<ADE, NPOLES, T, LBulk, false>(P, maps[it.inst], it, m, gplane, err, 0)) return;
+        if (!bulk_item<ADE, NPOLES, T, LBulk, 0>(P, maps[it.inst], it, m, gplane, err, 0)) return;
     }
 }
 
@@ -623,27 +632,28 @@ size_t smem_bytes_l(int nclasses, int storage)
     return storage == FDTD_STORE_F32 ? smem_bytes_t<float, L>(nclasses) : smem_bytes_t<__half, L>(nclasses);
 }
 
-template <class T, class L, bool CP>
+template <class T, class L, int CPF>
 cudaError_t configure_tl()
 {
     const int smem = (int)smem_bytes_t<T, L>(256);
     const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(tile_kernel<false, 0, T, L, CP>, A, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(tile_kernel<true, 0, T, L, CP>, A, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(tile_kernel<true, 2, T, L, CP>, A, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(tile_kernel_batch<false, 0, T, L, CP>, A, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(tile_kernel_batch<true, 0, T, L, CP>, A, smem)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(tile_kernel_batch<true, 2, T, L, CP>, A, smem);
+    if ((e = cudaFuncSetAttribute(tile_kernel<false, 0, T, L, CPF>, A, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(tile_kernel<true, 0, T, L, CPF>, A, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(tile_kernel<true, 2, T, L, CPF>, A, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(tile_kernel_batch<false, 0, T, L, CPF>, A, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(tile_kernel_batch<true, 0, T, L, CPF>, A, smem)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(tile_kernel_batch<true, 2, T, L, CPF>, A, smem);
 }
 
 template <class T>
 cudaError_t configure_t()
 {
     cudaError_t e;
-    if ((e = configure_tl<T, LBulk, false>()) != cudaSuccess) return e;
-    if ((e = configure_tl<T, LXY, true>()) != cudaSuccess) return e;
-    if ((e = configure_tl<T, LZ, true>()) != cudaSuccess) return e;
+    if ((e = configure_tl<T, LBulk, 0>()) != cudaSuccess) return e;
+    if ((e = configure_tl<T, LXY, CPF_X | CPF_Y | CPF_Z>()) != cudaSuccess) return e;
+    if ((e = configure_tl<T, LXY, CPF_Y | CPF_Z>()) != cudaSuccess) return e;
+    if ((e = configure_tl<T, LZ, CPF_Z>()) != cudaSuccess) return e;
     const int smem = (int)smem_bytes_t<T, LBulk>(256);
     const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if ((e = cudaFuncSetAttribute(bulk_kernel_batch<false, 0, T>, A, smem)) != cudaSuccess) return e;
@@ -651,48 +661,50 @@ cudaError_t configure_t()
     return cudaFuncSetAttribute(bulk_kernel_batch<true, 2, T>, A, smem);
 }
 
-template <class T, class L, bool CP>
+template <class T, class L, int CPF>
 void launch_tl(const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade, int npoles,
                int stall, cudaStream_t st)
 {
     const size_t smem = smem_bytes_t<T, L>(p.nclasses);
     if (!ade)
-        tile_kernel<false, 0, T, L, CP><<<nitems, L::NTH, smem, st>>>(p, m, items, err, stall);
+        tile_kernel<false, 0, T, L, CPF><<<nitems, L::NTH, smem, st>>>(p, m, items, err, stall);
     else if (npoles == 0)
-        tile_kernel<true, 0, T, L, CP><<<nitems, L::NTH, smem, st>>>(p, m, items, err, stall);
+        tile_kernel<true, 0, T, L, CPF><<<nitems, L::NTH, smem, st>>>(p, m, items, err, stall);
     else
-        tile_kernel<true, 2, T, L, CP><<<nitems, L::NTH, smem, st>>>(p, m, items, err, stall);
+        tile_kernel<true, 2, T, L, CPF><<<nitems, L::NTH, smem, st>>>(p, m, items, err, stall);
 }
 
 template <class T>
 void launch_t(int kind, const DevPlan &p, const BulkMaps &m, const BulkItem *items, int nitems, int *err, bool ade,
               int npoles, int stall, cudaStream_t st)
 {
-    if (kind == TILE_CPXY) launch_tl<T, LXY, true>(p, m, items, nitems, err, ade, npoles, stall, st);
-    else if (kind == TILE_CPZ) launch_tl<T, LZ, true>(p, m, items, nitems, err, ade, npoles, stall, st);
-    else launch_tl<T, LBulk, false>(p, m, items, nitems, err, ade, npoles, stall, st);
+    if (kind == TILE_CPX) launch_tl<T, LXY, CPF_X | CPF_Y | CPF_Z>(p, m, items, nitems, err, ade, npoles, stall, st);
+    else if (kind == TILE_CPY) launch_tl<T, LXY, CPF_Y | CPF_Z>(p, m, items, nitems, err, ade, npoles, stall, st);
+    else if (kind == TILE_CPZ) launch_tl<T, LZ, CPF_Z>(p, m, items, nitems, err, ade, npoles, stall, st);
+    else launch_tl<T, LBulk, 0>(p, m, items, nitems, err, ade, npoles, stall, st);
 }
 
-template <class T, class L, bool CP>
+template <class T, class L, int CPF>
 void launch_tlb(const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems, int ncls_layout, int *err,
                 bool ade, int npoles, cudaStream_t st)
 {
     const size_t smem = smem_bytes_t<T, L>(ncls_layout);
     if (!ade)
-        tile_kernel_batch<false, 0, T, L, CP><<<nitems, L::NTH, smem, st>>>(plans, maps, items, ncls_layout, err);
+        tile_kernel_batch<false, 0, T, L, CPF><<<nitems, L::NTH, smem, st>>>(plans, maps, items, ncls_layout, err);
     else if (npoles == 0)
-        tile_kernel_batch<true, 0, T, L, CP><<<nitems, L::NTH, smem, st>>>(plans, maps, items, ncls_layout, err);
+        tile_kernel_batch<true, 0, T, L, CPF><<<nitems, L::NTH, smem, st>>>(plans, maps, items, ncls_layout, err);
     else
-        tile_kernel_batch<true, 2, T, L, CP><<<nitems, L::NTH, smem, st>>>(plans, maps, items, ncls_layout, err);
+        tile_kernel_batch<true, 2, T, L, CPF><<<nitems, L::NTH, smem, st>>>(plans, maps, items, ncls_layout, err);
 }
 
 template <class T>
 void launch_tb(int kind, const DevPlan *plans, const BulkMaps *maps, const BulkItem *items, int nitems, int ncls_layout,
                int *err, bool ade, int npoles, cudaStream_t st)
 {
-    if (kind == TILE_CPXY) launch_tlb<T, LXY, true>(plans, maps, items, nitems, ncls_layout, err, ade, npoles, st);
-    else if (kind == TILE_CPZ) launch_tlb<T, LZ, true>(plans, maps, items, nitems, ncls_layout, err, ade, npoles, st);
-    else launch_tlb<T, LBulk, false>(plans, maps, items, nitems, ncls_layout, err, ade, npoles, st);
+    if (kind == TILE_CPX) launch_tlb<T, LXY, CPF_X | CPF_Y | CPF_Z>(plans, maps, items, nitems, ncls_layout, err, ade, npoles, st);
+    else if (kind == TILE_CPY) launch_tlb<T, LXY, CPF_Y | CPF_Z>(plans, maps, items, nitems, ncls_layout, err, ade, npoles, st);
+    else if (kind == TILE_CPZ) launch_tlb<T, LZ, CPF_Z>(plans, maps, items, nitems, ncls_layout, err, ade, npoles, st);
+    else launch_tlb<T, LBulk, 0>(plans, maps, items, nitems, ncls_layout, err, ade, npoles, st);
 }
 
 template <class T>
@@ -721,7 +733,7 @@ void box_shape(int storage, cuuint32_t *bwe, cuuint32_t *bwh, cuuint32_t *bwc, c
 
 size_t tile_smem_bytes(int kind, int nclasses, int storage)
 {
-    if (kind == TILE_CPXY) return smem_bytes_l<LXY>(nclasses, storage);
+    if (kind == TILE_CPX || kind == TILE_CPY) return smem_bytes_l<LXY>(nclasses, storage);
     if (kind == TILE_CPZ) return smem_bytes_l<LZ>(nclasses, storage);
     return smem_bytes_l<LBulk>(nclasses, storage);
 }
@@ -789,7 +801,7 @@ int tile_make_maps(int kind, void *encode_fn, const DevPlan &p, float *const f[6
                                       : storage == FDTD_STORE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     cuuint32_t bwe, bwh, bwc, rows_e, rows_h;
-    if (kind == TILE_CPXY) box_shape<LXY>(storage, &bwe, &bwh, &bwc, &rows_e, &rows_h);
+    if (kind == TILE_CPX || kind == TILE_CPY) box_shape<LXY>(storage, &bwe, &bwh, &bwc, &rows_e, &rows_h);
     else if (kind == TILE_CPZ) box_shape<LZ>(storage, &bwe, &bwh, &bwc, &rows_e, &rows_h);
     else box_shape<LBulk>(storage, &bwe, &bwh, &bwc, &rows_e, &rows_h);
     const cuuint64_t strides[2] = {(cuuint64_t)p.zr * es, (cuuint64_t)p.zr * es * (cuuint64_t)p.yr};

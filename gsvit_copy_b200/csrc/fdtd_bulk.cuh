@@ -25,11 +25,13 @@ struct BulkItem {
 // Tile layouts: own rows (TJ) and own k cells (TK) of one CTA of 256 threads.
 //  bulk  15 x 60: the interior box, where every cell takes the plain update
 //        (no CPML, kappa 1, no edge rule);
-//  cpxy  15 x 60: the x slabs (whole planes) and the y slabs;
-//  cpz   31 x 28: the z slabs between the y slabs.
-// The CPML tiles run the plain update on their plain 4-cell groups and the
-// special path of fdtd_cpgroup.cuh (psi, kappa, zeroed planes, ADE-in-CPML,
-// edges) on the rest.  k0 and khi are multiples of 4 in every layout.
+//  cpxy  15 x 60: the x slabs (whole planes; kind TILE_CPX) and the y slabs
+//        (kind TILE_CPY);
+//  cpz   31 x 28: the z slabs between the y slabs (TILE_CPZ).
+// The CPML tiles run the special path of fdtd_cpgroup.cuh (psi, kappa, zeroed
+// planes, ADE-in-CPML, edges) on every group; each kind's kernel carries the
+// code of the faces its tiles can meet only.  k0, klo and khi are multiples
+// of 4 in every layout.
 #define BULK_TJ 15
 #define BULK_TK 60
 #define CPXY_TJ 15
@@ -37,7 +39,9 @@ struct BulkItem {
 #define CPZ_TJ 31
 #define CPZ_TK 28
 
-enum { TILE_BULK = 0, TILE_CPXY = 1, TILE_CPZ = 2 };
+enum { TILE_BULK = 0, TILE_CPX = 1, TILE_CPY = 2, TILE_CPZ = 3, NTILE = 4 };
+// faces a CPML tile kind can meet (its kernel carries only their code)
+enum { CPF_X = 1, CPF_Y = 2, CPF_Z = 4 };
 
 size_t tile_smem_bytes(int kind, int nclasses, int storage);
 cudaError_t bulk_configure();

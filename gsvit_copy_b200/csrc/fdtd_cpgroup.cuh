@@ -26,6 +26,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "fdtd_bulk.cuh"
 #include "fdtd_cells.cuh"
 #include "fdtd_device.cuh"
 
@@ -91,7 +92,7 @@ __device__ __forceinline__ void cp_prefetch_psi(const DevPlan &P, int i, int j, 
 // H^{n+1/2} of a special group: h_update (special = true) then h_special,
 // for the four cells.  d*: the forward E differences of the cells; h: H^n
 // (FP32, unscaled) in, H^{n+1/2} out.  `owner` groups write psi_H.
-template <class T>
+template <int CPF, class T>
 __device__ __forceinline__ void cp_h_group(const DevPlan &P, const float4 *scls, uint32_t cw, int i, int j, int kq, bool owner,
                                            bool tsf, const float (&dey_i)[4], const float (&dez_i)[4],
                                            const float (&dex_j)[4], const float (&dez_j)[4], const float (&dex_k)[4],
@@ -214,11 +215,17 @@ __device__ __forceinline__ void cp_h_group(const DevPlan &P, const float4 *scls,
             azn = azn || an;
         }
     }
-    if (P.cp_on[X0] && i < P.cp_d[X0] - 1 && jin) xface(X0, i);
-    else if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1 && i < xr - 1 && jin) xface(XN, i - (xr - P.cp_d[XN]));
-    if (P.cp_on[Y0] && j < P.cp_d[Y0] - 1 && iin) yface(Y0, j);
-    else if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1 && j < yr - 1 && iin) yface(YN, j - (yr - P.cp_d[YN]));
-    if (az0 || azn) zface(az0 ? Z0 : ZN, az0 ? 0 : zr - P.cp_d[ZN], mz);
+    if constexpr ((CPF & CPF_X) != 0) {
+        if (P.cp_on[X0] && i < P.cp_d[X0] - 1 && jin) xface(X0, i);
+        else if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1 && i < xr - 1 && jin) xface(XN, i - (xr - P.cp_d[XN]));
+    }
+    if constexpr ((CPF & CPF_Y) != 0) {
+        if (P.cp_on[Y0] && j < P.cp_d[Y0] - 1 && iin) yface(Y0, j);
+        else if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1 && j < yr - 1 && iin) yface(YN, j - (yr - P.cp_d[YN]));
+    }
+    if constexpr ((CPF & CPF_Z) != 0) {
+        if (az0 || azn) zface(az0 ? Z0 : ZN, az0 ? 0 : zr - P.cp_d[ZN], mz);
+    }
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const bool kl = kq + c == zr - 1;
@@ -233,7 +240,7 @@ __device__ __forceinline__ void cp_h_group(const DevPlan &P, const float4 *scls,
 // the new E in ne (before the store).  adem, aq, aep: the components owned by
 // the ADE in some cell of the group and their Q and E^{n-1}, which the caller
 // requested before the H phase (the loads then overlap it).
-template <bool ADE, int NPOLES, class T>
+template <int CPF, bool ADE, int NPOLES, class T>
 __device__ __forceinline__ void cp_e_group(const DevPlan &P, const float4 *scls, const DevAde *sade, uint32_t cw, int i, int j,
                                            int kq, int64_t c0i, bool tsf, const float (&ex)[4], const float (&ey)[4],
                                            const float (&ez)[4], const float (&hx)[4], const float (&hy)[4],
@@ -442,11 +449,17 @@ __device__ __forceinline__ void cp_e_group(const DevPlan &P, const float4 *scls,
             azn = azn || an;
         }
     }
-    if (P.cp_on[X0] && i >= 1 && i < P.cp_d[X0]) xface(X0, i, i > 1);
-    else if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1) xface(XN, i - (xr - P.cp_d[XN]), true);
-    if (P.cp_on[Y0] && j >= 1 && j < P.cp_d[Y0]) yface(Y0, j, j > 1);
-    else if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1) yface(YN, j - (yr - P.cp_d[YN]), true);
-    if (az0 || azn) zface(az0 ? Z0 : ZN, az0 ? 0 : zr - P.cp_d[ZN], iz);
+    if constexpr ((CPF & CPF_X) != 0) {
+        if (P.cp_on[X0] && i >= 1 && i < P.cp_d[X0]) xface(X0, i, i > 1);
+        else if (P.cp_on[XN] && i >= xr - P.cp_d[XN] + 1) xface(XN, i - (xr - P.cp_d[XN]), true);
+    }
+    if constexpr ((CPF & CPF_Y) != 0) {
+        if (P.cp_on[Y0] && j >= 1 && j < P.cp_d[Y0]) yface(Y0, j, j > 1);
+        else if (P.cp_on[YN] && j >= yr - P.cp_d[YN] + 1) yface(YN, j - (yr - P.cp_d[YN]), true);
+    }
+    if constexpr ((CPF & CPF_Z) != 0) {
+        if (az0 || azn) zface(az0 ? Z0 : ZN, az0 ? 0 : zr - P.cp_d[ZN], iz);
+    }
     // polarisation recursions of the owned components, their PEC rule
     if (ADE && adem) {
 #pragma unroll

@@ -503,7 +503,12 @@ __global__ void nfff_accumulate_batch(const DevNfff *N)
 // shared memory with their accumulators for NF frequencies (read once per
 // CTA instead of once per point).  exp(-i omega R dt) comes from a table over
 // R; exp(+i omega istart dt), the face area and the sum over groups are
-// applied by farfield_reduce_kernel.  FP64 throughout.
+// applied by farfield_reduce_kernel.  FP64 throughout.  The pair geometry
+// takes one reciprocal (1/rc) and the retarded index its exact division;
+// the other factors are products with constants.  A thread owns a far point
+// so that each staged surface cell serves the CTA's 128 points (the pair
+// loop is FP64-arithmetic bound; a warp per point would stage every cell 16
+// times as often).
 template <int NF>
 __global__ void __launch_bounds__(128) farfield_partial_kernel(const DevFarfield F, int f0)
 {
@@ -516,6 +521,7 @@ __global__ void __launch_bounds__(128) farfield_partial_kernel(const DevFarfield
     const int s0 = blockIdx.y * per, s1 = min(F.ns, s0 + per);
     const double C0 = 299792458.0, PI = 3.14159265358979323846;
     const double dt = F.dt, dx = F.dx, c0dt = C0 * dt;
+    const double idx = 1.0 / dx, k4 = 1.0 / (4.0 * PI), kc = 1.0 / (4.0 * PI * C0 * 2.0 * dt);
     double x = 0, y = 0, z = 0;
     if (live) { x = F.points[3 * p]; y = F.points[3 * p + 1]; z = F.points[3 * p + 2]; }
     double cw[NF], sw[NF], c2[NF], s2[NF];
@@ -552,13 +558,16 @@ __global__ void __launch_bounds__(128) farfield_partial_kernel(const DevFarfield
             case 4: dot = -rz; break;
             default: dot = rz; break;
             }
-            const double ct = dot / rc;
+            // one reciprocal for the geometry; the retarded index keeps the
+            // reference's division (it must round as there)
+            const double irc = 1.0 / rc;
+            const double ct = dot * irc;
             const double r = rc * dx;
             const int R = min((int)(1.0 + r / c0dt), F.ntw - 1);
-            const double ir = 1.0 / r;
-            const double a = ir / (4.0 * PI);
-            const double b = -ct / (4.0 * PI) * ir * ir;
-            const double cp = -ct / (4.0 * PI * C0) * ir / (2.0 * dt);
+            const double ir = irc * idx;
+            const double a = ir * k4;
+            const double b = -ct * k4 * ir * ir;
+            const double cp = -ct * kc * ir;
             const double sg = (g.w & 1) ? 1.0 : -1.0;
             for (int f = 0; f < NF; f++) {
                 const double2 w = F.tw[(size_t)(f0 + f) * F.ntw + R];

@@ -459,18 +459,47 @@ def batch_scenes(n: int = 48, nsteps: int = 2000, seed: int = 7, sizes_xy=(64, 9
     x, y drawn from {64, 96, 128, 192} and z from {64, 96, 128}; rms height
     5-20 nm, correlation length 30-100 nm, Drude silver or a single-pole
     Lorentz substrate, incidence 0-60 deg, 8-cell CPML, dx = 5 nm."""
-    rng = np.random.default_rng(seed)
     out = []
-    for q in range(n):
-        xr, yr = int(rng.choice(sizes_xy)), int(rng.choice(sizes_xy))
-        zr = int(rng.choice(sizes_z))
-        s = rough_surface_scene(res=xr, yres=yr, zres=zr, nsteps=nsteps, cpml_depth=8, seed=int(rng.integers(1 << 30)),
-                                rms=float(rng.uniform(5e-9, 20e-9)), corr_len=float(rng.uniform(30e-9, 100e-9)),
-                                theta_deg=180.0 - float(rng.uniform(0.0, 60.0)), tsf_margin=6,
-                                material="drude" if rng.random() < 0.5 else "lorentz", nfff_angles=nfff_angles)
+    for q, p in enumerate(batch_params(n, seed, sizes_xy, sizes_z)):
+        xr, yr, zr = p["shape"]
+        s = rough_surface_scene(res=xr, yres=yr, zres=zr, nsteps=nsteps, cpml_depth=8, seed=p["seed"], rms=p["rms"],
+                                corr_len=p["corr_len"], theta_deg=p["theta_deg"], tsf_margin=6, material=p["material"],
+                                nfff_angles=nfff_angles)
         s.name = f"batch{q}_{xr}x{yr}x{zr}"
         out.append(s)
     return out
+
+
+def batch_params(n: int = 48, seed: int = 7, sizes_xy=(64, 96, 128, 192), sizes_z=(64, 96, 128)) -> List[dict]:
+    """The seeded draws of batch_scenes (shape, surface seed, rms, correlation
+    length, incidence, material) without building the scenes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        xr, yr = int(rng.choice(sizes_xy)), int(rng.choice(sizes_xy))
+        zr = int(rng.choice(sizes_z))
+        out.append(dict(shape=(xr, yr, zr), seed=int(rng.integers(1 << 30)), rms=float(rng.uniform(5e-9, 20e-9)),
+                        corr_len=float(rng.uniform(30e-9, 100e-9)), theta_deg=180.0 - float(rng.uniform(0.0, 60.0)),
+                        material="drude" if rng.random() < 0.5 else "lorentz"))
+    return out
+
+
+def shard_instances(cells: Sequence[int], world: int) -> List[List[int]]:
+    """Whole instances per rank for a batched run on `world` GPUs (instances
+    are independent: no exchange).  Longest processing time first: instances
+    by descending cell count (ties by index), each to the rank with the fewest
+    cells so far (ties to the lower rank); every rank lists its instances in
+    ascending order.  Deterministic, so each rank computes the same split
+    without communicating."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0] * world
+    out: List[List[int]] = [[] for _ in range(world)]
+    for q in sorted(range(len(cells)), key=lambda q: (-int(cells[q]), q)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        out[r].append(q)
+        load[r] += int(cells[q])
+    return [sorted(o) for o in out]
 
 
 def selftest_scene(code: str, res: int, nsteps: int) -> Scene:

@@ -246,6 +246,13 @@ class Batch:
     def sync(self):
         abi.check(self.lib.fdtd_batch_sync(self.h), "fdtd_batch_sync")
 
+    def stream_handle(self) -> int:
+        """The batch's CUDA stream (cudaStream_t as an integer), e.g. for
+        torch.cuda.ExternalStream and events around its steps."""
+        p = C.c_void_p()
+        abi.check(self.lib.fdtd_batch_get_stream(self.h, C.byref(p)), "fdtd_batch_get_stream")
+        return p.value or 0
+
     def tune(self, trial_steps: int = 4):
         """Autotune the work list; returns [(planes per item (0 = whole), persistent, ms/step), ...]."""
         rep = (C.c_double * 60)()

@@ -369,6 +369,9 @@ int fdtd_batch_tune(fdtd_batch *batch, int trial_steps, double *report, int repo
 /* The bulk work list in use: planes per item (0 = whole), persistent launch,
  * grid size and number of items. */
 int fdtd_batch_config(const fdtd_batch *batch, int *planes_per_item, int *persistent, int *grid, int *items);
+/* The CUDA stream (cudaStream_t) every launch of the batch goes to, so that a
+ * caller can record events around its steps or order work after them. */
+int fdtd_batch_get_stream(const fdtd_batch *batch, void **stream);
 
 /* ---- checkpoint (forward snapshots) ---------------------------------------- */
 

@@ -29,7 +29,10 @@ def small_design_scene(nsteps=NSTEPS, seed=5, metal_cells=0):
                               pulse_delay=2e-15, pulse_width=0.7e-15, seed=seed, metal_cells=metal_cells)
 
 
-def test_design_forward_vs_oracle():
+@pytest.mark.parametrize("tiles", ["0", "1"])
+def test_design_forward_vs_oracle(tiles, monkeypatch):
+    """tiles = 1: the design cells take the bulk tile layout's per-cell path."""
+    monkeypatch.setenv("GSVIT_B200_TILES", tiles)
     s = small_design_scene(nsteps=250)
     obj = plan.cone_objective(s, nth=5, nph=7)
     g, o = Solver(s), CpuSolver(s.expanded())

@@ -18,6 +18,12 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-5
 
 
+@pytest.fixture(autouse=True)
+def _tiles_on(monkeypatch):
+    """These CPML depths (6-12) take the slab kernels by default; force the tiles."""
+    monkeypatch.setenv("GSVIT_B200_TILES", "1")
+
+
 def tiled_scene(kind, shape, depth, nsteps):
     s = plan.small_scene(kind, shape=shape, nsteps=nsteps)
     xr, yr, zr = shape
@@ -61,14 +67,14 @@ def test_tiles_tsf_driven_farfield(kind, shape, depth):
 def test_tiles_use_three_layouts_and_match_slab_path(monkeypatch):
     """The same run through the tiles and through the slab kernels (the path of
     plans without tiles, selected by GSVIT_B200_NO_BULK) agree to FP32
-    rounding; the tiled step launches the bulk and both CPML layouts."""
+    rounding; the tiled step launches the bulk and the three CPML kinds."""
     s = tiled_scene("full", (40, 52, 72), 8, 40)
     init = random_fields((s.xres, s.yres, s.zres), 4)
     g = Solver(s)
     g.set_fields(init)
     prof = g.step_profile(1)
-    # aux grid, TSF faces, three tile layouts, NFFF running DFT
-    assert int(prof["launches_per_step"]) == 6, prof
+    # aux grid, TSF faces, four tile kinds (bulk; CPML x, y and z slabs), NFFF running DFT
+    assert int(prof["launches_per_step"]) == 7, prof
     g.step(29)
     monkeypatch.setenv("GSVIT_B200_NO_BULK", "1")
     h = Solver(s)

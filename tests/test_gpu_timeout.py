@@ -25,6 +25,7 @@ def _code(fn):
 
 
 def test_expired_wait_is_reported_and_plan_is_refused(monkeypatch):
+    monkeypatch.setenv("GSVIT_B200_TILES", "1")   # the stall hook lives in the tile kernels
     s = plan.small_scene("full", nsteps=16)
     init = random_fields((s.xres, s.yres, s.zres), 9)
     ref = Solver(s)                    # created without the stall
