@@ -325,8 +325,11 @@ void push_tiles(std::vector<BulkItem> &v, const std::vector<std::pair<int, int>>
                 int tj, int tk, bool jend = false, bool kend = false)
 {
     if (jlo >= jhi || klo >= khi) return;
-    const int js = jend ? jhi - (jhi - jlo + tj - 1) / tj * tj : jlo;
-    const int ks = kend ? khi - (khi - klo + tk - 1) / tk * tk : klo;
+    // a region starting at the grid's first row (group) needs own rows from
+    // row 1 (k 4) only: the tile starting there owns its halo row 0 (group 0)
+    const int j1 = jlo == 0 ? 1 : jlo, k1 = klo == 0 ? 4 : klo;
+    const int js = jend ? jhi - std::max(1, (jhi - j1 + tj - 1) / tj) * tj : jlo;
+    const int ks = kend ? khi - std::max(1, (khi - k1 + tk - 1) / tk) * tk : klo;
     for (const auto &c : ch)
         for (int j0 = js; j0 < jhi; j0 += tj)
             for (int k0 = ks; k0 < khi; k0 += tk) v.push_back({j0, k0, c.first, c.second, jlo, jhi, klo, khi, 0, 0});
@@ -385,6 +388,15 @@ int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls
     while (lo[2] < hi[2] && !(lo[2] - 4 >= a[2] - (below[2] ? 1 : 0))) lo[2] += 4;
     hi[2] = hi[2] / 4 * 4;
     int bi0 = lo[0], bi1 = hi[0], bj0 = lo[1], bj1 = hi[1], bk0 = lo[2], bk1 = hi[2];
+    // the z slabs in whole z tiles: the first starts at k0 = 4 and owns the
+    // group at k = 0 (28 + 4 cells), the last ends at the grid's edge; the
+    // plain cells they take from the interior box fill lanes that would idle
+    // (only while the box keeps at least one bulk tile's width of k)
+    {
+        const int a0 = bk0 > 0 ? 4 + (bk0 - 4 + CPZ_TK - 1) / CPZ_TK * CPZ_TK : bk0;
+        const int a1 = bk1 < Z ? Z - (Z - bk1 + CPZ_TK - 1) / CPZ_TK * CPZ_TK : bk1;
+        if (a1 - a0 >= BULK_TK) { bk0 = a0; bk1 = a1; }
+    }
     const bool bulk = bi0 < bi1 && bj0 < bj1 && bk0 < bk1;
     // design cells (per-cell E coefficients) are handled by the bulk layout
     // only: a plan whose design cells reach outside the interior box keeps the

@@ -231,8 +231,13 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
 
     // this thread's cells: row j = j0 - 1 + tr, k = kq .. kq + 3
     const int j = j0 - 1 + tr, kq = k0 - 4 + 4 * tg;
-    // groups are whole (klo, khi and k0 are multiples of 4)
-    const bool own = tr >= 1 && tg >= 1 && j >= it.jlo && j < it.jhi && kq >= it.klo && kq < it.khi;
+    // groups are whole (klo, khi and k0 are multiples of 4).  A halo row or
+    // group that is the grid's first (j = 0, k = 0 .. 3) is owned as well:
+    // the E update there reads nothing below it (the backward differences
+    // vanish), so a tile starting at j0 = 1 / k0 = 4 also covers row 0 / the
+    // first group
+    const bool own = (tr >= 1 || j == 0) && (tg >= 1 || kq == 0) && j >= it.jlo && j < it.jhi && kq >= it.klo &&
+                     kq < it.khi;
     const int eb = tr * BWE + off + 4 * tg, hb = tr * BWH + off + 4 * tg, cb = tr * BWC + off8 + 4 * tg;
     // CPML tiles: every group inside the grid takes the special path (on a
     // plain cell it computes the plain update: kappa 1, no psi, no edge rule)
@@ -405,7 +410,8 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
         // ---- E phase on own cells
         const float hyk0 = __shfl_up_sync(0xffffffffu, hy[3], 1), hxk0 = __shfl_up_sync(0xffffffffu, hx[3], 1);
         if (act) {
-            const int xb = ((int)(i & 1) * 2 * TROWS + tr - 1) * TGRP + tg;
+            // the H row below (a halo row owned at j = 0 reads its own: unused, j - 1 is outside the grid)
+            const int xb = ((int)(i & 1) * 2 * TROWS + (tr > 0 ? tr - 1 : 0)) * TGRP + tg;
             const float4 hxj4 = xch[xb], hzj4 = xch[xb + NTH];
             const float hxj[4] = {hxj4.x, hxj4.y, hxj4.z, hxj4.w}, hzj[4] = {hzj4.x, hzj4.y, hzj4.z, hzj4.w};
             const float *eo[3] = {ex, ey, ez};

@@ -6,8 +6,9 @@ of two; every update computes in FP32.  BF16 stores round stochastically
 Tolerances (relative L2 against the FP64 oracle, 40 steps from a seeded
 white-noise state, the worst case for rounding): FP16 5e-3, BF16 4e-2.
 Far field of the rough-surface workload at 128^3 from rest (the physical
-pulse, 4000 steps): FP16 within 1e-3 of the FP32 run, which itself is within 1e-5 of
-the FP64 path; BF16 within 1e-2."""
+pulse, 4000 steps, the 91 x 181 far grid) against an FP64 run of the same
+scene: FP32 within 1e-5, FP16 within the 1e-3 storage target; BF16 misses
+that target (expected failure, reason in the test)."""
 import numpy as np
 import pytest
 
@@ -19,7 +20,6 @@ from tests._util import rel_l2, random_fields
 pytestmark = pytest.mark.gpu
 
 FIELD_TOL = {abi.STORE_F16: 5e-3, abi.STORE_BF16: 4e-2}
-FAR_TOL = {abi.STORE_F16: 1e-3, abi.STORE_BF16: 1e-2}
 STORES = [pytest.param(abi.STORE_F16, id="f16"), pytest.param(abi.STORE_BF16, id="bf16")]
 # k rows of 64 cells are 128 bytes at 16 bits: the TMA tiles run, and the
 # interior box is large enough for the bulk layout
@@ -66,23 +66,43 @@ def test_set_get_round_trip_is_exact_for_representable_values(storage):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("storage", STORES)
-def test_far_field_rough_surface_128(storage):
-    """Rough Drude-silver surface at 128^3 lit from rest by the TSF pulse
-    (peak at step 2392), 4000 steps: the far-field spectrum of the 16-bit
-    run against FP32."""
-    spec = {}
-    for st in (abi.STORE_F32, storage):
-        s = plan.rough_surface_scene(res=128, nsteps=4000, nfff_angles=(10, 19))
-        s.storage = st
-        g = Solver(s)
-        g.step_graph(4000)
-        spec[st] = g.nfff_spectrum()
-        g.close()
-    err = rel_l2(spec[storage], spec[abi.STORE_F32])
-    print("far-field error", storage, "%.3e" % err, "peak", np.abs(spec[abi.STORE_F32]).max())
-    assert np.abs(spec[abi.STORE_F32]).max() > 0
-    assert err < FAR_TOL[storage], err
+@pytest.fixture(scope="module")
+def f64_rough_128():
+    """The rough Drude-silver surface at 128^3 (the 512^3 workload's recipe:
+    16-cell CPML, TSF 30 deg, 91 x 181 far grid) lit from rest by the TSF
+    pulse (peak at step 2392), 4000 steps, in FP64 storage and arithmetic."""
+    s = plan.rough_surface_scene(res=128, nsteps=4000)
+    s.storage = abi.STORE_F64
+    g = Solver(s)
+    g.step_graph(4000)
+    out = {"spec": g.nfff_spectrum(), "probes": g.probes(), "E": g.fields(abi.E_ALL)[:3]}
+    g.close()
+    return out
+
+
+BF16_FAR = ("BF16 misses the 1e-3 far-field target: 1.4e-3 against the FP64 run at 512^3 (8 significant "
+            "bits with stochastic rounding)")
+
+
+@pytest.mark.parametrize("storage", [pytest.param(abi.STORE_F32, id="f32"), pytest.param(abi.STORE_F16, id="f16"),
+                                     pytest.param(abi.STORE_BF16, id="bf16",
+                                                  marks=pytest.mark.xfail(reason=BF16_FAR, strict=False))])
+def test_far_field_rough_surface_128_vs_f64(storage, f64_rough_128):
+    """The same run with FP32, FP16 and BF16 storage against the FP64 run:
+    far-field spectrum within 1e-5 (FP32) and 1e-3 (16-bit, the storage
+    target); the probe series and final E are printed."""
+    s = plan.rough_surface_scene(res=128, nsteps=4000)
+    s.storage = storage
+    g = Solver(s)
+    g.step_graph(4000)
+    spec, probes, E = g.nfff_spectrum(), g.probes(), g.fields(abi.E_ALL)[:3]
+    g.close()
+    ref = f64_rough_128
+    err = rel_l2(spec, ref["spec"])
+    print("storage", storage, "far field %.3e" % err, "probes %.3e" % rel_l2(probes, ref["probes"]),
+          "E", ["%.2e" % rel_l2(x, y) for x, y in zip(E, ref["E"])])
+    assert np.abs(ref["spec"]).max() > 0
+    assert err < (1e-5 if storage == abi.STORE_F32 else 1e-3), err
 
 
 @pytest.mark.parametrize("storage", STORES)
