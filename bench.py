@@ -613,6 +613,13 @@ def run_adjoint(a):
     g.sync()
     fwd_s = time.perf_counter() - t0
     J0 = g.objective_value(obj)
+    # the same forward run replayed from CUDA graphs, and its per-kernel split
+    g.restore(init)
+    t0 = time.perf_counter()
+    g.step_graph(n, chunk=50)
+    g.sync()
+    fwd_graph_s = time.perf_counter() - t0
+    prof = g.step_profile(8)
     g.restore(init)
     t0 = time.perf_counter()
     J, grad = g.adjoint_gradient(obj, n, 200)
@@ -662,6 +669,8 @@ def run_adjoint(a):
                                "glass eps_r 2.1, 550 nm TSF normal incidence, J = far-field power in a 10 deg cone "
                                "about theta 20 deg, checkpoints every 200 steps", "cells": s.ncells,
                    "design_cells": int(grad.size), "cone_points": int(len(obj["points"]))},
+        "forward_graph_s": fwd_graph_s, "forward_graph_gcells": s.ncells * n / fwd_graph_s / 1e9,
+        "kernel_ms_per_step": {k: prof[k] / 8 for k in ("bulk_ms", "slab_ms", "aux_ms", "nfff_ms", "total_ms")},
         "adjoint": {"J": J, "J_forward_only": J0, "forward_s": fwd_s, "gradient_s": adj_s, "gradient_over_forward": adj_s / fwd_s,
                     "grad_min": float(grad.min()), "grad_max": float(grad.max()), "fd": fd},
         "timing": "host clock around synchronised device work",

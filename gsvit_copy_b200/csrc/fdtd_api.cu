@@ -114,6 +114,10 @@ struct fdtd_plan {
     BulkMaps tmaps[NTILE][2];
     std::vector<BulkItem> h_tiles[NTILE];   // host copies of the tile lists (batched launches)
     int stall = 0;                        // tests: expire every CTA's first wait after this many polls
+    // the CPML tile kinds run beside the bulk kind: forked from the plan's
+    // stream by an event, joined back before the NFFF step
+    cudaStream_t side[NTILE] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[NTILE] = {};
     double tile_bytes[NTILE] = {};         // algorithmic HBM bytes per launch of each tile kind
     int *d_err = nullptr;                 // set by a bulk CTA whose bounded wait expired
     const int *batch_err = nullptr;       // the batch's error word, for an instance of a batch
@@ -201,9 +205,26 @@ int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
     DevPlan d = plan_for(P, in);
     cudaError_t e;
     if (P->tiles_on) {
-        for (int kind = 0; kind < NTILE; kind++) {
-            const int rc = launch_tile_kind(P, d, in, kind, st);
+        // the four kinds touch disjoint cells and read only the input set:
+        // the CPML kinds on side streams, so that each kind's last partial
+        // wave of CTAs overlaps the others
+        cudaError_t e = cudaEventRecord(P->ev_fork, st);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("tile fork: ") + cudaGetErrorString(e));
+        for (int kind = TILE_CPX; kind < NTILE; kind++) {
+            if (!P->ntiles[kind]) continue;
+            if ((e = cudaStreamWaitEvent(P->side[kind], P->ev_fork, 0)) != cudaSuccess)
+                return fail(FDTD_E_CUDA, std::string("tile fork: ") + cudaGetErrorString(e));
+            const int rc = launch_tile_kind(P, d, in, kind, P->side[kind]);
             if (rc != FDTD_OK) return rc;
+            if ((e = cudaEventRecord(P->ev_join[kind], P->side[kind])) != cudaSuccess)
+                return fail(FDTD_E_CUDA, std::string("tile join: ") + cudaGetErrorString(e));
+        }
+        const int rc = launch_tile_kind(P, d, in, TILE_BULK, st);
+        if (rc != FDTD_OK) return rc;
+        for (int kind = TILE_CPX; kind < NTILE; kind++) {
+            if (!P->ntiles[kind]) continue;
+            if ((e = cudaStreamWaitEvent(st, P->ev_join[kind], 0)) != cudaSuccess)
+                return fail(FDTD_E_CUDA, std::string("tile join: ") + cudaGetErrorString(e));
         }
         return FDTD_OK;
     }
@@ -504,17 +525,23 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
     P->device = device;
     cudaError_t ce = cudaSetDevice(device);
     if (ce != cudaSuccess) { delete P; return fail(FDTD_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce)); }
-    auto bail = [&](cudaError_t e, const char *what) {
+    auto release = [&]() {
+        for (int k = 0; k < NTILE; k++) {
+            if (P->side[k]) cudaStreamDestroy(P->side[k]);
+            if (P->ev_join[k]) cudaEventDestroy(P->ev_join[k]);
+        }
+        if (P->ev_fork) cudaEventDestroy(P->ev_fork);
         P->mem.free_all();
         if (P->own_stream) cudaStreamDestroy(P->own_stream);
         delete P;
+    };
+    auto bail = [&](cudaError_t e, const char *what) {
+        release();
         return fail(e == cudaErrorMemoryAllocation ? FDTD_E_NOMEM : FDTD_E_CUDA,
                     std::string(what) + ": " + cudaGetErrorString(e));
     };
     auto bail_rc = [&](int rc) {   // the error text is already set
-        P->mem.free_all();
-        if (P->own_stream) cudaStreamDestroy(P->own_stream);
-        delete P;
+        release();
         return rc;
     };
 #define CA(x, what) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return bail(e_, what); } while (0)
@@ -1096,6 +1123,13 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             int rc = build_tiles(P, hp, d, cls);
             if (rc != FDTD_OK) return bail_rc(rc);
         }
+        if (P->tiles_on) {   // side streams and events of the concurrent CPML kinds
+            CA(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming), "tile events");
+            for (int k = TILE_CPX; k < NTILE; k++) {
+                CA(cudaStreamCreateWithFlags(&P->side[k], cudaStreamNonBlocking), "tile streams");
+                CA(cudaEventCreateWithFlags(&P->ev_join[k], cudaEventDisableTiming), "tile events");
+            }
+        }
     }
     P->step_bytes = bytes;
     CA(cudaDeviceSynchronize(), "plan set-up");
@@ -1192,6 +1226,11 @@ int fdtd_plan_destroy(fdtd_plan *P)
     if (P->stream) cudaStreamSynchronize(P->stream);
     for (int s = 0; s < 2; s++)
         if (P->graph[s]) cudaGraphExecDestroy(P->graph[s]);
+    for (int k = 0; k < NTILE; k++) {
+        if (P->side[k]) { cudaStreamSynchronize(P->side[k]); cudaStreamDestroy(P->side[k]); }
+        if (P->ev_join[k]) cudaEventDestroy(P->ev_join[k]);
+    }
+    if (P->ev_fork) cudaEventDestroy(P->ev_fork);
     P->mem.free_all();
     if (P->own_stream) cudaStreamDestroy(P->own_stream);
     delete P;
