@@ -228,6 +228,26 @@ int launch_fused(fdtd_plan *P, int in, cudaStream_t st)
         }
         return FDTD_OK;
     }
+    if (P->bulk_on && P->side[TILE_CPX] && P->slabs.hblocks > 0) {
+        // the slab H kernel beside the bulk kernel (disjoint cells, input set
+        // only); the slab E kernels after both: they read H^{n+1/2} the bulk
+        // kernel wrote next to the slabs
+        if ((e = cudaEventRecord(P->ev_fork, st)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(P->side[TILE_CPX], P->ev_fork, 0)) != cudaSuccess)
+            return fail(FDTD_E_CUDA, std::string("slab fork: ") + cudaGetErrorString(e));
+        e = launch_slab_steps(d, P->slabs, P->hp.has_ade, P->hp.maxpoles, P->storage, P->side[TILE_CPX], 1);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
+        if ((e = cudaEventRecord(P->ev_join[TILE_CPX], P->side[TILE_CPX])) != cudaSuccess)
+            return fail(FDTD_E_CUDA, std::string("slab join: ") + cudaGetErrorString(e));
+        e = launch_tiles(TILE_BULK, d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles,
+                         P->storage, 0, st);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("bulk step launch: ") + cudaGetErrorString(e));
+        if ((e = cudaStreamWaitEvent(st, P->ev_join[TILE_CPX], 0)) != cudaSuccess)
+            return fail(FDTD_E_CUDA, std::string("slab join: ") + cudaGetErrorString(e));
+        e = launch_slab_steps(d, P->slabs, P->hp.has_ade, P->hp.maxpoles, P->storage, st, 2);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("slab step launch: ") + cudaGetErrorString(e));
+        return FDTD_OK;
+    }
     if (P->bulk_on) {   // first: the slab E update reads H^{n+1/2} the bulk kernel wrote next to the slabs
         e = launch_tiles(TILE_BULK, d, P->bmaps[in], P->d_bulk, P->nbulk, P->d_err, P->hp.has_ade, P->hp.maxpoles,
                          P->storage, 0, st);
@@ -931,7 +951,9 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
         lo[2] = std::max(4, (lo[2] + 3) / 4 * 4);   // the k halo group k0-4..k0-1 stays in the grid
         hi[2] = hi[2] / 4 * 4;
         const char *nob = getenv("GSVIT_B200_NO_BULK");
-        P->bulk_on = !hp.design && !r64 && ((size_t)Z * esz % 16 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
+        // (design cells take the bulk kernel's per-cell coefficient path; those
+        // outside the box take e_special's)
+        P->bulk_on = !r64 && ((size_t)Z * esz % 16 == 0) && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2] && !(nob && nob[0] == '1');
         std::vector<SlabBox> boxes;
         std::vector<BulkItem> blk;
         long long nblk = 0;
@@ -1107,14 +1129,16 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
                 if (hp.cp[f].enabled) dmin = std::min(dmin, hp.cp[f].depth);
         }
         const bool can_tile = !r64 && roomy && ((size_t)Z * esz % 16 == 0) && !(nob && nob[0] == '1');
-        // Default: tiles for CPML of depth >= 16.  Thinner slabs fill the CPML
-        // tiles poorly (a z slab of depth 8 uses 12 of a z tile's 28 k cells)
-        // and the slab kernels are faster there (the 48-instance batch with
-        // 8-cell CPML: 8.4 Gcell/s tiled against 13.8 on the slab kernels; the
-        // 512^3 rough surface with 16-cell CPML: 3.03 against 3.05 ms).
-        // GSVIT_B200_TILES=1 / 0 at plan creation forces them on / off.
+        // Default: tiles for grids of at least 2^24 cells with CPML of depth
+        // >= 12.  Rough-surface steps, ms, slab kernels / tiles (the CPML kinds
+        // concurrent with the bulk): 512^3 d16 3.11 / 2.74, 384^3 d16 1.56 /
+        // 1.39, 256^3 d16 0.62 / 0.58, 256^3 d12 0.59 / 0.59; smaller grids
+        // and thinner slabs fill the CPML tiles poorly and the slab kernels
+        // win: 256x256x128 d12 0.42 / 0.44, 192^3 d16 0.36 / 0.40, 128^3 d8
+        // 0.16 / 0.21.  GSVIT_B200_TILES=1 / 0 at plan creation forces them
+        // on / off.
         const char *tv = getenv("GSVIT_B200_TILES");
-        const bool want = tv ? tv[0] == '1' : dmin >= 16;
+        const bool want = tv ? tv[0] == '1' : (dmin >= 12 && (double)hp.n >= 16777216.0);
         P->tiles_on = can_tile && want;
         // test hook of the bounded-wait error path: every tile CTA of this plan
         // also waits, at most this many polls, on an mbarrier nothing arrives on
@@ -1123,7 +1147,7 @@ int plan_create_impl(const fdtd_desc *desc, int device, fdtd_plan **out, bool po
             int rc = build_tiles(P, hp, d, cls);
             if (rc != FDTD_OK) return bail_rc(rc);
         }
-        if (P->tiles_on) {   // side streams and events of the concurrent CPML kinds
+        if (P->tiles_on || P->bulk_on) {   // side streams and events of the concurrent CPML kinds / slab H
             CA(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming), "tile events");
             for (int k = TILE_CPX; k < NTILE; k++) {
                 CA(cudaStreamCreateWithFlags(&P->side[k], cudaStreamNonBlocking), "tile streams");
@@ -1791,6 +1815,8 @@ struct fdtd_batch {
     // and tile kind, one CTA per item) or the bulk box and slab kernels (the
     // lists above hold only these instances).
     int ntiled = 0;
+    cudaStream_t side = nullptr;           // the slab H kernels beside the bulk kernels
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     BulkItem *d_titems[3][NTILE] = {};   // [variant group][tile kind]
     int ntitems[3][NTILE] = {};
     BulkMaps *d_tmaps[NTILE][2] = {};    // [tile kind][parity], indexed by instance
@@ -1806,6 +1832,9 @@ void batch_free(fdtd_batch *B)
     for (int s = 0; s < 2; s++)
         if (B->graph[s]) cudaGraphExecDestroy(B->graph[s]);
     for (auto *p : B->plans) fdtd_plan_destroy(p);
+    if (B->side) { cudaStreamSynchronize(B->side); cudaStreamDestroy(B->side); }
+    if (B->ev_fork) cudaEventDestroy(B->ev_fork);
+    if (B->ev_join) cudaEventDestroy(B->ev_join);
     B->mem.free_all();
     if (B->stream) cudaStreamDestroy(B->stream);
     delete B;
@@ -1857,16 +1886,36 @@ int batch_launch_step(fdtd_batch *B, cudaStream_t st)
                                                B->ntitems[g][kind], B->ncls, B->d_err, g > 0, g == 2 ? 2 : 0, B->storage, st);
             if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched tile launch: ") + cudaGetErrorString(e));
         }
-    for (int g = 0; g < 3; g++) {   // the others: bulk box and slab kernels
-        if (!B->nitems[g] && !B->nboxes[g] && !B->neboxes[g]) continue;
-        const bool ade = g > 0;
-        const int npoles = g == 2 ? 2 : 0;
+    // the others: bulk box and slab kernels; the slab H kernels of every
+    // variant on the side stream beside the bulk kernels, the slab E kernels
+    // after both (they read the H the bulk kernels wrote next to the slabs)
+    {
+        cudaError_t e = cudaEventRecord(B->ev_fork, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(B->side, B->ev_fork, 0);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batch fork: ") + cudaGetErrorString(e));
+    }
+    for (int g = 0; g < 3; g++) {
+        if (!B->nboxes[g]) continue;
+        cudaError_t e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], B->d_boxes4[g],
+                                                B->nslab_blocks4[g], B->d_eboxes[g], B->neboxes[g], B->neblocks[g], g > 0,
+                                                g == 2 ? 2 : 0, B->storage, B->side, 1);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
+    }
+    for (int g = 0; g < 3; g++) {
         cudaError_t e = launch_bulk_batch(B->d_plans[in], B->d_maps[in], B->d_items[g], B->nitems[g], B->bulk_grid[g], B->ncls,
-                                          B->d_err, ade, npoles, B->storage, st);
+                                          B->d_err, g > 0, g == 2 ? 2 : 0, B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched bulk launch: ") + cudaGetErrorString(e));
-        e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], B->d_boxes4[g],
-                                    B->nslab_blocks4[g], B->d_eboxes[g], B->neboxes[g], B->neblocks[g], ade, npoles,
-                                    B->storage, st);
+    }
+    {
+        cudaError_t e = cudaEventRecord(B->ev_join, B->side);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, B->ev_join, 0);
+        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batch join: ") + cudaGetErrorString(e));
+    }
+    for (int g = 0; g < 3; g++) {
+        if (!B->nboxes[g]) continue;
+        cudaError_t e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], B->d_boxes4[g],
+                                                B->nslab_blocks4[g], B->d_eboxes[g], B->neboxes[g], B->neblocks[g], g > 0,
+                                                g == 2 ? 2 : 0, B->storage, st, 2);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
     }
     if (B->nepboxes) {   // E of every instance's plain runs (after all H half steps)
@@ -1915,6 +1964,12 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
     if (cudaSetDevice(device) != cudaSuccess) { delete B; return fail(FDTD_E_CUDA, "cudaSetDevice"); }
     cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, device);
     if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess) { delete B; return fail(FDTD_E_CUDA, "stream"); }
+    if (cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&B->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&B->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        batch_free(B);
+        return fail(FDTD_E_CUDA, "batch streams");
+    }
     for (int q = 0; q < nplans; q++) {
         fdtd_plan *P = nullptr;
         const int rc = plan_create_impl(&descs[q], device, &P, false);

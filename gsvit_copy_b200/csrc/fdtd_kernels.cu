@@ -671,16 +671,19 @@ void launch_tsf_faces(const DevPlan &p, int total, cudaStream_t st)
 }
 
 template <class T>
-cudaError_t slab_steps_t(const DevPlan &p, const SlabLists &L, bool ade, int npoles, cudaStream_t st)
+cudaError_t slab_steps_t(const DevPlan &p, const SlabLists &L, bool ade, int npoles, cudaStream_t st, int part)
 {
     bool h4 = false;
-    if constexpr (sizeof(T) <= 4) {   // 4-cell groups: FP32 and 16-bit storage
-        if (L.h4blocks > 0) {
-            slab_h4_kernel<T><<<(unsigned)L.h4blocks, 256, 0, st>>>(p, L.h4, L.nh);
-            h4 = true;
+    if (part & 1) {
+        if constexpr (sizeof(T) <= 4) {   // 4-cell groups: FP32 and 16-bit storage
+            if (L.h4blocks > 0) {
+                slab_h4_kernel<T><<<(unsigned)L.h4blocks, 256, 0, st>>>(p, L.h4, L.nh);
+                h4 = true;
+            }
         }
+        if (!h4) slab_h_kernel<T><<<(unsigned)L.hblocks, 256, 0, st>>>(p, L.h, L.nh);
     }
-    if (!h4) slab_h_kernel<T><<<(unsigned)L.hblocks, 256, 0, st>>>(p, L.h, L.nh);
+    if (!(part & 2)) return cudaGetLastError();
     if (L.eblocks > 0) {
         if (!ade)
             slab_e_kernel<false, 0, T><<<(unsigned)L.eblocks, 256, 0, st>>>(p, L.e, L.ne);
@@ -693,13 +696,14 @@ cudaError_t slab_steps_t(const DevPlan &p, const SlabLists &L, bool ade, int npo
     return cudaGetLastError();
 }
 
-cudaError_t launch_slab_steps(const DevPlan &p, const SlabLists &L, bool ade, int npoles, int storage, cudaStream_t st)
+cudaError_t launch_slab_steps(const DevPlan &p, const SlabLists &L, bool ade, int npoles, int storage, cudaStream_t st,
+                              int part)
 {
     if (L.hblocks <= 0) return cudaSuccess;
-    if (storage == FDTD_STORE_F64) return slab_steps_t<double>(p, L, ade, npoles, st);
-    if (storage == FDTD_STORE_F16) return slab_steps_t<__half>(p, L, ade, npoles, st);
-    if (storage == FDTD_STORE_BF16) return slab_steps_t<__nv_bfloat16>(p, L, ade, npoles, st);
-    return slab_steps_t<float>(p, L, ade, npoles, st);
+    if (storage == FDTD_STORE_F64) return slab_steps_t<double>(p, L, ade, npoles, st, part);
+    if (storage == FDTD_STORE_F16) return slab_steps_t<__half>(p, L, ade, npoles, st, part);
+    if (storage == FDTD_STORE_BF16) return slab_steps_t<__nv_bfloat16>(p, L, ade, npoles, st, part);
+    return slab_steps_t<float>(p, L, ade, npoles, st, part);
 }
 
 void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st)
@@ -715,13 +719,15 @@ void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStr
 template <class T>
 cudaError_t slab_steps_batch_t(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, const SlabBox *boxes4,
                                long long nblocks4, const SlabBox *eboxes, int neboxes, long long neblocks, bool ade,
-                               int npoles, cudaStream_t st)
+                               int npoles, cudaStream_t st, int part)
 {
-    if (nblocks4 > 0)
-        slab_h4_batch<T><<<(unsigned)nblocks4, 256, 0, st>>>(p, boxes4, nboxes);
-    else
-        slab_h_batch<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
-    if (neblocks > 0) {
+    if (part & 1) {
+        if (nblocks4 > 0)
+            slab_h4_batch<T><<<(unsigned)nblocks4, 256, 0, st>>>(p, boxes4, nboxes);
+        else
+            slab_h_batch<T><<<(unsigned)nblocks, 256, 0, st>>>(p, boxes, nboxes);
+    }
+    if ((part & 2) && neblocks > 0) {
         if (!ade)
             slab_e_batch<false, 0, T><<<(unsigned)neblocks, 256, 0, st>>>(p, eboxes, neboxes);
         else if (npoles == 0)
@@ -734,15 +740,17 @@ cudaError_t slab_steps_batch_t(const DevPlan *p, const SlabBox *boxes, int nboxe
 
 cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks,
                                     const SlabBox *boxes4, long long nblocks4, const SlabBox *eboxes, int neboxes,
-                                    long long neblocks, bool ade, int npoles, int storage, cudaStream_t st)
+                                    long long neblocks, bool ade, int npoles, int storage, cudaStream_t st, int part)
 {
     if (nblocks <= 0) return cudaSuccess;
     if (storage == FDTD_STORE_F16)
-        return slab_steps_batch_t<__half>(p, boxes, nboxes, nblocks, boxes4, nblocks4, eboxes, neboxes, neblocks, ade, npoles, st);
+        return slab_steps_batch_t<__half>(p, boxes, nboxes, nblocks, boxes4, nblocks4, eboxes, neboxes, neblocks, ade, npoles, st,
+                                          part);
     if (storage == FDTD_STORE_BF16)
         return slab_steps_batch_t<__nv_bfloat16>(p, boxes, nboxes, nblocks, boxes4, nblocks4, eboxes, neboxes, neblocks, ade,
-                                                 npoles, st);
-    return slab_steps_batch_t<float>(p, boxes, nboxes, nblocks, boxes4, nblocks4, eboxes, neboxes, neblocks, ade, npoles, st);
+                                                 npoles, st, part);
+    return slab_steps_batch_t<float>(p, boxes, nboxes, nblocks, boxes4, nblocks4, eboxes, neboxes, neblocks, ade, npoles, st,
+                                     part);
 }
 
 cudaError_t launch_slab_e_plain_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, int storage,

@@ -62,9 +62,10 @@ void launch_aux_step_batch(const DevAux *a, int nplans, cudaStream_t st);
 void launch_tsf_faces_batch(const DevPlan *p, int nplans, int max_cells, cudaStream_t st);
 // H over boxes (or boxes4 in 4-cell groups, nblocks4 > 0) and E over eboxes,
 // the instances' runs of k planes with a dispersive cell (SlabLists::e)
+// part: 1 the H kernel, 2 the E kernel over the dispersive runs, 3 both
 cudaError_t launch_slab_steps_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks,
                                     const SlabBox *boxes4, long long nblocks4, const SlabBox *eboxes, int neboxes,
-                                    long long neblocks, bool ade, int npoles, int storage, cudaStream_t st);
+                                    long long neblocks, bool ade, int npoles, int storage, cudaStream_t st, int part = 3);
 // E over every instance's runs without a dispersive cell (SlabLists::ep)
 cudaError_t launch_slab_e_plain_batch(const DevPlan *p, const SlabBox *boxes, int nboxes, long long nblocks, int storage,
                                       cudaStream_t st);
@@ -89,7 +90,9 @@ struct SlabLists {
     int nep;
     long long epblocks;
 };
-cudaError_t launch_slab_steps(const DevPlan &p, const SlabLists &L, bool ade, int npoles, int storage, cudaStream_t st);
+// part: 1 the H kernel, 2 the E kernels, 3 both (in that order)
+cudaError_t launch_slab_steps(const DevPlan &p, const SlabLists &L, bool ade, int npoles, int storage, cudaStream_t st,
+                              int part = 3);
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st);
 // folds the samples of the steps since the last multiple of NFFF_RING into the
 // accumulators and clears their ring slots; due before the accumulators are read
