@@ -430,9 +430,13 @@ int build_tiles(fdtd_plan *P, const HostPlan &hp, DevPlan &d, const uint8_t *cls
     hi[2] = hi[2] / 4 * 4;
     int bi0 = lo[0], bi1 = hi[0], bj0 = lo[1], bj1 = hi[1], bk0 = lo[2], bk1 = hi[2];
     // the z slabs in whole z tiles: the first starts at k0 = 4 and owns the
-    // group at k = 0 (28 + 4 cells), the last ends at the grid's edge; the
+    // group at k = 0 (CPZ_TK + 4 cells), the last ends at the grid's edge; the
     // plain cells they take from the interior box fill lanes that would idle
-    // (only while the box keeps at least one bulk tile's width of k)
+    // (only while the box keeps at least one bulk tile's width of k).  At
+    // 512^3 with 16-cell CPML this also keeps the TSF box's z faces (k = 24,
+    // 488) out of the bulk tiles, whose per-cell path they would take in
+    // every column: 34 x 20 z tiles (box from k = 24) ran the z kind in 0.48
+    // instead of 0.64 ms but the bulk kind in 1.67 instead of 1.45 ms.
     {
         const int a0 = bk0 > 0 ? 4 + (bk0 - 4 + CPZ_TK - 1) / CPZ_TK * CPZ_TK : bk0;
         const int a1 = bk1 < Z ? Z - (Z - bk1 + CPZ_TK - 1) / CPZ_TK * CPZ_TK : bk1;
@@ -1815,8 +1819,6 @@ struct fdtd_batch {
     // and tile kind, one CTA per item) or the bulk box and slab kernels (the
     // lists above hold only these instances).
     int ntiled = 0;
-    cudaStream_t side = nullptr;           // the slab H kernels beside the bulk kernels
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     BulkItem *d_titems[3][NTILE] = {};   // [variant group][tile kind]
     int ntitems[3][NTILE] = {};
     BulkMaps *d_tmaps[NTILE][2] = {};    // [tile kind][parity], indexed by instance
@@ -1832,9 +1834,6 @@ void batch_free(fdtd_batch *B)
     for (int s = 0; s < 2; s++)
         if (B->graph[s]) cudaGraphExecDestroy(B->graph[s]);
     for (auto *p : B->plans) fdtd_plan_destroy(p);
-    if (B->side) { cudaStreamSynchronize(B->side); cudaStreamDestroy(B->side); }
-    if (B->ev_fork) cudaEventDestroy(B->ev_fork);
-    if (B->ev_join) cudaEventDestroy(B->ev_join);
     B->mem.free_all();
     if (B->stream) cudaStreamDestroy(B->stream);
     delete B;
@@ -1886,36 +1885,19 @@ int batch_launch_step(fdtd_batch *B, cudaStream_t st)
                                                B->ntitems[g][kind], B->ncls, B->d_err, g > 0, g == 2 ? 2 : 0, B->storage, st);
             if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched tile launch: ") + cudaGetErrorString(e));
         }
-    // the others: bulk box and slab kernels; the slab H kernels of every
-    // variant on the side stream beside the bulk kernels, the slab E kernels
-    // after both (they read the H the bulk kernels wrote next to the slabs)
-    {
-        cudaError_t e = cudaEventRecord(B->ev_fork, st);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(B->side, B->ev_fork, 0);
-        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batch fork: ") + cudaGetErrorString(e));
-    }
+    // the others: bulk box and slab kernels, variant by variant (a side
+    // stream for the slab H kernels, as single plans have, measured slower on
+    // the 48-instance batch: 11.3 against 13.9 Gcell/s)
     for (int g = 0; g < 3; g++) {
-        if (!B->nboxes[g]) continue;
-        cudaError_t e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], B->d_boxes4[g],
-                                                B->nslab_blocks4[g], B->d_eboxes[g], B->neboxes[g], B->neblocks[g], g > 0,
-                                                g == 2 ? 2 : 0, B->storage, B->side, 1);
-        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
-    }
-    for (int g = 0; g < 3; g++) {
+        if (!B->nitems[g] && !B->nboxes[g] && !B->neboxes[g]) continue;
+        const bool ade = g > 0;
+        const int npoles = g == 2 ? 2 : 0;
         cudaError_t e = launch_bulk_batch(B->d_plans[in], B->d_maps[in], B->d_items[g], B->nitems[g], B->bulk_grid[g], B->ncls,
-                                          B->d_err, g > 0, g == 2 ? 2 : 0, B->storage, st);
+                                          B->d_err, ade, npoles, B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched bulk launch: ") + cudaGetErrorString(e));
-    }
-    {
-        cudaError_t e = cudaEventRecord(B->ev_join, B->side);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, B->ev_join, 0);
-        if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batch join: ") + cudaGetErrorString(e));
-    }
-    for (int g = 0; g < 3; g++) {
-        if (!B->nboxes[g]) continue;
-        cudaError_t e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], B->d_boxes4[g],
-                                                B->nslab_blocks4[g], B->d_eboxes[g], B->neboxes[g], B->neblocks[g], g > 0,
-                                                g == 2 ? 2 : 0, B->storage, st, 2);
+        e = launch_slab_steps_batch(B->d_plans[in], B->d_boxes[g], B->nboxes[g], B->nslab_blocks[g], B->d_boxes4[g],
+                                    B->nslab_blocks4[g], B->d_eboxes[g], B->neboxes[g], B->neblocks[g], ade, npoles,
+                                    B->storage, st);
         if (e != cudaSuccess) return fail(FDTD_E_CUDA, std::string("batched slab launch: ") + cudaGetErrorString(e));
     }
     if (B->nepboxes) {   // E of every instance's plain runs (after all H half steps)
@@ -1964,12 +1946,6 @@ int fdtd_batch_create(const fdtd_desc *descs, int nplans, int device, fdtd_batch
     if (cudaSetDevice(device) != cudaSuccess) { delete B; return fail(FDTD_E_CUDA, "cudaSetDevice"); }
     cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, device);
     if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess) { delete B; return fail(FDTD_E_CUDA, "stream"); }
-    if (cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&B->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&B->ev_join, cudaEventDisableTiming) != cudaSuccess) {
-        batch_free(B);
-        return fail(FDTD_E_CUDA, "batch streams");
-    }
     for (int q = 0; q < nplans; q++) {
         fdtd_plan *P = nullptr;
         const int rc = plan_create_impl(&descs[q], device, &P, false);

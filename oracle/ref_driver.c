@@ -234,6 +234,8 @@ ref_state *ref_create(const fdtd_desc *desc, char *err)
     if (desc->tsf.enabled && set->ss.tsf.box_boundary_skipdepth >= 0) {
         int sd = set->ss.tsf.box_boundary_skipdepth, ii, jj, kk;
         d->sourceskip = sv_icube_new(d->xres, d->yres, d->zres, d->xres * d->dx, d->yres * d->dy, d->zres * d->dz, 1);
+        /* cells are independent (pure lookups): split over the host threads */
+#pragma omp parallel for private(j, k, ii, jj, kk) schedule(dynamic, 1)
         for (i = 0; i < d->xres; i++)
             for (j = 0; j < d->yres; j++)
                 for (k = 0; k < d->zres; k++) {
@@ -250,7 +252,8 @@ ref_state *ref_create(const fdtd_desc *desc, char *err)
                     if (hit) d->sourceskip->data[i][j][k] = 1;
                 }
     }
-    /* internal boundaries, plan.c:5387-5416 */
+    /* internal boundaries, plan.c:5387-5416 (cells independent, as above) */
+#pragma omp parallel for private(j, k) schedule(dynamic, 1)
     for (i = 0; i < d->xres; i++)
         for (j = 0; j < d->yres; j++)
             for (k = 0; k < d->zres; k++) {
@@ -420,8 +423,10 @@ int ref_get_step(const ref_state *r) { return r->set->sc.step_act; }
  * Drop-in check (test infrastructure): the same planned SvPool / SvSet, but
  * stepped through the GPU branch of svit.c:204-256 -- sv_pool_allocate_gpus
  * (pool.c:76-81) and the sv_pool_gpu_* family, here provided by
- * gsvit_copy_b200/dropin/gpu_b200.c over libgsvit_b200.  Built only into
- * oracle/_ref/libgsvit_dropin.so, with UCUDA defined for every object.
+ * gsvit_copy_b200/dropin/gpu_b200.c over libgsvit_b200.  Built into
+ * oracle/_ref/libgsvit_dropin.so, with UCUDA defined for every object, and
+ * (GSVIT_REFCUDA) into oracle/_ref/libgsvit_refcuda.so over GSvit's own
+ * src3d/gpu.c and gpu_kernels.cu.
  */
 int dropin_start(ref_state *r)
 {
@@ -443,8 +448,19 @@ int dropin_start(ref_state *r)
     }
     set->plan.gpumode = SV_GPUMODE_FULL;
     set->sc.ugpu[0] = 0;
+#ifdef GSVIT_REFCUDA
+    /* a deck with GPU = 1 and the default device query (settings.c:968-975):
+     * the first device, queried
+     * (sv_gpu_new reads the block size of its far-field kernels from the
+     * device properties, gpu.c:1976-2003) */
+    set->sc.usegpu = 1;
+    set->sc.devicequery = 1;
+#endif
     sv_pool_allocate_gpus(mp, set);
     if (!mp->gpu) return -1;
+#ifdef GSVIT_REFCUDA
+    if (((SvGpu *)mp->gpu)->ngset < 1) return -1;   /* no device found (gpu.c:2022-2040) */
+#endif
     if (sv_pool_gpu_init(mp, set)) return -1;
     return sv_pool_gpu_copyto(mp, set, SV_SYNC_ALL) ? -1 : 0;
 }

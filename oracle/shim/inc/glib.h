@@ -65,6 +65,21 @@ typedef struct _GRand { unsigned long long s; } GRand;
 /* opaque thread-queue types named by gpu.h (compiled with UCUDA for the drop-in build only) */
 typedef struct _GQueue GQueue;
 typedef struct _GMutex GMutex;
+/* the task queue and worker thread of src3d/gpu.c (sv_gpu_new, gpu_main),
+ * for the build of GSvit's own CUDA path; implemented over pthreads in
+ * oracle/shim/gthread.c */
+typedef struct _GThread GThread;
+typedef struct _GError { int code; gchar *message; } GError;
+typedef void *(*GThreadFunc)(void *);
+#define GINT_TO_POINTER(i) ((gpointer)(intptr_t)(i))
+#define GPOINTER_TO_INT(p) ((gint)(intptr_t)(p))
+GQueue *g_queue_new(void);
+void g_queue_push_tail(GQueue *q, gpointer data);
+gpointer g_queue_pop_tail(GQueue *q);
+gpointer g_queue_peek_tail(GQueue *q);
+gboolean g_queue_is_empty(GQueue *q);
+GMutex *g_mutex_new(void);
+GThread *g_thread_create(GThreadFunc func, gpointer data, gboolean joinable, GError **error);
 static inline GRand *g_rand_new(void) { GRand *r = (GRand *)g_malloc(sizeof(GRand)); r->s = 88172645463325252ULL; return r; }
 static inline GRand *g_rand_new_with_seed(guint32 seed) { GRand *r = g_rand_new(); r->s ^= seed; return r; }
 static inline void g_rand_set_seed(GRand *r, guint32 seed) { r->s = 88172645463325252ULL ^ seed; }
