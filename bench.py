@@ -64,6 +64,10 @@ def parse():
     ap.add_argument("--res", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="reference arm: skip the context run of GSvit's own CUDA build")
+    ap.add_argument("--refcuda-steps", type=int, default=5,
+                    help="reference arm: timed steps of GSvit's own CUDA build with its far field")
     ap.add_argument("--no-extensions", action="store_true",
                     help="skip the extensions block (FP16 / BF16 storage and the batched instances)")
     ap.add_argument("--ext-steps", type=int, default=20, help="timed steps of each extensions measurement")
@@ -310,10 +314,46 @@ def cpu_sample_run(steps=None, warmup=1, budget_s=15.0):
     return scene.ncells * steps / dt / 1e9, threads, kind, steps
 
 
+# GSvit's own CUDA path on this GPU (context, not the arm's value): the same
+# scene recipe with the far grid scaled so that the far-field work per cell
+# update is that of the 512^3 case (points proportional to the edge length)
+REFCUDA_RES = 256
+REFCUDA_ANGLES = (64, 129)
+
+
+def reference_cuda_context(a):
+    """Time GSvit's own CUDA build (src3d/gpu.c + gpu_kernels.cu compiled
+    unmodified for sm_100a, oracle/_ref/libgsvit_refcuda.so) through the GPU
+    branch of its loop, in a child process: the whole workload with its
+    time-domain far field, and the field update alone (no NFFF).  Returns a
+    block for the reference arm's line, or {"unavailable": why}."""
+    from oracle import refcuda
+    if not refcuda.available():
+        return {"unavailable": "oracle/_ref/libgsvit_refcuda.so is not built (GSvit's sources absent at build time)"}
+    if a.no_reference_cuda:
+        return {"unavailable": "skipped (--no-reference-cuda)"}
+    out = {"build": "GSvit src3d/gpu.c + src3d/gpu_kernels.cu, unmodified, nvcc -O2 -use_fast_math for sm_100a "
+                    "(configure.ac:57), stepped through sv_pool_gpu_* (svit.c:240-256); FP32",
+           "timing": "host clock around K steps; every reference stage ends in a device synchronisation"}
+    try:
+        full = refcuda.run("rough", REFCUDA_RES, steps=a.refcuda_steps, warmup=1, nfff=True, angles=REFCUDA_ANGLES,
+                           timeout=900)
+        bare = refcuda.run("rough", a.res, steps=2 * a.refcuda_steps, warmup=2, nfff=False, timeout=900)
+    except Exception as e:   # the context block must not take the arm down
+        return {"unavailable": f"reference CUDA run failed: {str(e)[-300:]}"}
+    out["workload"] = {"value": full["gcells"], "unit": UNIT, "ms_per_step": full["ms_per_step"], "steps": full["steps"],
+                       "sample": f"rough Drude-silver surface {REFCUDA_RES}^3, 16-cell CPML, TSF, time-domain NFFF on "
+                                 f"{REFCUDA_ANGLES[0]}x{REFCUDA_ANGLES[1]} far points (far work per cell update as at 512^3)"}
+    out["field_update"] = {"value": bare["gcells"], "unit": UNIT, "ms_per_step": bare["ms_per_step"],
+                           "steps": bare["steps"], "sample": f"rough Drude-silver surface {a.res}^3 without the NFFF"}
+    return out
+
+
 def run_reference(a):
     rank, _, world = dist_env()
     if rank != 0:
         return 0
+    refcuda_block = reference_cuda_context(a)
     value, threads, kind, steps = cpu_sample_run(steps=a.steps, warmup=a.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
@@ -326,6 +366,7 @@ def run_reference(a):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     line["ms_per_step"] = SAMPLE_RES ** 3 / (value * 1e9) * 1e3
+    line["reference_cuda"] = refcuda_block
     print(json.dumps(line), flush=True)
     return 0
 

@@ -52,6 +52,11 @@ def _scene(kind: str, res: int, nsteps: int, nfff: bool, angles):
     from gsvit_copy_b200 import plan
     if kind == "rough":
         return plan.rough_surface_scene(res=res, nsteps=nsteps, nfff_angles=tuple(angles) if nfff else None)
+    if kind == "vacuum":
+        # the small scene's CPML, TSF, NFFF and probes without its materials
+        s = plan.small_scene("lintab", shape=(res, res + 8, res + 24), nsteps=nsteps)
+        s.mat[:] = 0
+        return s
     return plan.small_scene(kind, shape=(res, res + 8, res + 24), nsteps=nsteps)
 
 
