@@ -24,6 +24,11 @@ Arms:
                     farfield.c ... compiled from its sources into
                     oracle/_ref/libgsvit_ref.so) on all host threads, on a
                     bounded sample of the same workload (see SAMPLE below).
+                    The line also carries `reference_cuda`: GSvit's own CUDA
+                    path (gpu.c + gpu_kernels.cu built unmodified for sm_100a,
+                    oracle/_ref/libgsvit_refcuda.so) timed on this GPU, the
+                    whole workload on a 256^3 sample and the field update at
+                    the full size (context, not the arm's value).
 
 Multi-GPU: the time step does not shard here; `--gpus N` under torchrun runs N
 independent replicas (one per rank and GPU), timed as the max over ranks, and
