@@ -261,7 +261,12 @@ int fdtd_set_fields_f32(fdtd_plan *plan, int mask, const float *const comps[6]);
  * svit.c:240-256 (wrap_hKernel ... wrap_cpml_estep, farfield, outpoint). */
 int fdtd_step(fdtd_plan *plan, int nsteps);
 
-/* Same, captured once into a CUDA graph of `chunk` steps and replayed.  */
+/* Same, captured once into a CUDA graph of `chunk` steps and replayed
+ * (chunk rounded down to an even number >= 2; one graph per field-set
+ * parity, kept until a call with another chunk or the plan's destruction;
+ * the steps past the last whole chunk run as fdtd_step).  Bitwise equal to
+ * fdtd_step and the faster of the two for long runs: 2.69 against 2.75 ms
+ * a step on the 512^3 rough surface.  */
 int fdtd_step_graph(fdtd_plan *plan, int nsteps, int chunk);
 
 /* Same as fdtd_step, with its scratch in static device memory.  No
