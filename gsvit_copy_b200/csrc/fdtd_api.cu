@@ -1636,7 +1636,7 @@ int fdtd_step_profile(fdtd_plan *P, int nsteps, double out[8])
         const SlabLists &L = P->slabs;   // slab H, then E over the dispersive and the plain runs
         nyee = (P->bulk_on ? 1 : 0) + (L.hblocks > 0 ? 1 + (L.eblocks > 0 ? 1 : 0) + (L.epblocks > 0 ? 1 : 0) : 0);
     }
-    out[7] = 1 + (P->tsf_cells ? 1 : 0) + nyee + (P->nfff_nfreq > 0 ? 1 : 0) + (P->nfff_series ? 1 : 0);
+    out[7] = 1 + (P->tsf_cells ? 1 : 0) + nyee + (P->nfff_nfreq > 0 ? 2 : 0) + (P->nfff_series ? 1 : 0);
     return FDTD_OK;
 }
 

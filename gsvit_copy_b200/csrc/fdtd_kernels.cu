@@ -480,10 +480,54 @@ __global__ void nfff_fold_pending_kernel(const DevNfff N)
     }
 }
 
-__global__ void nfff_accumulate_kernel(const DevNfff N)
+// A single plan's NFFF step in two launches: the sampling, which every step
+// does, in a light kernel (few registers, full occupancy: its nine gathered
+// loads a cell want many in flight), and the fold, which only the step that
+// fills the ring does, in a kernel that every other step leaves at once.
+// Both launch every step, so a captured graph is right at any step offset.
+template <class S>
+__device__ __forceinline__ void nfff_sample_cell(const DevNfff &N, int s)
 {
-    if (N.storage == FDTD_STORE_F64) nfff_accumulate_cell<double>(N, blockIdx.x * blockDim.x + threadIdx.x);
-    else nfff_accumulate_cell<float>(N, blockIdx.x * blockDim.x + threadIdx.x);
+    if (N.ns <= 0 || N.nfreq <= 0 || s >= N.ns) return;
+    const int step = *N.step - 1;
+    if (step < 0) return;
+    const size_t ns = (size_t)N.ns;
+    const int64_t c = N.cell[s];
+    const int64_t st = N.nstride[s];
+    S *r = reinterpret_cast<S *>(N.ring) + (size_t)(step % NFFF_RING) * 9 * ns + s;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float *E = N.e[a];
+        r[(3 * a) * ns] = (S)ld_any(E, c, N.storage);
+        r[(3 * a + 1) * ns] = (S)ld_any(E, c + st, N.storage);
+        r[(3 * a + 2) * ns] = (S)ld_any(E, c - st, N.storage);
+    }
+}
+
+__global__ void nfff_sample_kernel(const DevNfff N)
+{
+    if (N.storage == FDTD_STORE_F64) nfff_sample_cell<double>(N, blockIdx.x * blockDim.x + threadIdx.x);
+    else nfff_sample_cell<float>(N, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// the step counter is the same for every thread of the launch: a CTA either
+// leaves at once or reaches the twiddle table's barrier with all its threads
+template <class S>
+__device__ __forceinline__ void nfff_fold_full_ring(const DevNfff &N, int s)
+{
+    if (N.ns <= 0 || N.nfreq <= 0) return;
+    const int step = *N.step - 1;
+    if (step < 0 || step % NFFF_RING != NFFF_RING - 1) return;
+    __shared__ double2 tw[NFFF_RING * NFFF_TW_MAXF];
+    const bool table = N.nfreq <= NFFF_TW_MAXF;
+    if (table) nfff_twiddles(N, step - (NFFF_RING - 1), NFFF_RING, tw);
+    if (s < N.ns) nfff_fold<S>(N, s, step - (NFFF_RING - 1), NFFF_RING, false, table ? tw : nullptr);
+}
+
+__global__ void nfff_fold_kernel(const DevNfff N)
+{
+    if (N.storage == FDTD_STORE_F64) nfff_fold_full_ring<double>(N, blockIdx.x * blockDim.x + threadIdx.x);
+    else nfff_fold_full_ring<float>(N, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __global__ void nfff_accumulate_batch(const DevNfff *N)
@@ -774,7 +818,8 @@ void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, c
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st)
 {
     if (n.ns <= 0) return;
-    nfff_accumulate_kernel<<<(n.ns + 255) / 256, 256, 0, st>>>(n);
+    nfff_sample_kernel<<<(n.ns + 255) / 256, 256, 0, st>>>(n);
+    nfff_fold_kernel<<<(n.ns + 255) / 256, 256, 0, st>>>(n);
 }
 
 void launch_nfff_fold_pending(const DevNfff &n, cudaStream_t st)

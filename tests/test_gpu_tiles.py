@@ -73,8 +73,8 @@ def test_tiles_use_three_layouts_and_match_slab_path(monkeypatch):
     g = Solver(s)
     g.set_fields(init)
     prof = g.step_profile(1)
-    # aux grid, TSF faces, four tile kinds (bulk; CPML x, y and z slabs), NFFF running DFT
-    assert int(prof["launches_per_step"]) == 7, prof
+    # aux grid, TSF faces, four tile kinds (bulk; CPML x, y and z slabs), NFFF sampling and ring fold
+    assert int(prof["launches_per_step"]) == 8, prof
     g.step(29)
     monkeypatch.setenv("GSVIT_B200_NO_BULK", "1")
     h = Solver(s)
