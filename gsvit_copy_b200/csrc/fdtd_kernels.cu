@@ -401,11 +401,48 @@ __device__ __forceinline__ void nfff_twiddles(const DevNfff &N, int first_step, 
 
 // tw: the CTA's twiddle table, or nullptr to evaluate them per cell.  S: the
 // element type of the sample ring (FP32; FP64 for FP64-storage plans)
-template <class S>
+// STAGE (FP32 samples only): the cell's ring (8 x 9 values) is read once into
+// registers instead of once per frequency (the ring is far larger than L2),
+// at 144 registers a thread; the same arithmetic in the same order.
+template <class S, bool STAGE = false>
 __device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_step, int nslots, bool clear, const double2 *tw)
 {
     const size_t ns = (size_t)N.ns;
     S *ring = reinterpret_cast<S *>(N.ring);
+    if constexpr (STAGE && sizeof(S) == 4) {
+        float rv[NFFF_RING][9];
+#pragma unroll
+        for (int j = 0; j < NFFF_RING; j++)
+#pragma unroll
+            for (int q = 0; q < 9; q++) rv[j][q] = j < nslots ? ring[((size_t)j * 9 + q) * ns + s] : 0.f;
+        for (int f = 0; f < N.nfreq; f++) {
+            double2 A[6];
+            for (int q = 0; q < 6; q++) A[q] = N.acc[((size_t)f * 6 + q) * ns + s];
+#pragma unroll
+            for (int j = 0; j < NFFF_RING; j++) {
+                if (j >= nslots) break;
+                double v[6];
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    v[a] = (double)rv[j][3 * a];
+                    v[3 + a] = ((double)rv[j][3 * a + 1] - (double)rv[j][3 * a + 2]) * N.inv2dx;
+                }
+                double sn, cs;
+                if (tw) { cs = tw[f * nslots + j].x; sn = tw[f * nslots + j].y; }
+                else sincos(N.omega_dt[f] * (double)(first_step + j), &sn, &cs);
+#pragma unroll
+                for (int q = 0; q < 6; q++) {
+                    A[q].x += v[q] * cs;
+                    A[q].y -= v[q] * sn;
+                }
+            }
+            for (int q = 0; q < 6; q++) N.acc[((size_t)f * 6 + q) * ns + s] = A[q];
+        }
+        if (clear)
+            for (int j = 0; j < nslots; j++)
+                for (int q = 0; q < 9; q++) ring[((size_t)j * 9 + q) * ns + s] = 0;
+        return;
+    }
     for (int f = 0; f < N.nfreq; f++) {
         double2 A[6];
         for (int q = 0; q < 6; q++) A[q] = N.acc[((size_t)f * 6 + q) * ns + s];
@@ -521,10 +558,10 @@ __device__ __forceinline__ void nfff_fold_full_ring(const DevNfff &N, int s)
     __shared__ double2 tw[NFFF_RING * NFFF_TW_MAXF];
     const bool table = N.nfreq <= NFFF_TW_MAXF;
     if (table) nfff_twiddles(N, step - (NFFF_RING - 1), NFFF_RING, tw);
-    if (s < N.ns) nfff_fold<S>(N, s, step - (NFFF_RING - 1), NFFF_RING, false, table ? tw : nullptr);
+    if (s < N.ns) nfff_fold<S, true>(N, s, step - (NFFF_RING - 1), NFFF_RING, false, table ? tw : nullptr);
 }
 
-__global__ void nfff_fold_kernel(const DevNfff N)
+__global__ void __launch_bounds__(128, 3) nfff_fold_kernel(const DevNfff N)
 {
     if (N.storage == FDTD_STORE_F64) nfff_fold_full_ring<double>(N, blockIdx.x * blockDim.x + threadIdx.x);
     else nfff_fold_full_ring<float>(N, blockIdx.x * blockDim.x + threadIdx.x);
@@ -819,7 +856,7 @@ void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st)
 {
     if (n.ns <= 0) return;
     nfff_sample_kernel<<<(n.ns + 255) / 256, 256, 0, st>>>(n);
-    nfff_fold_kernel<<<(n.ns + 255) / 256, 256, 0, st>>>(n);
+    nfff_fold_kernel<<<(n.ns + 127) / 128, 128, 0, st>>>(n);
 }
 
 void launch_nfff_fold_pending(const DevNfff &n, cudaStream_t st)
