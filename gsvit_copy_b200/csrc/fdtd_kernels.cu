@@ -468,9 +468,10 @@ __device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_ste
             for (int q = 0; q < 9; q++) ring[((size_t)j * 9 + q) * ns + s] = 0;
 }
 
-// the step counter, the slot and the fold decision are the same for every
-// thread of a launch (one plan per CTA in a batch), so the CTA-wide twiddle
-// table and its barrier are reached by all threads
+// Sampling and fold in one pass, for batches (one plan per CTA row, so the
+// step counter, the slot and the fold decision are the same for every thread
+// of a CTA, and the CTA-wide twiddle table and its barrier are reached by all
+// of them).  Single plans split the two (nfff_sample_kernel, nfff_fold_kernel).
 template <class S>
 __device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
 {
