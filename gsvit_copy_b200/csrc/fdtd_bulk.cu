@@ -325,6 +325,8 @@ __device__ __forceinline__ bool bulk_item(const DevPlan &P, const BulkMaps &M, c
                 }
             }
         }
+        // the TSF correction entries this group's H and E will take, into L1
+        if (tsf_plane && ok) tsf_prefetch_group<float>(P, i, j, kq);
         // CPML tiles: the next plane's psi lines into L2, one request per
         // 128-byte line of a row (the row's first own group and every group
         // on a line boundary)

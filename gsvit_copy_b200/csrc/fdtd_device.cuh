@@ -247,6 +247,7 @@ __device__ __forceinline__ void stPsiE(const DevPlan &P, float *p, int64_t i, re
 
 // a hint that moves the line holding p into L2; no register, no wait
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 // ---- 4-vectors of the storage type
 
@@ -428,5 +429,39 @@ __device__ __forceinline__ void tsf_add_e(const DevPlan &P, int i, int j, int k,
     if (ii && ji) {
         if (k == k0) { const V2 d = tc[4][(i - i0) * P.tnb[4] + (j - j0)]; ex += d.x; ey += d.y; }
         if (k == kn) { const V2 d = tc[5][(i - i0) * P.tnb[5] + (j - j0)]; ex += d.x; ey += d.y; }
+    }
+}
+
+// L1 prefetch of the entries tsf_add_h and tsf_add_e read for the cells
+// (i, j, kq .. kq+3) of a 4-cell group, under the same tests (every address
+// is one those calls read).  Issued at the top of a plane: their reads come
+// at the end of the H and E phases, where an L2 round trip of the warp that
+// holds a face group would hold the whole CTA at the plane's barrier.
+template <class R>
+__device__ __forceinline__ void tsf_prefetch_group(const DevPlan &P, int i, int j, int kq)
+{
+    using V2 = typename Tab<R>::V2;
+    const V2 *const *th = reinterpret_cast<const V2 *const *>(P.tcor_h);
+    const V2 *const *te = reinterpret_cast<const V2 *const *>(P.tcor_e);
+    const int i0 = P.t0[0], j0 = P.t0[1], k0 = P.t0[2], in = P.t1[0], jn = P.t1[1], kn = P.t1[2];
+    const int kh = kq + 3;
+    const bool ji = j >= j0 && j <= jn, ii = i >= i0 && i <= in;
+    const bool kany = kh >= k0 && kq <= kn;               // some cell of the group has k0 <= k <= kn
+    const int kk = (kq > k0 ? kq : k0) - k0;              // its first such cell, from k0
+    if (ii && ji) {   // k faces: one entry per (i, j)
+        const int q4 = (i - i0) * P.tnb[4] + (j - j0), q5 = (i - i0) * P.tnb[5] + (j - j0);
+        if (kq <= k0 - 1 && kh >= k0 - 1) prefetch_l1(th[4] + q4);
+        if (kq <= k0 && kh >= k0) prefetch_l1(te[4] + q4);
+        if (kq <= kn && kh >= kn) { prefetch_l1(th[5] + q5); prefetch_l1(te[5] + q5); }
+    }
+    if (ii && kany) {   // j faces: the group's entries are consecutive in k
+        if (j == j0 - 1) prefetch_l1(th[2] + (i - i0) * P.tnb[2] + kk);
+        if (j == j0) prefetch_l1(te[2] + (i - i0) * P.tnb[2] + kk);
+        if (j == jn) { prefetch_l1(th[3] + (i - i0) * P.tnb[3] + kk); prefetch_l1(te[3] + (i - i0) * P.tnb[3] + kk); }
+    }
+    if (ji && kany) {   // i faces
+        if (i == i0 - 1) prefetch_l1(th[0] + (j - j0) * P.tnb[0] + kk);
+        if (i == i0) prefetch_l1(te[0] + (j - j0) * P.tnb[0] + kk);
+        if (i == in) { prefetch_l1(th[1] + (j - j0) * P.tnb[1] + kk); prefetch_l1(te[1] + (j - j0) * P.tnb[1] + kk); }
     }
 }
