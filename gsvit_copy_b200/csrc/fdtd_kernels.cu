@@ -468,38 +468,6 @@ __device__ __forceinline__ void nfff_fold(const DevNfff &N, int s, int first_ste
             for (int q = 0; q < 9; q++) ring[((size_t)j * 9 + q) * ns + s] = 0;
 }
 
-// Sampling and fold in one pass, for batches (one plan per CTA row, so the
-// step counter, the slot and the fold decision are the same for every thread
-// of a CTA, and the CTA-wide twiddle table and its barrier are reached by all
-// of them).  Single plans split the two (nfff_sample_kernel, nfff_fold_kernel).
-template <class S>
-__device__ __forceinline__ void nfff_accumulate_cell(const DevNfff &N, int s)
-{
-    if (N.ns <= 0 || N.nfreq <= 0) return;   // a batch instance without a running DFT: zeroed, no step counter
-    const int step = *N.step - 1;
-    if (step < 0) return;
-    const bool live = s < N.ns;
-    const int slot = step % NFFF_RING;
-    const size_t ns = (size_t)N.ns;
-    if (live) {
-        const int64_t c = N.cell[s];
-        const int64_t st = N.nstride[s];
-        S *r = reinterpret_cast<S *>(N.ring) + (size_t)slot * 9 * ns + s;
-        for (int a = 0; a < 3; a++) {
-            const float *E = N.e[a];
-            r[(3 * a) * ns] = (S)ld_any(E, c, N.storage);
-            r[(3 * a + 1) * ns] = (S)ld_any(E, c + st, N.storage);
-            r[(3 * a + 2) * ns] = (S)ld_any(E, c - st, N.storage);
-        }
-    }
-    if (slot == NFFF_RING - 1) {
-        __shared__ double2 tw[NFFF_RING * NFFF_TW_MAXF];
-        const bool table = N.nfreq <= NFFF_TW_MAXF;
-        if (table) nfff_twiddles(N, step - (NFFF_RING - 1), NFFF_RING, tw);
-        if (live) nfff_fold<S>(N, s, step - (NFFF_RING - 1), NFFF_RING, false, table ? tw : nullptr);
-    }
-}
-
 // the steps since the last full block (device step counter % NFFF_RING); their
 // slots are cleared, so the fold at the end of the block adds zeros for them
 __global__ void nfff_fold_pending_kernel(const DevNfff N)
@@ -518,7 +486,7 @@ __global__ void nfff_fold_pending_kernel(const DevNfff N)
     }
 }
 
-// A single plan's NFFF step in two launches: the sampling, which every step
+// The NFFF step in two launches (single plans and batches): the sampling, which every step
 // does, in a light kernel (few registers, full occupancy: its nine gathered
 // loads a cell want many in flight), and the fold, which only the step that
 // fills the ring does, in a kernel that every other step leaves at once.
@@ -568,9 +536,16 @@ __global__ void __launch_bounds__(128, 3) nfff_fold_kernel(const DevNfff N)
     else nfff_fold_full_ring<float>(N, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-__global__ void nfff_accumulate_batch(const DevNfff *N)
+// batches: one plan per CTA row (blockIdx.y), so the step counter and the fold
+// decision are the same for every thread of a CTA
+__global__ void nfff_sample_batch(const DevNfff *N)
 {
-    nfff_accumulate_cell<float>(N[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
+    nfff_sample_cell<float>(N[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void __launch_bounds__(128, 3) nfff_fold_batch(const DevNfff *N)
+{
+    nfff_fold_full_ring<float>(N[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------------ far-field integration
@@ -850,7 +825,9 @@ cudaError_t launch_slab_e_plain_batch(const DevPlan *p, const SlabBox *boxes, in
 
 void launch_nfff_accumulate_batch(const DevNfff *n, int nplans, int max_cells, cudaStream_t st)
 {
-    if (nplans > 0 && max_cells > 0) nfff_accumulate_batch<<<dim3((max_cells + 255) / 256, nplans), 256, 0, st>>>(n);
+    if (nplans <= 0 || max_cells <= 0) return;
+    nfff_sample_batch<<<dim3((max_cells + 255) / 256, nplans), 256, 0, st>>>(n);
+    nfff_fold_batch<<<dim3((max_cells + 127) / 128, nplans), 128, 0, st>>>(n);
 }
 
 void launch_nfff_accumulate(const DevNfff &n, cudaStream_t st)
